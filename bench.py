@@ -1,0 +1,355 @@
+"""Benchmark of the batched align_group_to_template path on B200.
+
+Workload (default): 2000 synthetic 512x512 uint16 frames (400-blob template, per-line random-walk
+motion with jumps, Poisson noise at a 200-photon peak), knots every 2 lines (257 knots per frame),
+aligned in groups of 64 frames, precision 'S' (FP32 pixel arithmetic, FP64 reduction and solve),
+lambda 5e-3, default settings otherwise. One step aligns all frames, every group from its initial
+knots to its stop criterion.
+
+  value   frames/s with the frames already resident in HBM (CUDA events on the engine's stream)
+  e2e     frames/s through the public C ABI (ss_align_groups) from pinned host buffers, host->device
+          and device->host copies inside the timed region
+Prints ONE JSON line (rank 0). ``--impl reference`` times the reference algorithm's CPU
+restatement on a bounded sample of the same workload instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s at 512², 2-line knots; p99 group latency vs plain GPU, ≤0.05px vs FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=2000)
+    ap.add_argument("--group", type=int, default=64)
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--precision", default="S", choices=["S", "D"])
+    ap.add_argument("--cpu-sample-frames", type=int, default=4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# workload
+
+def make_workload(n_frames, size, group, precision, seed, device):
+    """Returns (groups: list of host argument dicts, device frame tensors per group, settings)."""
+    import torch
+
+    from steadyscan_b200 import prep, synth
+    rng = np.random.default_rng(seed)
+    nk = size // 2 + 1
+    tmpl = synth.make_template(size, size, 400 * (size * size) // (512 * 512), (2.0, 6.0), rng)
+    walk = synth.make_walk(size * (n_frames + 1), 0.1, 10.0, (0, 3), size, 4.0, rng)
+    s = prep.init_settings({"nknots": nk, "gpu_forced_precision": precision, "lambda": 5e-3}, tmpl, size, size)
+    lay = prep.block_layout(s)
+    k = size // (nk - 1)
+    T = torch.tensor(tmpl, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    jj = torch.arange(size, device=device, dtype=torch.float64)[None, :]
+    ll = torch.arange(size, device=device, dtype=torch.float64)[:, None]
+    wl_all = torch.tensor(walk, device=device)
+    bg = float(tmpl.min())
+    frames_bm = []
+    for f in range(n_frames):
+        wl = wl_all[f * size:(f + 1) * size]
+        x = jj + wl[:, 0:1]
+        y = ll + wl[:, 1:2]
+        x0 = torch.floor(x)
+        y0 = torch.floor(y)
+        fx, fy = x - x0, y - y0
+        x0l, y0l = x0.long(), y0.long()
+        inside = (x0l >= 0) & (y0l >= 0) & (x0l < size - 1) & (y0l < size - 1)
+        xc, yc = x0l.clamp(0, size - 2), y0l.clamp(0, size - 2)
+        v = (1 - fx) * ((1 - fy) * T[yc, xc] + fy * T[yc + 1, xc]) + fx * ((1 - fy) * T[yc, xc + 1] + fy * T[yc + 1, xc + 1])
+        lam = torch.where(inside, v, torch.full_like(v, bg))
+        cnt = torch.poisson(lam, generator=gen).clamp(0, 65535).to(torch.int32).to(torch.uint16)
+        # block-matrix column cc holds lines cc*k .. cc*k+k-1, MATLAB column-major inside the block
+        frames_bm.append(cnt.view(nk - 1, k, size).permute(0, 2, 1).contiguous().view(-1))
+    groups, dev = [], []
+    for g0 in range(0, n_frames, group):
+        nF = min(group, n_frames - g0)
+        flat = torch.cat(frames_bm[g0:g0 + nF])
+        dev.append(flat)
+        host = flat.cpu().numpy().reshape(lay.frame_h, lay.frame_w * nF, order="F")
+        args = prep.boundary_arguments(s, tmpl, host, nF, layout=lay)
+        groups.append(args)
+    return groups, dev, s, lay
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap,power.draw")
+
+    def __init__(self, index=0):
+        self.rows, self.proc, self.index = [], None, index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_summary():
+    p = os.path.join(ROOT, "profiles", "k_eval_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return None
+
+
+# ------------------------------------------------------------------------------------------------
+
+def cpu_sample(groups, n_frames, threads):
+    """The FP64 CPU restatement on the first ``n_frames`` frames of the first group (frames/s)."""
+    from oracle import oracle
+    oracle.build()
+    a = dict(groups[0])
+    hb, w = a["tfrac"].shape
+    a["bmData"] = np.asarray(a["bmData"])[:, :w * n_frames].astype(np.float64)
+    a["nFrames"] = n_frames
+    a["est_dx_knots"] = np.zeros((w + 1, n_frames))
+    a["est_dy_knots"] = np.zeros((w + 1, n_frames))
+    a["flags"] = "D"
+    t0 = time.perf_counter()
+    o = oracle.align_group(a, n_threads=threads, want_mask=False)
+    dt = time.perf_counter() - t0
+    return n_frames / dt, dt, o, a
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        groups, _, _, _ = make_workload_cpu(args)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, dt, _, _ = cpu_sample(groups, args.cpu_sample_frames, threads)
+            if i >= args.warmup:
+                vals.append(v)
+        value = float(np.mean(vals))
+        sample = f"{args.cpu_sample_frames} frames of one {args.size}x{args.size} group, FP64, {threads} threads"
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s",
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1000.0 * args.cpu_sample_frames / value, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": workload_config(args),
+                          "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    device = torch.device("cuda", local)
+    from steadyscan_b200 import api
+    from steadyscan_b200._lib import SS_U16
+
+    groups, dev_frames, settings, lay = make_workload(args.frames, args.size, args.group, args.precision,
+                                                      1002 + 17 * rank, device)
+    torch.cuda.synchronize()
+    # device-resident inputs for `value`
+    dgroups = []
+    for g, t in zip(groups, dev_frames):
+        d = dict(g)
+        d["bmData"] = api.DeviceMatrix(t.data_ptr(), lay.frame_h, lay.frame_w * int(g["nFrames"]), SS_U16, owner=t)
+        dgroups.append(d)
+    batch = api.Batch(dgroups)
+    stream = torch.cuda.ExternalStream(batch.stream_ptr, device=device)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        batch.run()
+    barrier()
+    launches = 0
+    with ClockSampler(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            batch.run()
+            launches += batch.stats()["kernel_launches"]
+        e1.record(stream)
+        barrier()
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_total], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = args.frames * world / (ms_step / 1000.0)
+    st = batch.stats()
+
+    # roofline of the evaluation kernel from one extra run with event timing inside the engine
+    batch.set_timing(True)
+    batch.run()
+    torch.cuda.synchronize()
+    rs = batch.stats()
+    batch.set_timing(False)
+    results = batch.collect()
+    frame_bytes = lay.frame_h * lay.frame_w * 2
+    passes = rs["frame_passes"]
+    eval_ms = sum(rs["eval_ms"])
+    launches_eval = None
+    algo_bytes = sum(passes) * frame_bytes
+    achieved = algo_bytes / (eval_ms / 1000.0) / 1e9 if eval_ms > 0 else None
+    peak, peak_kind = peaks()
+    tr = traffic_summary()
+    roofline = {"kernel": "k_eval (assembly, trial, correlation, final passes)", "bound": "hbm",
+                "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                "traffic": tr.get("bytes_per_frame_pass") if tr else None,
+                "algorithmic_bytes_per_frame_pass": frame_bytes,
+                "frame_passes": passes, "eval_ms_by_pass": rs["eval_ms"], "eval_share_of_step":
+                    eval_ms / rs["run_ms"] if rs["run_ms"] else None}
+
+    # end to end through the public C ABI from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        pinned = []
+        hgroups = []
+        h2d = 0
+        for g in groups:
+            d = dict(g)
+            src = np.asarray(g["bmData"])
+            pt = torch.empty(src.size, dtype=torch.int16, pin_memory=True)
+            pv = pt.numpy().view(np.uint16).reshape(src.shape, order="F")
+            pv[...] = src
+            pinned.append(pt)
+            d["bmData"] = pv
+            hgroups.append(d)
+            h2d += src.nbytes + sum(np.asarray(g[k]).nbytes for k in ("template_image", "xgrad", "ygrad", "tfrac",
+                                                                      "basex", "basey", "base_mask"))
+        api.align_groups(hgroups, want_mask=False)  # warm-up
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(max(1, min(args.steps, 2))):
+            res = api.align_groups(hgroups, want_mask=False)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / max(1, min(args.steps, 2))
+        w1 = lay.frame_w + 1
+        d2h = sum(int(g["nFrames"]) * (2 * w1 + 2) * 8 + 8 for g in groups)
+        e2e = {"value": args.frames * world / dt, "unit": "frames/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "api": "ss_align_groups"}
+
+    cpu = None
+    acc = None
+    if rank == 0 and not args.no_cpu:
+        v, dt, o, a = cpu_sample(groups, args.cpu_sample_frames, threads)
+        cpu = {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_sample_frames} frames of one {args.size}x{args.size} group, FP64 oracle, "
+                         f"{dt:.1f} s"}
+        # accuracy of the timed precision against the FP64 oracle on that sample
+        a2 = dict(a)
+        a2["flags"] = args.precision
+        g = api.align_group(a2, want_mask=False)
+        rms = float(np.sqrt(np.mean(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]) ** 2)))
+        mx = float(np.max(np.abs(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]))))
+        acc = {"rms_px_vs_fp64": rms, "max_px_vs_fp64": mx, "sample": f"{args.cpu_sample_frames} frames"}
+
+    if rank == 0:
+        iters = [r["iter_used"] for r in results]
+        line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32" if args.precision == "S" else "f64", "data": "synthetic",
+                "config": workload_config(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc,
+                "run": {"cycles": st["cycles"], "linesearch_rounds": st["linesearch_rounds"],
+                        "iterations_min": int(min(iters)), "iterations_max": int(max(iters)),
+                        "arena_bytes": st["arena_bytes"]}}
+        print(json.dumps(line))
+    batch.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def workload_config(args):
+    return {"workload": f"{args.frames} frames {args.size}x{args.size} uint16, knots every 2 lines "
+                        f"({args.size // 2 + 1} knots), groups of {args.group} frames, precision {args.precision} "
+                        f"(FP32 pixel arithmetic, FP64 reduction and solve), lambda 5e-3, default settings",
+            "frames": args.frames, "group_frames": args.group, "frame_size": args.size,
+            "l2": "frames resident in HBM exceed L2 (1 GB vs 126 MB); no flush"}
+
+
+def make_workload_cpu(args):
+    import torch
+    return make_workload(min(args.frames, args.cpu_sample_frames), args.size, args.group, "D", 1002, "cpu")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/* steadyscan_b200: B200-native align_group_to_template behind a plain C ABI.
+ *
+ * The entry points below replace the reference's MATLAB MEX function
+ *   void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[])
+ * (setup/source/mex/align_group_to_template.cpp:21-85), whose 26 inputs are converted in
+ * setup/source/mex/mexgateway.cpp:31-255 and whose outputs are produced in mexgateway.cpp:261-370.
+ * The arguments keep the MEX order, names and meaning; matrices keep MATLAB's column-major layout.
+ * No torch or CUDA types appear in the signatures. Errors are returned as status codes (the
+ * reference aborts the MATLAB call through mexErrMsgIdAndTxt, mex/reporter/reporter.cpp:25-27);
+ * ss_last_error() gives the message of the calling thread's last failure.
+ */
+#ifndef STEADYSCAN_B200_H_
+#define STEADYSCAN_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SS_API __attribute__((visibility("default")))
+#else
+#define SS_API
+#endif
+
+/* Element types of an ss_matrix. */
+enum ss_dtype {
+  SS_F64 = 0, /* double */
+  SS_F32 = 1, /* float */
+  SS_U16 = 2, /* uint16 photon counts (frame storage) */
+  SS_F16 = 3, /* IEEE half (frame or template storage) */
+  SS_U8 = 4,  /* logical / uint8 */
+  SS_I32 = 5  /* int32 */
+};
+
+/* Where an ss_matrix's data lives. */
+enum ss_location {
+  SS_HOST = 0,  /* host memory; copied to the device inside the call */
+  SS_DEVICE = 1 /* device memory of gpu_device_id; used in place */
+};
+
+/* Status codes. */
+enum ss_status {
+  SS_OK = 0,
+  SS_ERR_INVALID_ARGUMENT = -1, /* GPUMC:InvalidArgument / NotEnoughInputs (mex/reporter/reporter.cpp:3-12) */
+  SS_ERR_CUDA = -2,             /* GPUMC:CudaError */
+  SS_ERR_OUT_OF_MEMORY = -3,    /* device allocation failed (task.cpp:116-131) */
+  SS_ERR_NO_DEVICE = -4,
+  SS_ERR_BUSY = -5,             /* serving: admission refused (memory budget or queue) */
+  SS_ERR_NOT_FOUND = -6         /* serving: unknown session or request */
+};
+
+/* A matrix argument, MATLAB layout: element (i, j) at data[i + j * rows]. */
+typedef struct ss_matrix {
+  const void* data;
+  int64_t rows;
+  int64_t cols;
+  int32_t dtype;    /* enum ss_dtype */
+  int32_t location; /* enum ss_location */
+} ss_matrix;
+
+/* The 26 inputs of align_group_to_template, in MEX order (mexgateway.cpp:38-174;
+ * caller steady_scan.m:239-242). Index comments give the prhs[] slot. */
+typedef struct ss_inputs {
+  const char* flags;              /*  0: precision letter 'D' or 'S' + gpu_flags (configuration.cpp:83-152) */
+  ss_matrix template_image;       /*  1: Ht x Wt */
+  ss_matrix xgrad;                /*  2: Ht x Wt, forward difference along x, NaN last column */
+  ss_matrix ygrad;                /*  3: Ht x Wt, forward difference along y, NaN last row */
+  ss_matrix tfrac;                /*  4: Hb x W, scan-time fraction between knots */
+  ss_matrix basex;                /*  5: Hb x W, 0-based template x of each undisplaced pixel */
+  ss_matrix basey;                /*  6: Hb x W */
+  ss_matrix base_mask;            /*  7: Hb x W logical */
+  ss_matrix bm_data;              /*  8: Hb x (W * n_frames) frames in block-matrix order */
+  ss_matrix est_dx_knots;         /*  9: (W+1) x n_frames initial x knots */
+  ss_matrix est_dy_knots;         /* 10: (W+1) x n_frames initial y knots */
+  int32_t group_size;             /* 11: W * gpu_frame_groupsize; a positive multiple of W */
+  int32_t n_frames;               /* 12 */
+  ss_matrix min_points_per_block; /* 13: >= W entries (int32 or double, truncated) */
+  int32_t max_iter;               /* 14 */
+  double move_thresh;             /* 15 */
+  double halt_correlation;        /* 16 */
+  double correlation_increase_threshold; /* 17 */
+  double filter_strength;         /* 18 */
+  int32_t max_filter_iterations;  /* 19 */
+  double filter_deactivation_threshold; /* 20 */
+  double lambda;                  /* 21: knot-difference regulariser weight (the reference ignores it; 0 = reference) */
+  double linesearch_reduction_multiplier; /* 22 */
+  int32_t solver_id;              /* 23: 0 ILU(0) in x|y order, 1 and 2 exact (2 keeps SolverEigen's matrix between solves) */
+  int32_t filter_id;              /* 24: 0 none, 1 smearing, 2 range */
+  int32_t gpu_device_id;          /* 25 */
+  /* Extension: storage type of template samples on the device for precision 'S'
+   * (SS_F32 default, or SS_F16). Precision 'D' always keeps FP64. */
+  int32_t template_storage;
+} ss_inputs;
+
+/* Outputs; every pointer may be NULL (that output is then not produced). Host memory. Index
+ * comments give the plhs[] slot (mexgateway.cpp:266-354). */
+typedef struct ss_outputs {
+  double* dx_knots;           /* 1: (W+1) * n_frames, per-frame knots (last repeats knot W-1) */
+  double* dy_knots;           /* 2 */
+  double* frame_corr;         /* 3: n_frames */
+  int32_t* iter_used;         /* 4: scalar */
+  uint8_t* mask;              /* 5: Hb x (W * n_frames) logical, column-major */
+  double* residrms;           /* 6: n_frames */
+  double* device_init_time;   /* 7: seconds */
+  double* iteration_corr;     /* 8: max_iter (flag C) */
+  double* frame_corr_history; /* 11: n_frames x max_iter column-major (flag c) */
+  double* iteration_errvals;  /* 12: (2 * max_iter) x n_frames column-major (flag e) */
+  double* raw_params;         /* 13: 2N chain (flag P) */
+  double* all_params;         /* 15: 2N x max_iter column-major */
+  double* frame_params;       /* flag p: n_frames x 2(W+1) column-major */
+  int32_t stop_reason;        /* StopCriterion (interface/stopcriterion.h:4-10) */
+  int32_t trial_cap_hit;      /* a line search hit its trial bound (the reference loops without one) */
+  int64_t n_frame_passes;     /* frame evaluations read from memory (assembly, trials, correlation, final) */
+  double elapsed_ms;          /* wall time of the call */
+} ss_outputs;
+
+/* align_group_to_template: one group of frames (replaces mexFunction,
+ * mex/align_group_to_template.cpp:21-85, and MexGateway<T>::execute, mexgateway.cpp:372-445). */
+SS_API int ss_align_group_to_template(const ss_inputs* in, ss_outputs* out);
+
+/* Many independent groups in one batched run on one GPU (the MATLAB driver's per-set loop,
+ * steady_scan.m:216-287, done concurrently). in[i] and out[i] describe group i; all groups must
+ * use the same precision letter, frame dtype and device. */
+SS_API int ss_align_groups(int32_t n_groups, const ss_inputs* in, ss_outputs* out);
+
+/* A prepared batch: inputs validated and resident on the device, reusable for repeated runs
+ * (each run starts every group from its initial knots). ss_align_groups is create + run +
+ * collect + destroy. Run statistics come back in ss_batch_stats. */
+typedef struct ss_batch ss_batch;
+
+typedef struct ss_batch_stats {
+  int32_t n_groups;
+  int32_t cycles;             /* half-step cycles of the last run */
+  int32_t linesearch_rounds;  /* trial rounds of the last run */
+  int32_t kernel_launches;    /* kernels launched by the last run */
+  int64_t frame_passes[4];    /* frames evaluated per pass kind: assembly, trial, correlation, final */
+  double eval_ms[4];          /* device time of the evaluation kernels per pass kind (timing on) */
+  int64_t arena_bytes;        /* device memory held by the batch */
+  double run_ms;              /* wall time of the last run */
+} ss_batch_stats;
+
+SS_API int ss_batch_create(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_batch** batch);
+SS_API int ss_batch_run(ss_batch* batch);
+SS_API int ss_batch_collect(ss_batch* batch);
+/* 1 turns on CUDA-event timing of the evaluation kernels for later runs (adds events to the stream). */
+SS_API int ss_batch_set_timing(ss_batch* batch, int32_t on);
+SS_API int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats);
+/* The cudaStream_t the batch launches on, as an opaque pointer (for the caller's own events). */
+SS_API void* ss_batch_stream(const ss_batch* batch);
+SS_API void ss_batch_destroy(ss_batch* batch);
+
+/* Message of the calling thread's last error ("" if none). */
+SS_API const char* ss_last_error(void);
+
+/* SS_ABI_VERSION of the loaded library. */
+SS_API int32_t ss_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STEADYSCAN_B200_H_ */

@@ -1,0 +1,228 @@
+"""Python mirror of the reference's ``align_group_to_template`` MEX interface.
+
+``align_group_to_template(flags, template_image, xgrad, ygrad, tfrac, basex, basey, base_mask, bmData,
+est_dx_knots, est_dy_knots, group_size, nFrames, min_points_per_block, max_iter, move_thresh,
+halt_correlation, correlation_increase_threshold, filter_strength, max_filter_iterations,
+filter_deactivation_threshold, lambda, linesearch_reduction_multiplier, solver_id, filter_id,
+gpu_device_id, nargout=6)`` takes the 26 arguments of the MEX call (steady_scan.m:239-242,
+mex/mexgateway.cpp:38-174) and returns its first ``nargout`` outputs
+``(dx_knots, dy_knots, frame_corr, iter_used, mask, residrms, ...)`` (mexgateway.cpp:266-354).
+All work runs in the CUDA library through its C ABI; errors raise :class:`SteadyScanError` with
+the library's message. ``align_group`` / ``align_groups`` take the argument dict built by
+:func:`steadyscan_b200.prep.boundary_arguments` and return dicts; ``align_groups`` runs many groups
+in one batched GPU run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (SS_DEVICE, SS_F16, SS_F32, SS_F64, SS_HOST, SS_I32, SS_U8, SS_U16, STOP_NAMES, SSInputs,
+                   SSMatrix, SSOutputs, SteadyScanError, check, load)
+
+__all__ = ["align_group_to_template", "align_group", "align_groups", "DeviceMatrix", "SteadyScanError",
+           "ARG_NAMES", "STOP_NAMES"]
+
+ARG_NAMES = ["flags", "template_image", "xgrad", "ygrad", "tfrac", "basex", "basey", "base_mask", "bmData",
+             "est_dx_knots", "est_dy_knots", "group_size", "nFrames", "min_points_per_block", "max_iter",
+             "move_thresh", "halt_correlation", "correlation_increase_threshold", "filter_strength",
+             "max_filter_iterations", "filter_deactivation_threshold", "lambda", "linesearch_reduction_multiplier",
+             "solver_id", "filter_id", "gpu_device_id"]
+
+_NP_DTYPE = {np.dtype(np.float64): SS_F64, np.dtype(np.float32): SS_F32, np.dtype(np.uint16): SS_U16,
+             np.dtype(np.float16): SS_F16, np.dtype(np.uint8): SS_U8, np.dtype(np.bool_): SS_U8,
+             np.dtype(np.int32): SS_I32}
+_TORCH_DTYPE = {"torch.float64": SS_F64, "torch.float32": SS_F32, "torch.uint16": SS_U16,
+                "torch.float16": SS_F16, "torch.uint8": SS_U8, "torch.int32": SS_I32}
+
+
+class DeviceMatrix:
+    """A column-major matrix already in device memory: ``ptr`` to ``rows * cols`` elements."""
+
+    def __init__(self, ptr: int, rows: int, cols: int, dtype: int, owner=None):
+        self.ptr, self.rows, self.cols, self.dtype, self.owner = int(ptr), int(rows), int(cols), int(dtype), owner
+
+
+def _matrix(a, keep: list) -> SSMatrix:
+    if isinstance(a, DeviceMatrix):
+        return SSMatrix(a.ptr, a.rows, a.cols, a.dtype, SS_DEVICE)
+    if hasattr(a, "is_cuda") and a.is_cuda:  # torch tensor in column-major memory order
+        t = a
+        if t.dim() == 1:
+            rows, cols = t.shape[0], 1
+        else:
+            rows, cols = t.shape
+            if not (t.T.is_contiguous() or cols == 1):
+                raise ValueError("device matrices must be column-major (use tensor.T.contiguous().T)")
+        keep.append(t)
+        return SSMatrix(t.data_ptr(), rows, cols, _TORCH_DTYPE[str(t.dtype)], SS_DEVICE)
+    arr = np.asarray(a)
+    if arr.dtype not in _NP_DTYPE:
+        arr = arr.astype(np.float64)
+    if arr.dtype == np.bool_:
+        arr = arr.astype(np.uint8)
+    if arr.ndim == 0:
+        arr = arr.reshape(1, 1)
+    elif arr.ndim == 1:
+        arr = arr.reshape(-1, 1)
+    arr = np.asfortranarray(arr)
+    keep.append(arr)
+    return SSMatrix(arr.ctypes.data, arr.shape[0], arr.shape[1], _NP_DTYPE[arr.dtype], SS_HOST)
+
+
+def _inputs(args: dict, template_storage=None):
+    keep: list = []
+    flags = args["flags"].encode() if isinstance(args["flags"], str) else bytes(args["flags"])
+    keep.append(flags)
+    ts = {None: 0, "f32": SS_F32, "f16": SS_F16, np.float32: SS_F32, np.float16: SS_F16}.get(template_storage,
+                                                                                          template_storage)
+    i = SSInputs(
+        flags,
+        _matrix(args["template_image"], keep), _matrix(args["xgrad"], keep), _matrix(args["ygrad"], keep),
+        _matrix(args["tfrac"], keep), _matrix(args["basex"], keep), _matrix(args["basey"], keep),
+        _matrix(args["base_mask"], keep), _matrix(args["bmData"], keep), _matrix(args["est_dx_knots"], keep),
+        _matrix(args["est_dy_knots"], keep), int(args["group_size"]), int(args["nFrames"]),
+        _matrix(np.asarray(args["min_points_per_block"]).reshape(-1), keep), int(args["max_iter"]),
+        float(args["move_thresh"]), float(args["halt_correlation"]), float(args["correlation_increase_threshold"]),
+        float(args["filter_strength"]), int(args["max_filter_iterations"]),
+        float(args["filter_deactivation_threshold"]), float(args.get("lambda", 0.0)),
+        float(args["linesearch_reduction_multiplier"]), int(args["solver_id"]), int(args["filter_id"]),
+        int(args["gpu_device_id"]), int(ts or 0))
+    return i, keep
+
+
+def _outputs(args: dict, want_mask=True, want_history=False):
+    hb, w = np.asarray(args["tfrac"]).shape if not hasattr(args["tfrac"], "shape") else tuple(args["tfrac"].shape)
+    nF = int(args["nFrames"])
+    N = w * nF + 1
+    mi = int(args["max_iter"])
+    a = dict(dx=np.zeros((w + 1) * nF), dy=np.zeros((w + 1) * nF), frame_corr=np.zeros(nF),
+             iter_used=np.zeros(1, np.int32), residrms=np.zeros(nF), device_init_time=np.zeros(1),
+             raw_params=np.zeros(2 * N), frame_params=np.zeros(2 * (w + 1) * nF))
+    if want_mask:
+        a["mask"] = np.zeros(hb * w * nF, np.uint8)
+    if want_history:
+        a["iteration_corr"] = np.zeros(mi)
+        a["frame_corr_history"] = np.zeros(nF * mi)
+        a["iteration_errvals"] = np.zeros(2 * mi * nF)
+        a["all_params"] = np.zeros(2 * N * mi)
+    p = lambda k: a[k].ctypes.data if k in a else None
+    o = SSOutputs(p("dx"), p("dy"), p("frame_corr"), p("iter_used"), p("mask"), p("residrms"),
+                  p("device_init_time"), p("iteration_corr"), p("frame_corr_history"), p("iteration_errvals"),
+                  p("raw_params"), p("all_params"), p("frame_params"), 0, 0, 0, 0.0)
+    return o, a, (hb, w, nF, N, mi)
+
+
+def _result(o: SSOutputs, a: dict, dims) -> dict:
+    hb, w, nF, N, mi = dims
+    r = dict(dx=a["dx"], dy=a["dy"], frame_corr=a["frame_corr"], iter_used=int(a["iter_used"][0]),
+             residrms=a["residrms"], device_init_time=float(a["device_init_time"][0]),
+             stop_reason=int(o.stop_reason), stop_name=STOP_NAMES[o.stop_reason] if 0 <= o.stop_reason < 5 else "?",
+             trial_cap_hit=bool(o.trial_cap_hit), n_frame_passes=int(o.n_frame_passes),
+             elapsed_ms=float(o.elapsed_ms), raw_params=a["raw_params"],
+             frame_params=a["frame_params"].reshape(nF, 2 * (w + 1), order="F"))
+    if "mask" in a:
+        r["mask"] = a["mask"].reshape(hb, w * nF, order="F").astype(bool)
+    if "iteration_corr" in a:
+        r["iteration_corr"] = a["iteration_corr"]
+        r["frame_corr_history"] = a["frame_corr_history"].reshape(nF, mi, order="F")
+        r["iteration_errvals"] = a["iteration_errvals"].reshape(2 * mi, nF, order="F")
+        r["all_params"] = a["all_params"].reshape(2 * N, mi, order="F")
+    return r
+
+
+def align_groups(groups: list, want_mask: bool = True, want_history: bool = False, template_storage=None) -> list:
+    """Runs many groups (argument dicts) in one batched run on one GPU; returns a list of dicts."""
+    lib = load()
+    n = len(groups)
+    ins = (SSInputs * n)()
+    outs = (SSOutputs * n)()
+    keep, arrays, dims = [], [], []
+    for k, g in enumerate(groups):
+        i, kk = _inputs(g, template_storage)
+        ins[k] = i
+        keep.append(kk)
+        o, a, d = _outputs(g, want_mask, want_history)
+        outs[k] = o
+        arrays.append(a)
+        dims.append(d)
+    check(lib.ss_align_groups(n, ins, outs))
+    return [_result(outs[k], arrays[k], dims[k]) for k in range(n)]
+
+
+def align_group(args: dict, want_mask: bool = True, want_history: bool = False, template_storage=None) -> dict:
+    """One align_group_to_template call from the argument dict; returns a dict of outputs."""
+    lib = load()
+    i, keep = _inputs(args, template_storage)
+    o, a, d = _outputs(args, want_mask, want_history)
+    check(lib.ss_align_group_to_template(C.byref(i), C.byref(o)))
+    del keep
+    return _result(o, a, d)
+
+
+def align_group_to_template(*argv, nargout: int = 6, template_storage=None):
+    """MEX-style call with the 26 positional arguments; returns the first ``nargout`` outputs."""
+    if len(argv) < 26:
+        raise SteadyScanError(-1, f"not enough input arguments, expected 26 - received {len(argv)}")
+    args = dict(zip(ARG_NAMES, argv[:26]))
+    r = align_group(args, want_mask=nargout >= 5, want_history=nargout >= 8, template_storage=template_storage)
+    outs = [r["dx"], r["dy"], r["frame_corr"], np.int32(r["iter_used"]), r.get("mask"), r["residrms"],
+            r["device_init_time"]]
+    if nargout >= 8:
+        outs += [r["iteration_corr"], None, None, r["frame_corr_history"], r["iteration_errvals"], r["raw_params"],
+                 None, r["all_params"]]
+    return tuple(outs[:nargout])
+
+
+class Batch:
+    """A prepared batch of groups (ss_batch_*): inputs resident on the device, runnable repeatedly."""
+
+    def __init__(self, groups: list, want_mask: bool = False, want_history: bool = False, template_storage=None):
+        from ._lib import SSBatchStats  # noqa: F401
+        self._lib = load()
+        n = len(groups)
+        self._ins = (SSInputs * n)()
+        self._outs = (SSOutputs * n)()
+        self._keep, self._arrays, self._dims = [], [], []
+        for k, g in enumerate(groups):
+            i, kk = _inputs(g, template_storage)
+            self._ins[k] = i
+            self._keep.append(kk)
+            o, a, d = _outputs(g, want_mask, want_history)
+            self._outs[k] = o
+            self._arrays.append(a)
+            self._dims.append(d)
+        h = C.c_void_p()
+        check(self._lib.ss_batch_create(n, self._ins, self._outs, C.byref(h)))
+        self._h = h
+
+    def run(self):
+        check(self._lib.ss_batch_run(self._h))
+
+    def collect(self) -> list:
+        check(self._lib.ss_batch_collect(self._h))
+        return [_result(self._outs[k], self._arrays[k], self._dims[k]) for k in range(len(self._dims))]
+
+    def set_timing(self, on: bool):
+        check(self._lib.ss_batch_set_timing(self._h, 1 if on else 0))
+
+    def stats(self) -> dict:
+        from ._lib import SSBatchStats
+        st = SSBatchStats()
+        check(self._lib.ss_batch_stats_get(self._h, C.byref(st)))
+        return dict(n_groups=st.n_groups, cycles=st.cycles, linesearch_rounds=st.linesearch_rounds,
+                    kernel_launches=st.kernel_launches, frame_passes=list(st.frame_passes),
+                    eval_ms=list(st.eval_ms), arena_bytes=st.arena_bytes, run_ms=st.run_ms)
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self._lib.ss_batch_stream(self._h) or 0)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ss_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

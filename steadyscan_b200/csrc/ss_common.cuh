@@ -1,0 +1,176 @@
+// Shared types and device helpers of the B200 align_group_to_template engine.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ss {
+
+// Values the reference leaves in buffers it allocates (task_allocate.cu:226, :244).
+constexpr double kPnewFill = 1e6;
+constexpr double kErrvalFill = 1e6;
+// Bound on line-search trials per frame; the reference has none (task_linesearch.cu:95-149).
+constexpr int kTrialCap = 2048;
+
+// Evaluation modes of k_eval.
+enum EvalMode : int { kAssemble = 0, kTrial = 1, kCorr = 2, kFinal = 3 };
+
+// Group phases of the device-side control state machine.
+enum Phase : int { kPhHalf = 0, kPhIterEnd = 1, kPhFinal = 2, kPhDone = 3 };
+
+// StopCriterion (interface/stopcriterion.h:4-10).
+enum Stop : int { kStopCorrInc = 0, kStopHaltCorr = 1, kStopMovement = 2, kStopIterLimit = 3, kStopError = 4 };
+
+// Flag bits parsed from the gpu_flags string (mex/configuration.cpp:83-152).
+enum FlagBits : int {
+  kFlagMaskInactive = 1 << 0,   // M
+  kFlagIterCorr = 1 << 1,       // C
+  kFlagFrameCorr = 1 << 2,      // c
+  kFlagIterErrvals = 1 << 3,    // e
+  kFlagMedianBefore = 1 << 4,   // R
+  kFlagRawParams = 1 << 5,      // P
+  kFlagFrameOrdered = 1 << 6,   // p
+};
+
+// Per-column sums written by k_eval. Assembly uses all slots; other modes a prefix.
+enum ColSum : int {
+  kCsSsd = 0,
+  kCsAxx, kCsAyy, kCsAxy,   // sum g g' (1-f)^2            (diagonal, own knot)
+  kCsBxx, kCsByy, kCsBxy,   // sum g g' f'^2, f' of column (c+1) mod W (diagonal, next knot)
+  kCsOxx, kCsOyy, kCsOxy,   // sum g g' (f - f^2)          (coupling c, c+1)
+  kCsJ1x, kCsJ1y,           // sum d (1-f) g               (gradient, own knot)
+  kCsJ2x, kCsJ2y,           // sum d f g                   (gradient, next knot)
+  kCsAssemble = 14,
+  // correlation / final pass
+  kCsSumD = 0,              // sum over all pixels of the swapped difference image D'
+  kCsSetN, kCsSetD, kCsSetDD, kCsSetI, kCsSetII, kCsSetDI,  // leading-valid-run set
+  kCsFrD, kCsFrI, kCsFrDD, kCsFrII, kCsFrDI,                 // valid pixels (per-frame corr)
+  kCsFinalSsd,              // final pass: SSD at the mask knots
+  kCsCorr = 13,
+  kCsStride = 16,
+};
+
+struct GroupCtl {
+  int phase, iteration, shift, improved, exec_result;
+  int filter_active, filter_kind, filter_id, n_filter_iter;
+  int stop_reason, cap_hit, eig_size, n_used;
+  int pad0;
+  double correlation, corr;
+  long long n_eval;      // frame evaluations the reference would count: errval passes and trials
+  long long passes[4];   // frames read per evaluation kind (EvalMode)
+};
+
+struct GroupDesc {
+  // geometry (mexgateway.cpp:176-198)
+  int Hb, W, nF, fW, N, Ht, Wt;
+  int group_size, n_rg;
+  int tile_base;    // first k_eval tile of this group
+  int frame_base;   // first global frame index of this group
+  // settings
+  int max_iter, solver_id, max_filter_iter, filter_id, flags, frac_uniform;
+  double move_thresh, halt_corr, corr_inc_thr, filter_strength, filter_corr_thr, lambda, ls_mult;
+  // inputs on the device
+  const double* frac;       // Hb x W column-major
+  const double* basex;
+  const double* basey;
+  const uint8_t* base_mask;
+  const int* min_points;    // W
+  const void* image;        // Hb x fW column-major, engine frame type
+  const void* tquad;        // (Ht-1)(Wt-1) template quads, engine template type
+  const void* gquad;        // gradient quads or nullptr when derived from the template
+  const double* sum_image; // sum of the frame data over all Hb x fW entries
+  // state
+  double *p, *p_last, *p_snap, *delta_p, *ndp;
+  double* colsum;           // fW x kCsStride
+  int* colcnt;              // fW
+  uint8_t *params_used, *blocks_present, *grp_active;
+  double* errval;           // 2 nF
+  double *kmask, *kdiff;    // nF x 2 x (W+1)
+  uint8_t* fstate;          // nF: 2 while the frame's line search runs
+  int* ls_trials;           // nF
+  double* eig_c;            // N x 4
+  uint8_t* eig_valid;       // N
+  int* list;                // 2N: knot of each list position, then list position of each knot
+  double* cr;               // N x 13
+  // outputs on the device
+  double *o_frame_corr, *o_residrms, *o_iter_corr, *o_frame_corr_hist, *o_iter_errvals, *o_all_params;
+  double *o_dx, *o_dy, *o_frame_params, *o_raw;
+  uint8_t* o_mask;          // Hb x fW column-major, may be null
+};
+
+// ---------------------------------------------------------------------------------------------
+// element loads
+
+__device__ __forceinline__ double to_double(double v) { return v; }
+__device__ __forceinline__ double to_double(float v) { return (double)v; }
+__device__ __forceinline__ double to_double(uint16_t v) { return (double)v; }
+__device__ __forceinline__ double to_double(__half v) { return (double)__half2float(v); }
+__device__ __forceinline__ float to_float(double v) { return (float)v; }
+__device__ __forceinline__ float to_float(float v) { return v; }
+__device__ __forceinline__ float to_float(uint16_t v) { return (float)v; }
+__device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
+
+template <class T>
+struct Quad {
+  T v[4];
+};
+
+// Template quad (T[iy][ix], T[iy][ix+1], T[iy+1][ix], T[iy+1][ix+1]) as Acc values.
+template <class Acc, class TplT>
+__device__ __forceinline__ void load_quad(const void* base, size_t i, Acc& t00, Acc& t01, Acc& t10, Acc& t11);
+
+template <>
+__device__ __forceinline__ void load_quad<double, double>(const void* base, size_t i, double& a, double& b,
+                                                          double& c, double& d) {
+  const double2* q = reinterpret_cast<const double2*>(base) + 2 * i;
+  double2 lo = __ldg(q), hi = __ldg(q + 1);
+  a = lo.x; b = lo.y; c = hi.x; d = hi.y;
+}
+template <>
+__device__ __forceinline__ void load_quad<float, float>(const void* base, size_t i, float& a, float& b, float& c,
+                                                        float& d) {
+  float4 q = __ldg(reinterpret_cast<const float4*>(base) + i);
+  a = q.x; b = q.y; c = q.z; d = q.w;
+}
+template <>
+__device__ __forceinline__ void load_quad<float, __half>(const void* base, size_t i, float& a, float& b, float& c,
+                                                         float& d) {
+  uint2 raw = __ldg(reinterpret_cast<const uint2*>(base) + i);
+  __half2 lo = *reinterpret_cast<__half2*>(&raw.x), hi = *reinterpret_cast<__half2*>(&raw.y);
+  float2 l = __half22float2(lo), h = __half22float2(hi);
+  a = l.x; b = l.y; c = h.x; d = h.y;
+}
+
+// ---------------------------------------------------------------------------------------------
+// warp reductions
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 2x2 blocks: symmetric S = (s0 s2; s2 s1); general M = (m0 m1; m2 m3)
+
+struct M2 {
+  double a, b, c, d;  // (a b; c d)
+};
+__device__ __forceinline__ M2 m2_mul(const M2& x, const M2& y) {
+  return {x.a * y.a + x.b * y.c, x.a * y.b + x.b * y.d, x.c * y.a + x.d * y.c, x.c * y.b + x.d * y.d};
+}
+__device__ __forceinline__ M2 m2_inv(const M2& x) {
+  double det = x.a * x.d - x.b * x.c;
+  double r = 1.0 / det;
+  return {x.d * r, -x.b * r, -x.c * r, x.a * r};
+}
+__device__ __forceinline__ M2 m2_neg(const M2& x) { return {-x.a, -x.b, -x.c, -x.d}; }
+__device__ __forceinline__ M2 m2_sub(const M2& x, const M2& y) { return {x.a - y.a, x.b - y.b, x.c - y.c, x.d - y.d}; }
+
+}  // namespace ss

@@ -1,0 +1,842 @@
+// Host engine and C-ABI of the B200 align_group_to_template.
+//
+// A Batch owns the device state of one or more groups (each group is one align_group_to_template
+// call's worth of frames) and runs them to completion together: every kernel covers all groups,
+// and a device-side state machine per group (GroupCtl) decides what each group does next, so
+// groups of different sizes and convergence speeds share launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "ss_common.cuh"
+#include "ss_engine.h"
+#include "ss_eval.cuh"
+#include "ss_group.cuh"
+#include "steadyscan_b200.h"
+
+namespace ss {
+
+static thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+const char* last_error() { return g_err.c_str(); }
+
+#define SS_CK(call)                                                                          \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      int code_ = (e_ == cudaErrorMemoryAllocation) ? SS_ERR_OUT_OF_MEMORY : SS_ERR_CUDA;    \
+      return fail(code_, std::string(#call) + ": " + cudaGetErrorString(e_));                \
+    }                                                                                        \
+  } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// set-up kernels
+
+// Template quads from a column-major FP64 template (mexgateway.cpp:46 reads it column-major and
+// the reference indexes it row-major, task_differenceimage.cuh:120).
+template <class TplT>
+__global__ void k_build_tquad(const double* __restrict__ T, int Ht, int Wt, TplT* __restrict__ q) {
+  const size_t n = (size_t)(Ht - 1) * (Wt - 1);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    int iy = (int)(i / (Wt - 1)), ix = (int)(i % (Wt - 1));
+    q[4 * i + 0] = (TplT)T[(size_t)ix * Ht + iy];
+    q[4 * i + 1] = (TplT)T[(size_t)(ix + 1) * Ht + iy];
+    q[4 * i + 2] = (TplT)T[(size_t)ix * Ht + iy + 1];
+    q[4 * i + 3] = (TplT)T[(size_t)(ix + 1) * Ht + iy + 1];
+  }
+}
+
+// Gradient quads (xg[iy][ix], xg[iy+1][ix], yg[iy][ix], yg[iy][ix+1]) for caller gradients that
+// are not the template's forward differences.
+template <class TplT>
+__global__ void k_build_gquad(const double* __restrict__ xg, const double* __restrict__ yg, int Ht, int Wt,
+                              TplT* __restrict__ q) {
+  const size_t n = (size_t)(Ht - 1) * (Wt - 1);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    int iy = (int)(i / (Wt - 1)), ix = (int)(i % (Wt - 1));
+    q[4 * i + 0] = (TplT)xg[(size_t)ix * Ht + iy];
+    q[4 * i + 1] = (TplT)xg[(size_t)ix * Ht + iy + 1];
+    q[4 * i + 2] = (TplT)yg[(size_t)ix * Ht + iy];
+    q[4 * i + 3] = (TplT)yg[(size_t)(ix + 1) * Ht + iy];
+  }
+}
+
+template <class FrameT>
+__global__ void __launch_bounds__(1024) k_sum_image(const void* __restrict__ img, size_t n, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0;
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += to_double(ld_frame<FrameT>(img, i));
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) *out = v;
+  }
+}
+
+__global__ void k_fill(double* p, size_t n, double v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+// ---------------------------------------------------------------------------------------------
+// kernel dispatch by (compute, frame type, template type)
+
+using EvalFn = void (*)(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, const GroupCtl* ctl);
+using SumFn = void (*)(const void* img, size_t n, double* out, cudaStream_t s);
+
+template <class Acc, class FrameT, class TplT>
+static void eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, const GroupCtl* ctl) {
+  if (tiles <= 0) return;
+  switch (mode) {
+    case kAssemble: k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
+    case kTrial: k_eval<Acc, FrameT, TplT, kTrial><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
+    case kCorr: k_eval<Acc, FrameT, TplT, kCorr><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
+    default: k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
+  }
+}
+template <class FrameT>
+static void sum_launch(const void* img, size_t n, double* out, cudaStream_t s) {
+  k_sum_image<FrameT><<<1, 1024, 0, s>>>(img, n, out);
+}
+
+static EvalFn pick_eval(int compute, int fdt, int tdt) {
+  if (compute == 0) {
+    switch (fdt) {
+      case SS_F64: return eval_launch<double, double, double>;
+      case SS_F32: return eval_launch<double, float, double>;
+      case SS_U16: return eval_launch<double, uint16_t, double>;
+      case SS_F16: return eval_launch<double, __half, double>;
+    }
+  } else if (tdt == SS_F16) {
+    switch (fdt) {
+      case SS_F64: return eval_launch<float, double, __half>;
+      case SS_F32: return eval_launch<float, float, __half>;
+      case SS_U16: return eval_launch<float, uint16_t, __half>;
+      case SS_F16: return eval_launch<float, __half, __half>;
+    }
+  } else {
+    switch (fdt) {
+      case SS_F64: return eval_launch<float, double, float>;
+      case SS_F32: return eval_launch<float, float, float>;
+      case SS_U16: return eval_launch<float, uint16_t, float>;
+      case SS_F16: return eval_launch<float, __half, float>;
+    }
+  }
+  return nullptr;
+}
+static SumFn pick_sum(int fdt) {
+  switch (fdt) {
+    case SS_F64: return sum_launch<double>;
+    case SS_F32: return sum_launch<float>;
+    case SS_U16: return sum_launch<uint16_t>;
+    case SS_F16: return sum_launch<__half>;
+  }
+  return nullptr;
+}
+
+static size_t dtype_size(int dt) {
+  switch (dt) {
+    case SS_F64: return 8;
+    case SS_F32: return 4;
+    case SS_U16: return 2;
+    case SS_F16: return 2;
+    case SS_U8: return 1;
+    case SS_I32: return 4;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// host-side conversion of small inputs
+
+static double elem_as_double(const ss_matrix& m, size_t i) {
+  const char* b = static_cast<const char*>(m.data);
+  switch (m.dtype) {
+    case SS_F64: return reinterpret_cast<const double*>(b)[i];
+    case SS_F32: return reinterpret_cast<const float*>(b)[i];
+    case SS_U16: return reinterpret_cast<const uint16_t*>(b)[i];
+    case SS_U8: return reinterpret_cast<const uint8_t*>(b)[i];
+    case SS_I32: return reinterpret_cast<const int32_t*>(b)[i];
+    case SS_F16: {
+      uint16_t h = reinterpret_cast<const uint16_t*>(b)[i];
+      int e = (h >> 10) & 31, mnt = h & 1023;
+      double v = e == 0 ? std::ldexp((double)mnt, -24) : (e == 31 ? (mnt ? NAN : INFINITY)
+                                                                : std::ldexp((double)(mnt | 1024), e - 25));
+      return (h & 0x8000) ? -v : v;
+    }
+  }
+  return NAN;
+}
+
+static int host_doubles(const ss_matrix& m, const char* name, std::vector<double>& out) {
+  if (m.location != SS_HOST) return fail(SS_ERR_INVALID_ARGUMENT, std::string(name) + " must be host memory");
+  if (!m.data && m.rows * m.cols > 0) return fail(SS_ERR_INVALID_ARGUMENT, std::string(name) + " is NULL");
+  if (dtype_size(m.dtype) == 0) return fail(SS_ERR_INVALID_ARGUMENT, std::string(name) + ": unknown dtype");
+  size_t n = (size_t)(m.rows * m.cols);
+  out.resize(n);
+  for (size_t i = 0; i < n; i++) out[i] = elem_as_double(m, i);
+  return SS_OK;
+}
+
+static int parse_flags(const char* flags, int& compute, int& bits) {
+  if (!flags) return fail(SS_ERR_INVALID_ARGUMENT, "flags is NULL");
+  compute = -1;
+  bits = 0;
+  for (const char* c = flags; *c; c++) {
+    switch (*c) {
+      case 'D': compute = 0; break;
+      case 'S': compute = 1; break;
+      case 'M': bits |= kFlagMaskInactive; break;
+      case 'C': bits |= kFlagIterCorr; break;
+      case 'c': bits |= kFlagFrameCorr; break;
+      case 'e': bits |= kFlagIterErrvals; break;
+      case 'R': bits |= kFlagMedianBefore; break;
+      case 'P': bits |= kFlagRawParams; break;
+      case 'p': bits |= kFlagFrameOrdered; break;
+      default: break;  // T t I F W w G E r f V: timing, printing and debug switches
+    }
+  }
+  if (compute < 0)
+    return fail(SS_ERR_INVALID_ARGUMENT, "invalid precision type! use 'S' for single-precision and 'D' for double-precision");
+  return SS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batch
+
+struct HostGroup {
+  const ss_inputs* in = nullptr;
+  int compute = 0, flags = 0;
+  int Hb = 0, W = 0, nF = 0, fW = 0, N = 0, Ht = 0, Wt = 0, group_size = 0, n_rg = 0;
+  int frame_dt = SS_F64, tpl_dt = SS_F64;
+  bool grad_derived = true, frac_uniform = true;
+  std::vector<double> p0, templ, xg, yg, frac, bx, by;
+  std::vector<uint8_t> bmask;
+  std::vector<int32_t> minp;
+  const void* frames_dev = nullptr;  // caller device pointer when bm_data is on the device
+  size_t frame_bytes = 0;
+  // device pointers
+  double* d_templ_stage = nullptr;
+  double* d_xg_stage = nullptr;
+  double* d_yg_stage = nullptr;
+  double* d_sum = nullptr;
+  double* d_p0 = nullptr;
+  void* d_image = nullptr;
+};
+
+static int validate_group(const ss_inputs* in, HostGroup& g) {
+  if (!in) return fail(SS_ERR_INVALID_ARGUMENT, "inputs is NULL");
+  int rc = parse_flags(in->flags, g.compute, g.flags);
+  if (rc) return rc;
+  g.in = in;
+  g.Ht = (int)in->template_image.rows;
+  g.Wt = (int)in->template_image.cols;
+  if (g.Ht < 2 || g.Wt < 2) return fail(SS_ERR_INVALID_ARGUMENT, "template_image must be at least 2 x 2");
+  if (in->xgrad.rows != g.Ht || in->xgrad.cols != g.Wt || in->ygrad.rows != g.Ht || in->ygrad.cols != g.Wt)
+    return fail(SS_ERR_INVALID_ARGUMENT, "xgrad and ygrad must match template_image");
+  g.Hb = (int)in->basex.rows;  // frameH, frameW from basex (mexgateway.cpp:176-177)
+  g.W = (int)in->basex.cols;
+  if (g.Hb < 1 || g.W < 1) return fail(SS_ERR_INVALID_ARGUMENT, "basex is empty");
+  const ss_matrix* geo[3] = {&in->tfrac, &in->basey, &in->base_mask};
+  const char* geon[3] = {"tfrac", "basey", "base_mask"};
+  for (int i = 0; i < 3; i++)
+    if (geo[i]->rows != g.Hb || geo[i]->cols != g.W)
+      return fail(SS_ERR_INVALID_ARGUMENT, std::string(geon[i]) + " must match basex");
+  g.nF = in->n_frames;
+  if (g.nF < 1) return fail(SS_ERR_INVALID_ARGUMENT, "n_frames must be positive");
+  g.fW = g.W * g.nF;
+  g.N = g.fW + 1;
+  if ((long long)g.Hb * g.fW > (1LL << 31) - 1) return fail(SS_ERR_INVALID_ARGUMENT, "too many pixels in one group");
+  if (in->bm_data.rows != g.Hb || in->bm_data.cols != g.fW)
+    return fail(SS_ERR_INVALID_ARGUMENT, "bm_data must be frameH x (frameW * n_frames)");
+  g.frame_dt = in->bm_data.dtype;
+  if (!(g.frame_dt == SS_F64 || g.frame_dt == SS_F32 || g.frame_dt == SS_U16 || g.frame_dt == SS_F16))
+    return fail(SS_ERR_INVALID_ARGUMENT, "bm_data dtype must be f64, f32, u16 or f16");
+  if (!in->bm_data.data) return fail(SS_ERR_INVALID_ARGUMENT, "bm_data is NULL");
+  if (in->est_dx_knots.rows * in->est_dx_knots.cols != (int64_t)(g.W + 1) * g.nF ||
+      in->est_dy_knots.rows * in->est_dy_knots.cols != (int64_t)(g.W + 1) * g.nF)
+    return fail(SS_ERR_INVALID_ARGUMENT, "est_dx_knots and est_dy_knots must hold (frameW + 1) x n_frames values");
+  if (in->min_points_per_block.rows * in->min_points_per_block.cols < g.W)
+    return fail(SS_ERR_INVALID_ARGUMENT, "min_points_per_block needs at least frameW entries");
+  g.group_size = in->group_size;
+  if (g.group_size <= 0 || g.group_size % g.W != 0)
+    return fail(SS_ERR_INVALID_ARGUMENT, "group_size must be a positive multiple of frameW");
+  g.n_rg = g.fW / g.group_size;
+  if (in->max_iter < 1) return fail(SS_ERR_INVALID_ARGUMENT, "max_iter must be positive");
+  if (in->solver_id < 0 || in->solver_id > 2)
+    return fail(SS_ERR_INVALID_ARGUMENT, "invalid solver id\n0:CuSparse solver\n1:CuSolver solver\n2:Eigen solver");
+  int fsel = in->filter_id & (0 - (in->max_filter_iterations != 0));  // task.cpp:54
+  if (fsel < 0 || fsel > 2)
+    return fail(SS_ERR_INVALID_ARGUMENT, "invalid filter ID\n0: disable filter\n1: smearingfiter\n2:rangefilter");
+  if (!(in->linesearch_reduction_multiplier > 0.0 && in->linesearch_reduction_multiplier < 1.0))
+    return fail(SS_ERR_INVALID_ARGUMENT, "linesearch_reduction_multiplier must be in (0, 1)");
+  g.tpl_dt = g.compute == 0 ? SS_F64 : (in->template_storage == SS_F16 ? SS_F16 : SS_F32);
+  return SS_OK;
+}
+
+static int load_host_inputs(HostGroup& g) {
+  const ss_inputs* in = g.in;
+  int rc;
+  if ((rc = host_doubles(in->template_image, "template_image", g.templ))) return rc;
+  if ((rc = host_doubles(in->xgrad, "xgrad", g.xg))) return rc;
+  if ((rc = host_doubles(in->ygrad, "ygrad", g.yg))) return rc;
+  if ((rc = host_doubles(in->tfrac, "tfrac", g.frac))) return rc;
+  if ((rc = host_doubles(in->basex, "basex", g.bx))) return rc;
+  if ((rc = host_doubles(in->basey, "basey", g.by))) return rc;
+  std::vector<double> tmp;
+  if ((rc = host_doubles(in->base_mask, "base_mask", tmp))) return rc;
+  g.bmask.resize(tmp.size());
+  for (size_t i = 0; i < tmp.size(); i++) g.bmask[i] = tmp[i] != 0.0;
+  if ((rc = host_doubles(in->min_points_per_block, "min_points_per_block", tmp))) return rc;
+  g.minp.resize(g.W);
+  for (int i = 0; i < g.W; i++) g.minp[i] = (int32_t)tmp[i];  // static_cast<int> (mexconverter.cpp:97)
+  std::vector<double> ex, ey;
+  if ((rc = host_doubles(in->est_dx_knots, "est_dx_knots", ex))) return rc;
+  if ((rc = host_doubles(in->est_dy_knots, "est_dy_knots", ey))) return rc;
+  // ParameterOrganizer::organize2D1 (parameterorganizer.cpp:31-55)
+  g.p0.assign(2 * (size_t)g.N, 0.0);
+  for (int f = 0; f < g.nF; f++) {
+    int j = f * g.W + (f != 0);
+    for (int i = (f != 0); i < g.W; i++, j++) {
+      g.p0[j] = ex[(size_t)f * (g.W + 1) + i];
+      g.p0[j + g.N] = ey[(size_t)f * (g.W + 1) + i];
+    }
+    if (f < g.nF - 1) {
+      g.p0[j] = (ex[(size_t)f * (g.W + 1) + g.W] + ex[(size_t)(f + 1) * (g.W + 1)]) / 2;
+      g.p0[j + g.N] = (ey[(size_t)f * (g.W + 1) + g.W] + ey[(size_t)(f + 1) * (g.W + 1)]) / 2;
+    } else {
+      g.p0[j] = ex[(size_t)f * (g.W + 1) + g.W];
+      g.p0[j + g.N] = ey[(size_t)f * (g.W + 1) + g.W];
+    }
+  }
+  // gradients that are exactly the template's forward differences are re-derived on the device
+  g.grad_derived = true;
+  for (int c = 0; c + 1 < g.Wt && g.grad_derived; c++)
+    for (int r = 0; r < g.Ht; r++) {
+      double d = g.templ[(size_t)(c + 1) * g.Ht + r] - g.templ[(size_t)c * g.Ht + r];
+      if (!(g.xg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
+    }
+  for (int c = 0; c < g.Wt && g.grad_derived; c++)
+    for (int r = 0; r + 1 < g.Ht; r++) {
+      double d = g.templ[(size_t)c * g.Ht + r + 1] - g.templ[(size_t)c * g.Ht + r];
+      if (!(g.yg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
+    }
+  g.frac_uniform = true;
+  for (int c = 1; c < g.W && g.frac_uniform; c++)
+    for (int r = 0; r < g.Hb; r++)
+      if (std::memcmp(&g.frac[(size_t)c * g.Hb + r], &g.frac[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
+  g.frame_bytes = (size_t)g.Hb * g.fW * dtype_size(g.frame_dt);
+  if (in->bm_data.location == SS_DEVICE) g.frames_dev = in->bm_data.data;
+  return SS_OK;
+}
+
+// Arena carving: every sub-buffer 256-byte aligned.
+struct Carve {
+  size_t off = 0;
+  char* base = nullptr;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+struct Batch::Impl {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int compute = 0, frame_dt = SS_F64, tpl_dt = SS_F64;
+  std::vector<HostGroup> hg;
+  std::vector<GroupDesc> gd;
+  std::vector<ss_outputs*> outs;
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  bool external_arena = false;
+  GroupDesc* d_gd = nullptr;
+  GroupCtl* d_ctl = nullptr;
+  int* d_tile_group = nullptr;
+  int* d_frame_group = nullptr;
+  int* d_counters = nullptr;  // [0] searching frames, [1] finished groups
+  int* h_counters = nullptr;  // pinned
+  int n_tiles = 0, n_frames_total = 0;
+  EvalFn eval = nullptr;
+  SumFn sum = nullptr;
+  std::vector<GroupCtl> h_ctl;
+  double init_ms = 0, run_ms = 0;
+  int cycles = 0, rounds = 0, launches = 0;
+  // optional CUDA-event timing of the evaluation kernels, per EvalMode
+  bool timing = false;
+  std::vector<cudaEvent_t> events;
+  std::vector<int> event_mode;
+  size_t event_used = 0;
+  double eval_ms[4] = {0, 0, 0, 0};
+
+  void eval_timed(int mode) {
+    if (timing) {
+      if (event_used + 2 > events.size()) {
+        for (int k = 0; k < 64; k++) {
+          cudaEvent_t e;
+          cudaEventCreate(&e);
+          events.push_back(e);
+          event_mode.push_back(0);
+        }
+      }
+      cudaEventRecord(events[event_used], stream);
+    }
+    eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl);
+    launches++;
+    if (timing) {
+      cudaEventRecord(events[event_used + 1], stream);
+      event_mode[event_used] = mode;
+      event_used += 2;
+    }
+  }
+};
+
+Batch::Batch() : d(new Impl) {}
+Batch::~Batch() {
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  for (cudaEvent_t e : d->events) cudaEventDestroy(e);
+  if (d->arena && !d->external_arena) cudaFree(d->arena);
+  if (d->h_counters) cudaFreeHost(d->h_counters);
+  if (d->stream) cudaStreamDestroy(d->stream);
+  delete d;
+}
+
+size_t Batch::arena_bytes() const { return d->arena_bytes; }
+
+// Lays out all device buffers of the batch; with base == nullptr only measures.
+static void layout(Batch::Impl* b, char* base) {
+  Carve cv;
+  cv.base = base;
+  const size_t tsz = dtype_size(b->tpl_dt);
+  b->n_tiles = 0;
+  b->n_frames_total = 0;
+  std::vector<GroupDesc>& gd = b->gd;
+  gd.assign(b->hg.size(), GroupDesc{});
+  for (size_t i = 0; i < b->hg.size(); i++) {
+    HostGroup& g = b->hg[i];
+    GroupDesc& G = gd[i];
+    G.Hb = g.Hb; G.W = g.W; G.nF = g.nF; G.fW = g.fW; G.N = g.N; G.Ht = g.Ht; G.Wt = g.Wt;
+    G.group_size = g.group_size; G.n_rg = g.n_rg;
+    G.tile_base = b->n_tiles;
+    b->n_tiles += (g.fW + 7) / 8;
+    G.frame_base = b->n_frames_total;
+    b->n_frames_total += g.nF;
+    const ss_inputs* in = g.in;
+    G.max_iter = in->max_iter; G.solver_id = in->solver_id; G.max_filter_iter = in->max_filter_iterations;
+    G.filter_id = in->filter_id; G.flags = g.flags; G.frac_uniform = g.frac_uniform ? 1 : 0;
+    G.move_thresh = in->move_thresh; G.halt_corr = in->halt_correlation;
+    G.corr_inc_thr = in->correlation_increase_threshold; G.filter_strength = in->filter_strength;
+    G.filter_corr_thr = in->filter_deactivation_threshold; G.lambda = in->lambda;
+    G.ls_mult = in->linesearch_reduction_multiplier;
+    const size_t hbw = (size_t)g.Hb * g.W, npx = (size_t)g.Hb * g.fW, N = g.N, nF = g.nF;
+    const size_t nq = (size_t)(g.Ht - 1) * (g.Wt - 1);
+    G.frac = cv.take<double>(hbw);
+    G.basex = cv.take<double>(hbw);
+    G.basey = cv.take<double>(hbw);
+    G.base_mask = cv.take<uint8_t>(hbw);
+    G.min_points = cv.take<int>(g.W);
+    g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
+    G.image = g.frames_dev ? g.frames_dev : g.d_image;
+    G.tquad = cv.take<char>(nq * 4 * tsz);
+    G.gquad = g.grad_derived ? nullptr : cv.take<char>(nq * 4 * tsz);
+    g.d_templ_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+    if (!g.grad_derived) {
+      g.d_xg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+      g.d_yg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+    }
+    g.d_sum = cv.take<double>(1);
+    G.sum_image = g.d_sum;
+    g.d_p0 = cv.take<double>(2 * N);
+    G.p = cv.take<double>(2 * N);
+    G.p_last = cv.take<double>(2 * N);
+    G.p_snap = cv.take<double>(2 * N);
+    G.delta_p = cv.take<double>(2 * N);
+    G.ndp = cv.take<double>(2 * N);
+    G.colsum = cv.take<double>((size_t)g.fW * kCsStride);
+    G.colcnt = cv.take<int>(g.fW);
+    G.params_used = cv.take<uint8_t>(N);
+    G.blocks_present = cv.take<uint8_t>(N);
+    G.grp_active = cv.take<uint8_t>(2 * (size_t)g.n_rg + 1);
+    G.errval = cv.take<double>(2 * nF);
+    G.kmask = cv.take<double>(nF * 2 * (g.W + 1));
+    G.kdiff = cv.take<double>(nF * 2 * (g.W + 1));
+    G.fstate = cv.take<uint8_t>(nF);
+    G.ls_trials = cv.take<int>(nF);
+    G.eig_c = cv.take<double>(4 * N);
+    G.eig_valid = cv.take<uint8_t>(N);
+    G.list = cv.take<int>(2 * N);
+    G.cr = cv.take<double>(kCrStride * N);
+    const ss_outputs* o = b->outs[i];
+    const int mi = in->max_iter;
+    G.o_frame_corr = cv.take<double>(nF);
+    G.o_residrms = cv.take<double>(nF);
+    G.o_dx = cv.take<double>((g.W + 1) * nF);
+    G.o_dy = cv.take<double>((g.W + 1) * nF);
+    G.o_iter_corr = (o && o->iteration_corr) ? cv.take<double>(mi) : nullptr;
+    G.o_frame_corr_hist = (o && o->frame_corr_history) ? cv.take<double>((size_t)mi * nF) : nullptr;
+    G.o_iter_errvals = (o && o->iteration_errvals) ? cv.take<double>((size_t)2 * mi * nF) : nullptr;
+    G.o_all_params = (o && o->all_params) ? cv.take<double>((size_t)2 * N * mi) : nullptr;
+    G.o_frame_params = (o && o->frame_params) ? cv.take<double>(2 * (size_t)(g.W + 1) * nF) : nullptr;
+    G.o_raw = (o && o->raw_params) ? cv.take<double>(2 * N) : nullptr;
+    G.o_mask = (o && o->mask) ? cv.take<uint8_t>(npx) : nullptr;
+  }
+  b->d_gd = cv.take<GroupDesc>(gd.size());
+  b->d_ctl = cv.take<GroupCtl>(gd.size());
+  b->d_tile_group = cv.take<int>(std::max(1, b->n_tiles));
+  b->d_frame_group = cv.take<int>(std::max(1, b->n_frames_total));
+  b->d_counters = cv.take<int>(4);
+  b->arena_bytes = cv.off + 256;
+}
+
+int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes) {
+  Impl* b = d;
+  if (n < 1) return fail(SS_ERR_INVALID_ARGUMENT, "no groups");
+  b->hg.assign(n, HostGroup{});
+  b->outs.assign(n, nullptr);
+  for (int i = 0; i < n; i++) {
+    int rc = validate_group(&in[i], b->hg[i]);
+    if (rc) return rc;
+    b->outs[i] = out ? &out[i] : nullptr;
+    if (i > 0) {
+      const HostGroup& a = b->hg[0];
+      const HostGroup& c = b->hg[i];
+      if (c.compute != a.compute || c.frame_dt != a.frame_dt || c.tpl_dt != a.tpl_dt ||
+          in[i].gpu_device_id != in[0].gpu_device_id)
+        return fail(SS_ERR_INVALID_ARGUMENT, "all groups of a batch need the same precision, frame dtype and device");
+    }
+    rc = load_host_inputs(b->hg[i]);
+    if (rc) return rc;
+  }
+  b->compute = b->hg[0].compute;
+  b->frame_dt = b->hg[0].frame_dt;
+  b->tpl_dt = b->hg[0].tpl_dt;
+  b->eval = pick_eval(b->compute, b->frame_dt, b->tpl_dt);
+  b->sum = pick_sum(b->frame_dt);
+  if (!b->eval || !b->sum) return fail(SS_ERR_INVALID_ARGUMENT, "unsupported dtype combination");
+
+  auto t0 = std::chrono::steady_clock::now();
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
+  b->device = in[0].gpu_device_id;
+  if (b->device < 0 || b->device >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
+  SS_CK(cudaSetDevice(b->device));
+  SS_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  SS_CK(cudaHostAlloc(&b->h_counters, 4 * sizeof(int), cudaHostAllocDefault));
+  layout(b, nullptr);
+  if (external) {
+    if (external_bytes < b->arena_bytes) return fail(SS_ERR_OUT_OF_MEMORY, "external arena too small");
+    b->arena = external;
+    b->external_arena = true;
+  } else {
+    SS_CK(cudaMalloc(&b->arena, b->arena_bytes));
+  }
+  char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(b->arena) + 255) & ~uintptr_t(255));
+  layout(b, base);
+  b->init_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+
+  // uploads
+  cudaStream_t s = b->stream;
+  std::vector<int> tile_group(std::max(1, b->n_tiles)), frame_group(std::max(1, b->n_frames_total));
+  for (size_t i = 0; i < b->hg.size(); i++) {
+    HostGroup& g = b->hg[i];
+    GroupDesc& G = b->gd[i];
+    const size_t hbw = (size_t)g.Hb * g.W;
+    SS_CK(cudaMemcpyAsync((void*)G.frac, g.frac.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync((void*)G.basex, g.bx.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync((void*)G.basey, g.by.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync((void*)G.base_mask, g.bmask.data(), hbw, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync((void*)G.min_points, g.minp.data(), g.W * 4, cudaMemcpyHostToDevice, s));
+    if (!g.frames_dev)
+      SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync(g.d_templ_stage, g.templ.data(), g.templ.size() * 8, cudaMemcpyHostToDevice, s));
+    if (!g.grad_derived) {
+      SS_CK(cudaMemcpyAsync(g.d_xg_stage, g.xg.data(), g.xg.size() * 8, cudaMemcpyHostToDevice, s));
+      SS_CK(cudaMemcpyAsync(g.d_yg_stage, g.yg.data(), g.yg.size() * 8, cudaMemcpyHostToDevice, s));
+    }
+    SS_CK(cudaMemcpyAsync(g.d_p0, g.p0.data(), g.p0.size() * 8, cudaMemcpyHostToDevice, s));
+    const int nb = 148 * 4;
+    if (b->tpl_dt == SS_F64) {
+      k_build_tquad<double><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (double*)G.tquad);
+      if (!g.grad_derived)
+        k_build_gquad<double><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (double*)G.gquad);
+    } else if (b->tpl_dt == SS_F32) {
+      k_build_tquad<float><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (float*)G.tquad);
+      if (!g.grad_derived)
+        k_build_gquad<float><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (float*)G.gquad);
+    } else {
+      k_build_tquad<__half><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (__half*)G.tquad);
+      if (!g.grad_derived)
+        k_build_gquad<__half><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (__half*)G.gquad);
+    }
+    SS_CK(cudaGetLastError());
+    b->sum(G.image, (size_t)g.Hb * g.fW, g.d_sum, s);
+    SS_CK(cudaGetLastError());
+    for (int t = 0; t < (g.fW + 7) / 8; t++) tile_group[G.tile_base + t] = (int)i;
+    for (int f = 0; f < g.nF; f++) frame_group[G.frame_base + f] = (int)i;
+  }
+  SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(b->d_tile_group, tile_group.data(), tile_group.size() * 4, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(b->d_frame_group, frame_group.data(), frame_group.size() * 4, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaStreamSynchronize(s));
+  return SS_OK;
+}
+
+// Resets the iteration state of every group to the call's start (task_allocate.cu:201-255).
+static int reset_state(Batch::Impl* b) {
+  cudaStream_t s = b->stream;
+  b->h_ctl.assign(b->gd.size(), GroupCtl{});
+  for (size_t i = 0; i < b->gd.size(); i++) {
+    const HostGroup& g = b->hg[i];
+    const GroupDesc& G = b->gd[i];
+    const size_t N = g.N, nF = g.nF;
+    SS_CK(cudaMemcpyAsync(G.p, g.d_p0, 2 * N * 8, cudaMemcpyDeviceToDevice, s));
+    SS_CK(cudaMemsetAsync(G.p_last, 0, 2 * N * 8, s));
+    SS_CK(cudaMemsetAsync(G.delta_p, 0, 2 * N * 8, s));
+    SS_CK(cudaMemsetAsync(G.params_used, 0, N, s));
+    SS_CK(cudaMemsetAsync(G.blocks_present, 0, N, s));
+    SS_CK(cudaMemsetAsync(G.grp_active, 1, 2 * (size_t)g.n_rg, s));
+    SS_CK(cudaMemsetAsync(G.grp_active + 2 * (size_t)g.n_rg, 0, 1, s));
+    SS_CK(cudaMemsetAsync(G.o_frame_corr, 0, nF * 8, s));
+    SS_CK(cudaMemsetAsync(G.eig_valid, 0, N, s));
+    k_fill<<<64, 256, 0, s>>>(G.errval, 2 * nF, kErrvalFill);
+    // the reference's x/y/mask/difference buffers start zero-filled: NaN knots give an all-invalid
+    // mask and a zero difference image
+    k_fill<<<64, 256, 0, s>>>(G.kmask, nF * 2 * (g.W + 1), NAN);
+    k_fill<<<64, 256, 0, s>>>(G.kdiff, nF * 2 * (g.W + 1), NAN);
+    SS_CK(cudaGetLastError());
+    GroupCtl& C = b->h_ctl[i];
+    std::memset(&C, 0, sizeof(C));
+    C.phase = kPhHalf;
+    C.iteration = 1;
+    C.improved = 1;
+    C.stop_reason = kStopError;
+    C.eig_size = -1;
+    const ss_inputs* in = g.in;
+    C.filter_id = in->filter_id;
+    C.n_filter_iter = in->max_filter_iterations;
+    int fsel = in->filter_id & (0 - (in->max_filter_iterations != 0));  // task.cpp:54-70
+    if (fsel == 0) {
+      C.filter_active = 0;
+      C.n_filter_iter = 0;
+    } else {
+      C.filter_active = 1;
+      C.filter_kind = fsel;
+    }
+  }
+  SS_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl.data(), b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(int), s));
+  return SS_OK;
+}
+
+static int run_cycles(Batch::Impl* b) {
+  cudaStream_t s = b->stream;
+  const int nG = (int)b->gd.size();
+  int max_iter = 1;
+  for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
+  const int max_cycles = 4 * (max_iter + 2) + 16;
+  for (int cycle = 0; cycle < max_cycles; cycle++) {
+    b->cycles++;
+    b->eval_timed(kAssemble);
+    k_solve<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+    b->launches++;
+    SS_CK(cudaGetLastError());
+    for (int round = 0; round < kTrialCap + 1; round++) {
+      b->rounds++;
+      b->eval_timed(kTrial);
+      SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
+      k_ls_decide<<<(b->n_frames_total + 7) / 8, 256, 0, s>>>(b->d_gd, b->d_frame_group, b->n_frames_total, b->d_ctl,
+                                                             b->d_counters);
+      b->launches++;
+      SS_CK(cudaGetLastError());
+      SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, sizeof(int), cudaMemcpyDeviceToHost, s));
+      SS_CK(cudaStreamSynchronize(s));
+      if (b->h_counters[0] == 0) break;
+    }
+    k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+    b->eval_timed(kCorr);
+    k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+    b->eval_timed(kFinal);
+    k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
+    b->launches += 3;
+    SS_CK(cudaGetLastError());
+    SS_CK(cudaMemcpyAsync(b->h_counters + 1, b->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SS_CK(cudaStreamSynchronize(s));
+    if (b->h_counters[1] >= nG) return SS_OK;
+  }
+  return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
+}
+
+int Batch::run() {
+  Impl* b = d;
+  auto t0 = std::chrono::steady_clock::now();
+  SS_CK(cudaSetDevice(b->device));
+  int rc = reset_state(b);
+  if (rc) return rc;
+  b->cycles = 0;
+  b->rounds = 0;
+  b->launches = 0;
+  b->event_used = 0;
+  rc = run_cycles(b);
+  if (rc) return rc;
+  for (int m = 0; m < 4; m++) b->eval_ms[m] = 0;
+  for (size_t k = 0; k < b->event_used; k += 2) {
+    float ms = 0;
+    SS_CK(cudaEventElapsedTime(&ms, b->events[k], b->events[k + 1]));
+    b->eval_ms[b->event_mode[k]] += ms;
+  }
+  b->run_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return SS_OK;
+}
+
+void Batch::set_timing(bool on) { d->timing = on; }
+
+void Batch::stats(ss_batch_stats* st) const {
+  std::memset(st, 0, sizeof(*st));
+  st->n_groups = (int32_t)d->gd.size();
+  st->cycles = d->cycles;
+  st->linesearch_rounds = d->rounds;
+  st->kernel_launches = d->launches;
+  for (const GroupCtl& C : d->h_ctl)
+    for (int m = 0; m < 4; m++) st->frame_passes[m] += C.passes[m];
+  for (int m = 0; m < 4; m++) st->eval_ms[m] = d->eval_ms[m];
+  st->arena_bytes = (int64_t)d->arena_bytes;
+  st->run_ms = d->run_ms;
+}
+
+int Batch::collect() {
+  Impl* b = d;
+  cudaStream_t s = b->stream;
+  SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost, s));
+  for (size_t i = 0; i < b->gd.size(); i++) {
+    ss_outputs* o = b->outs[i];
+    if (!o) continue;
+    const HostGroup& g = b->hg[i];
+    const GroupDesc& G = b->gd[i];
+    const size_t nF = g.nF, nk = (size_t)(g.W + 1) * nF;
+    const bool frame_ordered = g.flags & kFlagFrameOrdered;
+    if (o->dx_knots && !frame_ordered) SS_CK(cudaMemcpyAsync(o->dx_knots, G.o_dx, nk * 8, cudaMemcpyDeviceToHost, s));
+    if (o->dy_knots && !frame_ordered) SS_CK(cudaMemcpyAsync(o->dy_knots, G.o_dy, nk * 8, cudaMemcpyDeviceToHost, s));
+    if (o->frame_corr) SS_CK(cudaMemcpyAsync(o->frame_corr, G.o_frame_corr, nF * 8, cudaMemcpyDeviceToHost, s));
+    if (o->residrms) SS_CK(cudaMemcpyAsync(o->residrms, G.o_residrms, nF * 8, cudaMemcpyDeviceToHost, s));
+    if (o->mask) SS_CK(cudaMemcpyAsync(o->mask, G.o_mask, (size_t)g.Hb * g.fW, cudaMemcpyDeviceToHost, s));
+    const size_t mi = g.in->max_iter;
+    if (o->iteration_corr) SS_CK(cudaMemcpyAsync(o->iteration_corr, G.o_iter_corr, mi * 8, cudaMemcpyDeviceToHost, s));
+    if (o->frame_corr_history)
+      SS_CK(cudaMemcpyAsync(o->frame_corr_history, G.o_frame_corr_hist, mi * nF * 8, cudaMemcpyDeviceToHost, s));
+    if (o->iteration_errvals)
+      SS_CK(cudaMemcpyAsync(o->iteration_errvals, G.o_iter_errvals, 2 * mi * nF * 8, cudaMemcpyDeviceToHost, s));
+    if (o->all_params) SS_CK(cudaMemcpyAsync(o->all_params, G.o_all_params, 2 * (size_t)g.N * mi * 8, cudaMemcpyDeviceToHost, s));
+    if (o->frame_params && frame_ordered)
+      SS_CK(cudaMemcpyAsync(o->frame_params, G.o_frame_params, 2 * nk * 8, cudaMemcpyDeviceToHost, s));
+    if (o->raw_params && (g.flags & kFlagRawParams))
+      SS_CK(cudaMemcpyAsync(o->raw_params, G.o_raw, 2 * (size_t)g.N * 8, cudaMemcpyDeviceToHost, s));
+  }
+  SS_CK(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < b->gd.size(); i++) {
+    ss_outputs* o = b->outs[i];
+    if (!o) continue;
+    const GroupCtl& C = b->h_ctl[i];
+    if (o->iter_used) *o->iter_used = C.iteration;
+    if (o->device_init_time) *o->device_init_time = b->init_ms / 1000.0;
+    o->stop_reason = C.stop_reason;
+    o->trial_cap_hit = C.cap_hit;
+    o->n_frame_passes = C.n_eval;
+  }
+  return SS_OK;
+}
+
+int Batch::cycles() const { return d->cycles; }
+int Batch::rounds() const { return d->rounds; }
+int Batch::n_groups() const { return (int)d->gd.size(); }
+const GroupCtl* Batch::host_ctl() const { return d->h_ctl.data(); }
+void* Batch::stream() const { return d->stream; }
+
+}  // namespace ss
+
+// ---------------------------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+int ss_align_groups(int32_t n_groups, const ss_inputs* in, ss_outputs* out) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (!in || n_groups < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "no groups");
+  ss::Batch b;
+  int rc = b.prepare(n_groups, in, out, nullptr, 0);
+  if (rc) return rc;
+  rc = b.run();
+  if (rc) return rc;
+  rc = b.collect();
+  if (rc) return rc;
+  double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (out)
+    for (int i = 0; i < n_groups; i++) out[i].elapsed_ms = ms;
+  ss::g_err.clear();
+  return SS_OK;
+}
+
+int ss_align_group_to_template(const ss_inputs* in, ss_outputs* out) { return ss_align_groups(1, in, out); }
+
+struct ss_batch {
+  ss::Batch b;
+};
+
+int ss_batch_create(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_batch** batch) {
+  if (!batch || !in || n_groups < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad batch arguments");
+  *batch = nullptr;
+  ss_batch* h = new ss_batch;
+  int rc = h->b.prepare(n_groups, in, out, nullptr, 0);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *batch = h;
+  return SS_OK;
+}
+
+int ss_batch_run(ss_batch* batch) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  return batch->b.run();
+}
+
+int ss_batch_collect(ss_batch* batch) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  return batch->b.collect();
+}
+
+int ss_batch_set_timing(ss_batch* batch, int32_t on) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  batch->b.set_timing(on != 0);
+  return SS_OK;
+}
+
+int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats) {
+  if (!batch || !stats) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch or stats is NULL");
+  batch->b.stats(stats);
+  return SS_OK;
+}
+
+void* ss_batch_stream(const ss_batch* batch) { return batch ? batch->b.stream() : nullptr; }
+
+void ss_batch_destroy(ss_batch* batch) { delete batch; }
+
+const char* ss_last_error(void) { return ss::last_error(); }
+
+int32_t ss_abi_version(void) { return SS_ABI_VERSION; }
+
+}  // extern "C"
