@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--group", type=int, default=64)
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--precision", default="S", choices=["S", "D"])
-    ap.add_argument("--cpu-sample-frames", type=int, default=4)
+    ap.add_argument("--cpu-sample-frames", type=int, default=16)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -160,6 +160,16 @@ def traffic_summary():
 
 # ------------------------------------------------------------------------------------------------
 
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """The slowest rank's time (every rank calls this at the same point)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_sample(groups, n_frames, threads):
     """The FP64 CPU restatement on the first ``n_frames`` frames of the first group (frames/s)."""
     from oracle import oracle
@@ -246,11 +256,7 @@ def main():
             launches += batch.stats()["kernel_launches"]
         e1.record(stream)
         barrier()
-    ms_total = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_total], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist, device)
     ms_step = ms_total / args.steps
     value = args.frames * world / (ms_step / 1000.0)
     st = batch.stats()

@@ -154,6 +154,17 @@ SS_API int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats);
 SS_API void* ss_batch_stream(const ss_batch* batch);
 SS_API void ss_batch_destroy(ss_batch* batch);
 
+/* The FP64 knot-chain solve of one half-step on its own: the symmetric positive definite
+ * block-tridiagonal normal equations (2x2 blocks, one per used knot) that the reference assembles
+ * in task_filldiagonals.cu:47-159 and task_filljtr.cu:3-58 and hands to its sparse solvers
+ * (eigensolve.cpp:35-38, cusolversolver.cu:53-56), solved by block cyclic reduction on the
+ * device. All pointers are device memory of the current device: diag n x 3 (xx, yy, xy), coupling
+ * (n-1) x 4 ([[c0 c2] [c3 c1]] between block i and block i+1), rhs and x n x 2, row-major.
+ * stream is a cudaStream_t (NULL: the legacy default stream); the call returns after the solve.
+ * The workspace (104 bytes per block) is allocated and freed inside the call. */
+SS_API int ss_solve_block_tridiagonal(int32_t n, const double* diag, const double* coupling, const double* rhs,
+                                      double* x, void* stream);
+
 /* Message of the calling thread's last error ("" if none). */
 SS_API const char* ss_last_error(void);
 

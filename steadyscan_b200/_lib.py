@@ -86,6 +86,9 @@ def load(build_if_missing: bool = True):
     lib.ss_batch_stream.restype = C.c_void_p
     lib.ss_batch_destroy.argtypes = [C.c_void_p]
     lib.ss_batch_destroy.restype = None
+    lib.ss_solve_block_tridiagonal.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p]
+    lib.ss_solve_block_tridiagonal.restype = C.c_int
     _lib = lib
     return lib
 

@@ -175,6 +175,24 @@ def align_group_to_template(*argv, nargout: int = 6, template_storage=None):
     return tuple(outs[:nargout])
 
 
+def solve_block_tridiagonal(diag, coupling, rhs, stream: int = 0):
+    """FP64 block-tridiagonal solve on the GPU (ss_solve_block_tridiagonal).
+
+    diag (n, 3), coupling (n-1, 4) and rhs (n, 2) are float64 torch CUDA tensors (or arrays, copied
+    to the current device); returns x (n, 2) as a torch CUDA tensor."""
+    import torch
+    d = torch.as_tensor(diag, dtype=torch.float64, device="cuda").contiguous()
+    c = torch.as_tensor(coupling, dtype=torch.float64, device="cuda").contiguous()
+    b = torch.as_tensor(rhs, dtype=torch.float64, device="cuda").contiguous()
+    x = torch.empty_like(b)
+    n = d.shape[0]
+    lib = load()
+    torch.cuda.synchronize()
+    check(lib.ss_solve_block_tridiagonal(n, d.data_ptr(), c.data_ptr() if c.numel() else None, b.data_ptr(),
+                                         x.data_ptr(), stream or None))
+    return x
+
+
 class Batch:
     """A prepared batch of groups (ss_batch_*): inputs resident on the device, runnable repeatedly."""
 

@@ -69,11 +69,15 @@ struct GroupDesc {
   int frame_base;   // first global frame index of this group
   // settings
   int max_iter, solver_id, max_filter_iter, filter_id, flags, frac_uniform;
+  int frames_per_cta;       // assembly/final CTA frames (a tuning choice): eval tiles = W * ceil(nF / it)
   double move_thresh, halt_corr, corr_inc_thr, filter_strength, filter_corr_thr, lambda, ls_mult;
   // inputs on the device
   const double* frac;       // Hb x W column-major
   const double* basex;
   const double* basey;
+  const float* frac_f;      // FP32 copies for precision 'S'
+  const float* basex_f;
+  const float* basey_f;
   const uint8_t* base_mask;
   const int* min_points;    // W
   const void* image;        // Hb x fW column-major, engine frame type

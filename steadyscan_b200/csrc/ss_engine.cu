@@ -93,48 +93,91 @@ __global__ void k_fill(double* p, size_t n, double v) {
 // ---------------------------------------------------------------------------------------------
 // kernel dispatch by (compute, frame type, template type)
 
-using EvalFn = void (*)(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, const GroupCtl* ctl);
+// Dynamic shared memory for staging one block column's geometry (tfrac, basex, basey, the next
+// column's tfrac and base_mask) in k_eval.
+constexpr int kStageBytes = 96 * 1024;
+
+using EvalFn = cudaError_t (*)(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
+                               const GroupCtl* ctl, int max_hb);
+using LsFn = cudaError_t (*)(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl);
 using SumFn = void (*)(const void* img, size_t n, double* out, cudaStream_t s);
 
 template <class Acc, class FrameT, class TplT>
-static void eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, const GroupCtl* ctl) {
-  if (tiles <= 0) return;
-  switch (mode) {
-    case kAssemble: k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
-    case kTrial: k_eval<Acc, FrameT, TplT, kTrial><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
-    case kCorr: k_eval<Acc, FrameT, TplT, kCorr><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
-    default: k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 256, 0, s>>>(gd, tg, ctl); break;
+static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
+                               const GroupCtl* ctl, int max_hb) {
+  if (tiles <= 0) return cudaSuccess;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kAssemble>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    attr_set = true;
   }
+  const size_t row_bytes = 4 * sizeof(Acc) + 1;
+  const int rows = (size_t)max_hb * row_bytes <= (size_t)kStageBytes ? max_hb : 0;
+  const size_t smem = (size_t)rows * row_bytes + 64;
+  if (mode == kAssemble)
+    k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows);
+  else
+    k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows);
+  return cudaGetLastError();
 }
+
+template <class Acc, class FrameT, class TplT>
+static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl) {
+  if (frames <= 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(frames * kLsCluster, 1, 1);
+  cfg.blockDim = dim3(kLsThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kLsCluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_linesearch<Acc, FrameT, TplT>, gd, fg, ctl);
+}
+
+struct KernelSet {
+  EvalFn eval;
+  LsFn ls;
+};
 template <class FrameT>
 static void sum_launch(const void* img, size_t n, double* out, cudaStream_t s) {
   k_sum_image<FrameT><<<1, 1024, 0, s>>>(img, n, out);
 }
 
-static EvalFn pick_eval(int compute, int fdt, int tdt) {
+template <class Acc, class FrameT, class TplT>
+static KernelSet kset() {
+  return {eval_launch<Acc, FrameT, TplT>, ls_launch<Acc, FrameT, TplT>};
+}
+
+static KernelSet pick_kernels(int compute, int fdt, int tdt) {
   if (compute == 0) {
     switch (fdt) {
-      case SS_F64: return eval_launch<double, double, double>;
-      case SS_F32: return eval_launch<double, float, double>;
-      case SS_U16: return eval_launch<double, uint16_t, double>;
-      case SS_F16: return eval_launch<double, __half, double>;
+      case SS_F64: return kset<double, double, double>();
+      case SS_F32: return kset<double, float, double>();
+      case SS_U16: return kset<double, uint16_t, double>();
+      case SS_F16: return kset<double, __half, double>();
     }
   } else if (tdt == SS_F16) {
     switch (fdt) {
-      case SS_F64: return eval_launch<float, double, __half>;
-      case SS_F32: return eval_launch<float, float, __half>;
-      case SS_U16: return eval_launch<float, uint16_t, __half>;
-      case SS_F16: return eval_launch<float, __half, __half>;
+      case SS_F64: return kset<float, double, __half>();
+      case SS_F32: return kset<float, float, __half>();
+      case SS_U16: return kset<float, uint16_t, __half>();
+      case SS_F16: return kset<float, __half, __half>();
     }
   } else {
     switch (fdt) {
-      case SS_F64: return eval_launch<float, double, float>;
-      case SS_F32: return eval_launch<float, float, float>;
-      case SS_U16: return eval_launch<float, uint16_t, float>;
-      case SS_F16: return eval_launch<float, __half, float>;
+      case SS_F64: return kset<float, double, float>();
+      case SS_F32: return kset<float, float, float>();
+      case SS_U16: return kset<float, uint16_t, float>();
+      case SS_F16: return kset<float, __half, float>();
     }
   }
-  return nullptr;
+  return {nullptr, nullptr};
 }
 static SumFn pick_sum(int fdt) {
   switch (fdt) {
@@ -223,6 +266,8 @@ struct HostGroup {
   int frame_dt = SS_F64, tpl_dt = SS_F64;
   bool grad_derived = true, frac_uniform = true;
   std::vector<double> p0, templ, xg, yg, frac, bx, by;
+  std::vector<float> frac_f, bx_f, by_f;  // precision 'S' geometry
+  int frames_per_cta = 32;
   std::vector<uint8_t> bmask;
   std::vector<int32_t> minp;
   const void* frames_dev = nullptr;  // caller device pointer when bm_data is on the device
@@ -270,6 +315,7 @@ static int validate_group(const ss_inputs* in, HostGroup& g) {
     return fail(SS_ERR_INVALID_ARGUMENT, "est_dx_knots and est_dy_knots must hold (frameW + 1) x n_frames values");
   if (in->min_points_per_block.rows * in->min_points_per_block.cols < g.W)
     return fail(SS_ERR_INVALID_ARGUMENT, "min_points_per_block needs at least frameW entries");
+  if (g.W > kMaxFrameW) return fail(SS_ERR_INVALID_ARGUMENT, "frameW exceeds the supported maximum of 2048");
   g.group_size = in->group_size;
   if (g.group_size <= 0 || g.group_size % g.W != 0)
     return fail(SS_ERR_INVALID_ARGUMENT, "group_size must be a positive multiple of frameW");
@@ -371,8 +417,8 @@ struct Batch::Impl {
   int* d_frame_group = nullptr;
   int* d_counters = nullptr;  // [0] searching frames, [1] finished groups
   int* h_counters = nullptr;  // pinned
-  int n_tiles = 0, n_frames_total = 0;
-  EvalFn eval = nullptr;
+  int n_tiles = 0, n_frames_total = 0, max_hb = 0;
+  KernelSet ks = {nullptr, nullptr};
   SumFn sum = nullptr;
   std::vector<GroupCtl> h_ctl;
   double init_ms = 0, run_ms = 0;
@@ -396,7 +442,8 @@ struct Batch::Impl {
       }
       cudaEventRecord(events[event_used], stream);
     }
-    eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl);
+    if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl);
+    else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb);
     launches++;
     if (timing) {
       cudaEventRecord(events[event_used + 1], stream);
@@ -433,7 +480,9 @@ static void layout(Batch::Impl* b, char* base) {
     G.Hb = g.Hb; G.W = g.W; G.nF = g.nF; G.fW = g.fW; G.N = g.N; G.Ht = g.Ht; G.Wt = g.Wt;
     G.group_size = g.group_size; G.n_rg = g.n_rg;
     G.tile_base = b->n_tiles;
-    b->n_tiles += (g.fW + 7) / 8;
+    G.frames_per_cta = g.frames_per_cta;
+    b->n_tiles += g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
+    b->max_hb = std::max(b->max_hb, g.Hb);
     G.frame_base = b->n_frames_total;
     b->n_frames_total += g.nF;
     const ss_inputs* in = g.in;
@@ -448,6 +497,13 @@ static void layout(Batch::Impl* b, char* base) {
     G.frac = cv.take<double>(hbw);
     G.basex = cv.take<double>(hbw);
     G.basey = cv.take<double>(hbw);
+    if (b->compute == 1) {
+      G.frac_f = cv.take<float>(hbw);
+      G.basex_f = cv.take<float>(hbw);
+      G.basey_f = cv.take<float>(hbw);
+    } else {
+      G.frac_f = G.basex_f = G.basey_f = nullptr;
+    }
     G.base_mask = cv.take<uint8_t>(hbw);
     G.min_points = cv.take<int>(g.W);
     g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
@@ -525,9 +581,9 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
   b->compute = b->hg[0].compute;
   b->frame_dt = b->hg[0].frame_dt;
   b->tpl_dt = b->hg[0].tpl_dt;
-  b->eval = pick_eval(b->compute, b->frame_dt, b->tpl_dt);
+  b->ks = pick_kernels(b->compute, b->frame_dt, b->tpl_dt);
   b->sum = pick_sum(b->frame_dt);
-  if (!b->eval || !b->sum) return fail(SS_ERR_INVALID_ARGUMENT, "unsupported dtype combination");
+  if (!b->ks.eval || !b->sum) return fail(SS_ERR_INVALID_ARGUMENT, "unsupported dtype combination");
 
   auto t0 = std::chrono::steady_clock::now();
   int ndev = 0;
@@ -559,6 +615,14 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     SS_CK(cudaMemcpyAsync((void*)G.frac, g.frac.data(), hbw * 8, cudaMemcpyHostToDevice, s));
     SS_CK(cudaMemcpyAsync((void*)G.basex, g.bx.data(), hbw * 8, cudaMemcpyHostToDevice, s));
     SS_CK(cudaMemcpyAsync((void*)G.basey, g.by.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+    if (b->compute == 1) {
+      g.frac_f.assign(g.frac.begin(), g.frac.end());
+      g.bx_f.assign(g.bx.begin(), g.bx.end());
+      g.by_f.assign(g.by.begin(), g.by.end());
+      SS_CK(cudaMemcpyAsync((void*)G.frac_f, g.frac_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+      SS_CK(cudaMemcpyAsync((void*)G.basex_f, g.bx_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+      SS_CK(cudaMemcpyAsync((void*)G.basey_f, g.by_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+    }
     SS_CK(cudaMemcpyAsync((void*)G.base_mask, g.bmask.data(), hbw, cudaMemcpyHostToDevice, s));
     SS_CK(cudaMemcpyAsync((void*)G.min_points, g.minp.data(), g.W * 4, cudaMemcpyHostToDevice, s));
     if (!g.frames_dev)
@@ -586,7 +650,8 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     SS_CK(cudaGetLastError());
     b->sum(G.image, (size_t)g.Hb * g.fW, g.d_sum, s);
     SS_CK(cudaGetLastError());
-    for (int t = 0; t < (g.fW + 7) / 8; t++) tile_group[G.tile_base + t] = (int)i;
+    const int ntiles = g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
+    for (int t = 0; t < ntiles; t++) tile_group[G.tile_base + t] = (int)i;
     for (int f = 0; f < g.nF; f++) frame_group[G.frame_base + f] = (int)i;
   }
   SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
@@ -655,20 +720,10 @@ static int run_cycles(Batch::Impl* b) {
     k_solve<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
     b->launches++;
     SS_CK(cudaGetLastError());
-    for (int round = 0; round < kTrialCap + 1; round++) {
-      b->rounds++;
-      b->eval_timed(kTrial);
-      SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
-      k_ls_decide<<<(b->n_frames_total + 7) / 8, 256, 0, s>>>(b->d_gd, b->d_frame_group, b->n_frames_total, b->d_ctl,
-                                                             b->d_counters);
-      b->launches++;
-      SS_CK(cudaGetLastError());
-      SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, sizeof(int), cudaMemcpyDeviceToHost, s));
-      SS_CK(cudaStreamSynchronize(s));
-      if (b->h_counters[0] == 0) break;
-    }
+    b->rounds++;
+    b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
+    SS_CK(cudaGetLastError());
     k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
-    b->eval_timed(kCorr);
     k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
     b->eval_timed(kFinal);
     k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
@@ -693,6 +748,9 @@ int Batch::run() {
   b->event_used = 0;
   rc = run_cycles(b);
   if (rc) return rc;
+  SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost,
+                        b->stream));
+  SS_CK(cudaStreamSynchronize(b->stream));
   for (int m = 0; m < 4; m++) b->eval_ms[m] = 0;
   for (size_t k = 0; k < b->event_used; k += 2) {
     float ms = 0;
@@ -832,6 +890,25 @@ int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats) {
 }
 
 void* ss_batch_stream(const ss_batch* batch) { return batch ? batch->b.stream() : nullptr; }
+
+int ss_solve_block_tridiagonal(int32_t n, const double* diag, const double* coupling, const double* rhs, double* x,
+                               void* stream) {
+  if (n < 1 || !diag || !rhs || !x || (n > 1 && !coupling))
+    return ss::fail(SS_ERR_INVALID_ARGUMENT, "ss_solve_block_tridiagonal: bad arguments");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* work = nullptr;
+  cudaError_t e = cudaMallocAsync(&work, (size_t)n * ss::kCrStride * sizeof(double), s);
+  if (e != cudaSuccess) return ss::fail(SS_ERR_OUT_OF_MEMORY, std::string("workspace: ") + cudaGetErrorString(e));
+  ss::k_block_tridiag<<<1, ss::kSolveThreads, 0, s>>>(n, diag, coupling, rhs, x, work);
+  e = cudaGetLastError();
+  cudaError_t e2 = cudaFreeAsync(work, s);
+  cudaError_t e3 = cudaStreamSynchronize(s);
+  if (e != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+    return ss::fail(SS_ERR_CUDA, std::string("ss_solve_block_tridiagonal: ") +
+                                     cudaGetErrorString(e != cudaSuccess ? e : (e2 != cudaSuccess ? e2 : e3)));
+  ss::g_err.clear();
+  return SS_OK;
+}
 
 void ss_batch_destroy(ss_batch* batch) { delete batch; }
 

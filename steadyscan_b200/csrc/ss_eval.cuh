@@ -1,8 +1,8 @@
-// k_eval: one pass of the warp model over block columns of every group in a batch.
+// Evaluation of the warp model over block columns, and the per-frame line search.
 //
-// A warp owns one block column c (the pixels of the k scan lines between knots c and c+1 of one
-// frame, Hb rows in the reference's block-matrix order, steady_scan.m:601-613); its lanes stride the
-// rows, so frame and geometry loads are coalesced. Per pixel it evaluates the reference's
+// A warp evaluates one block column c (the pixels of the k scan lines between knots c and c+1 of
+// one frame, Hb rows in the reference's block-matrix order, steady_scan.m:601-613); its lanes stride
+// the rows, so frame and geometry loads are coalesced. Per pixel it evaluates the reference's
 // d_applyParameters (task_applyparameters.cuh:33-82), d_createDifferenceImage
 // (task_differenceimage.cuh:13-33) and d_updateGradients (task_updategradients.cu:3-29) in registers
 // and reduces, per column, the sums that d_fillDiagonals (task_filldiagonals.cu:47-159), d_fillJTr
@@ -13,11 +13,38 @@
 // read; here each frame carries two knot vectors instead: kmask (the knots of the last warp of the
 // frame: x, y, mask) and kdiff (the knots of its last difference image). A pass that must see the
 // reference's buffers evaluates both knot sets when they differ.
+//
+// Precision: Acc = double reproduces the reference's 'D' build (FP64 coordinates and sums, fma where
+// nvcc contracts the reference source). Acc = float is the mixed 'S' path: FP32 geometry,
+// coordinates, template samples and per-lane partial sums; the warp reductions, knots, solve and
+// line-search comparison stay FP64.
 #pragma once
+
+#include <cooperative_groups.h>
 
 #include "ss_common.cuh"
 
 namespace ss {
+
+namespace cg = cooperative_groups;
+
+constexpr int kEvalWarps = 8;       // warps per assembly/final CTA
+constexpr int kLsCluster = 8;       // CTAs per frame in the line-search cluster
+constexpr int kLsThreads = 256;
+constexpr int kLsMaxKnots = 256;    // knots per cluster CTA: frame_w <= kLsCluster * kLsMaxKnots
+constexpr int kMaxFrameW = kLsCluster * kLsMaxKnots;
+
+// Resident 256-thread CTAs per SM requested from the register allocator: the FP32 path is
+// latency-bound on frame loads and template gathers and needs the warps; the FP64 path keeps its
+// registers.
+template <class Acc>
+struct MinBlocks {
+  static constexpr int value = 2;
+};
+template <>
+struct MinBlocks<float> {
+  static constexpr int value = 4;
+};
 
 __device__ __forceinline__ bool frame_active(const GroupDesc& G, int f, int shift) {
   // groupActive[groupId + shift * nGroups] with zero-filled reads past the array
@@ -26,16 +53,42 @@ __device__ __forceinline__ bool frame_active(const GroupDesc& G, int f, int shif
   return gid < 2 * G.n_rg && G.grp_active[gid];
 }
 
-// Warped position and validity of one pixel (task_applyparameters.cuh:57-62), FP64 as in the
-// reference's 'D' build; a*b+c is contracted into fma the way nvcc contracts the reference source.
-__device__ __forceinline__ bool warp_pixel(double kx0, double kx1, double ky0, double ky1, double f, double bx,
-                                           double by, bool bm, double tw, double th, double& x, double& y) {
-  x = fma(kx1, f, fma(kx0, 1.0 - f, bx));
-  y = fma(ky1, f, fma(ky0, 1.0 - f, by));
-  return bm && x >= 0.0 && x < tw && y >= 0.0 && y < th;
+template <class Acc>
+struct Limits;
+template <>
+struct Limits<double> {  // templateW - eps<double>() (task_applyparameters.cuh:44-45, eps.h:14-22)
+  __device__ static double lim(int n) { return (double)(n - 1) - 2.220446049250313e-16; }
+};
+template <>
+struct Limits<float> {   // templateW - eps<float>()
+  __device__ static float lim(int n) { return (float)(n - 1) - 1.1920928955078125e-7f; }
+};
+
+// Warped position and validity of one pixel (task_applyparameters.cuh:57-62); a*b+c is contracted
+// into fma the way nvcc contracts the reference source.
+template <class Acc>
+__device__ __forceinline__ bool warp_pixel(Acc kx0, Acc kx1, Acc ky0, Acc ky1, Acc f, Acc bx, Acc by, bool bm, Acc tw,
+                                           Acc th, Acc& x, Acc& y) {
+  const Acc one = (Acc)1;
+  x = fma(kx1, f, fma(kx0, one - f, bx));
+  y = fma(ky1, f, fma(ky0, one - f, by));
+  return bm && x >= (Acc)0 && x < tw && y >= (Acc)0 && y < th;
 }
 
-template <class Acc, class TplT>
+// Integer part and fraction of a non-negative coordinate, as static_cast<int> in the reference.
+__device__ __forceinline__ int split(double x, double& frac) {
+  int i = (int)x;
+  frac = x - (double)i;
+  return i;
+}
+__device__ __forceinline__ int split(float x, float& frac) {
+  // x + 2^23 rounded down holds floor(x) in its mantissa (0 <= x < 2^23)
+  float v = __fadd_rd(x, 8388608.0f);
+  frac = x - (v - 8388608.0f);
+  return __float_as_int(v) - 0x4B000000;
+}
+
+template <class Acc>
 struct Sample {
   Acc wI, wx, wy;
 };
@@ -44,16 +97,16 @@ struct Sample {
 // task_updategradients.cu:12-20). With gquad == nullptr the gradients are the template's forward
 // differences (steady_scan.m:178-179), taken from the same four template values.
 template <class Acc, class TplT, bool kGrad>
-__device__ __forceinline__ Sample<Acc, TplT> sample(const GroupDesc& G, double x, double y) {
-  int ix = (int)x, iy = (int)y;
-  Acc xf = (Acc)(x - (double)ix), yf = (Acc)(y - (double)iy);
-  size_t qi = (size_t)iy * (size_t)(G.Wt - 1) + (size_t)ix;
+__device__ __forceinline__ Sample<Acc> sample(const GroupDesc& G, Acc x, Acc y) {
+  Acc xf, yf;
+  const int ix = split(x, xf), iy = split(y, yf);
+  const size_t qi = (size_t)iy * (size_t)(G.Wt - 1) + (size_t)ix;
   Acc t00, t01, t10, t11;
   load_quad<Acc, TplT>(G.tquad, qi, t00, t01, t10, t11);
-  Acc one = (Acc)1;
+  const Acc one = (Acc)1;
   Acc a = fma(yf, t10, (one - yf) * t00);
   Acc b = fma(yf, t11, (one - yf) * t01);
-  Sample<Acc, TplT> s;
+  Sample<Acc> s;
   s.wI = fma(xf, b, (one - xf) * a);
   if (kGrad) {
     Acc gx0, gx1, gy0, gy1;
@@ -79,104 +132,117 @@ __device__ __forceinline__ __half ld_frame<__half>(const void* base, size_t i) {
   unsigned short raw = __ldg(reinterpret_cast<const unsigned short*>(base) + i);
   return __ushort_as_half(raw);
 }
+template <class Acc, class FrameT>
+__device__ __forceinline__ Acc ld_pixel(const void* base, size_t i) {
+  return (Acc)to_double(ld_frame<FrameT>(base, i));
+}
+template <>
+__device__ __forceinline__ float ld_pixel<float, uint16_t>(const void* base, size_t i) {
+  return (float)ld_frame<uint16_t>(base, i);
+}
+template <>
+__device__ __forceinline__ float ld_pixel<float, __half>(const void* base, size_t i) {
+  return __half2float(ld_frame<__half>(base, i));
+}
+template <>
+__device__ __forceinline__ float ld_pixel<float, float>(const void* base, size_t i) {
+  return ld_frame<float>(base, i);
+}
 
+// Knots of one block column: set A (mask, position, gradients) and set B (difference image).
+template <class Acc>
+struct ColKnots {
+  Acc ax0, ax1, ay0, ay1, bx0, bx1, by0, by1;
+  bool dual;
+};
+
+template <class Acc>
+__device__ __forceinline__ void set_knots(ColKnots<Acc>& k, double ax0, double ax1, double ay0, double ay1, double bx0,
+                                          double bx1, double by0, double by1) {
+  k.ax0 = (Acc)ax0; k.ax1 = (Acc)ax1; k.ay0 = (Acc)ay0; k.ay1 = (Acc)ay1;
+  k.bx0 = (Acc)bx0; k.bx1 = (Acc)bx1; k.by0 = (Acc)by0; k.by1 = (Acc)by1;
+  k.dual = bx0 != ax0 || bx1 != ax1 || by0 != ay0 || by1 != ay1;
+}
+
+// Geometry of one block column; generic pointers (global or shared memory).
+template <class Acc>
+struct ColGeo {
+  const Acc* frac;
+  const Acc* bx;
+  const Acc* by;
+  const uint8_t* bm;
+  const Acc* fnext;  // tfrac of column (c+1) mod W; equals frac when all columns match
+};
+
+template <class Acc>
+__device__ __forceinline__ ColGeo<Acc> global_geo(const GroupDesc& G, int cc);
+template <>
+__device__ __forceinline__ ColGeo<double> global_geo<double>(const GroupDesc& G, int cc) {
+  const size_t o = (size_t)cc * G.Hb, on = (size_t)((cc + 1) % G.W) * G.Hb;
+  return {G.frac + o, G.basex + o, G.basey + o, G.base_mask + o, G.frac_uniform ? G.frac + o : G.frac + on};
+}
+template <>
+__device__ __forceinline__ ColGeo<float> global_geo<float>(const GroupDesc& G, int cc) {
+  const size_t o = (size_t)cc * G.Hb, on = (size_t)((cc + 1) % G.W) * G.Hb;
+  return {G.frac_f + o, G.basex_f + o, G.basey_f + o, G.base_mask + o, G.frac_uniform ? G.frac_f + o : G.frac_f + on};
+}
+
+__host__ __device__ constexpr int nsums(int mode) {
+  return mode == kAssemble ? kCsAssemble : (mode == kTrial ? 1 : kCsStride - 2);
+}
+
+// Evaluates one block column with one warp and returns the warp-reduced sums (all lanes) and the
+// valid-pixel count. coli is the column's offset in the frame data; mask_out (kFinal) receives the
+// reference's mask output.
 template <class Acc, class FrameT, class TplT, int MODE>
-__global__ void __launch_bounds__(256) k_eval(const GroupDesc* __restrict__ gds, const int* __restrict__ tile_group,
-                                              const GroupCtl* __restrict__ ctl) {
-  const int g = tile_group[blockIdx.x];
-  const GroupDesc& G = gds[g];
-  const GroupCtl& C = ctl[g];
-  const int want = (MODE == kCorr) ? kPhIterEnd : (MODE == kFinal ? kPhFinal : kPhHalf);
-  if (C.phase != want) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = (blockIdx.x - G.tile_base) * 8 + warp;
-  if (c >= G.fW) return;
-  const int f = c / G.W, cc = c - f * G.W;
-  const int W = G.W, N = G.N, Hb = G.Hb;
-  const int shift = C.shift;
-
-  // knots of set A (mask, position, gradients) and set B (difference image)
-  double ax0, ax1, ay0, ay1, bx0, bx1, by0, by1;
-  bool dual = false;
-  bool active = true;
-  if (MODE == kAssemble) {
-    ax0 = G.p[c]; ax1 = G.p[c + 1]; ay0 = G.p[N + c]; ay1 = G.p[N + c + 1];
-    active = frame_active(G, f, shift);
-    if (!active) {
-      const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
-      bx0 = kd[cc]; bx1 = kd[cc + 1]; by0 = kd[W + 1 + cc]; by1 = kd[W + 1 + cc + 1];
-      dual = bx0 != ax0 || bx1 != ax1 || by0 != ay0 || by1 != ay1;
-    }
-  } else if (MODE == kTrial) {
-    if (!(G.fstate[f] & 2)) return;
-    // pnew = p + deltaP (task_linesearch.cu:50-54); the frame's right boundary knot is the
-    // committed knot at line-search start, or the never-written 1e6 for the last frame.
-    ax0 = G.p[c] + G.delta_p[c];
-    ay0 = G.p[N + c] + G.delta_p[N + c];
-    if (cc + 1 < W) {
-      ax1 = G.p[c + 1] + G.delta_p[c + 1];
-      ay1 = G.p[N + c + 1] + G.delta_p[N + c + 1];
-    } else if (f + 1 < G.nF) {
-      ax1 = G.p_snap[c + 1];
-      ay1 = G.p_snap[N + c + 1];
-    } else {
-      ax1 = kPnewFill;
-      ay1 = kPnewFill;
-    }
-  } else {
-    const double* km = G.kmask + (size_t)f * 2 * (W + 1);
-    ax0 = km[cc]; ax1 = km[cc + 1]; ay0 = km[W + 1 + cc]; ay1 = km[W + 1 + cc + 1];
-    const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
-    bx0 = kd[cc]; bx1 = kd[cc + 1]; by0 = kd[W + 1 + cc]; by1 = kd[W + 1 + cc + 1];
-    dual = bx0 != ax0 || bx1 != ax1 || by0 != ay0 || by1 != ay1;
-  }
-
-  const double tw = (double)(G.Wt - 1) - 2.220446049250313e-16;  // templateW - eps<double>() (eps.h:14-22)
-  const double th = (double)(G.Ht - 1) - 2.220446049250313e-16;
-  const size_t colm = (size_t)cc * Hb;
-  const size_t coli = (size_t)c * Hb;
-  const size_t coln = (size_t)((cc + 1) % W) * Hb;
+__device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, const ColGeo<Acc>& geo,
+                                            const ColKnots<Acc>& k, double (&out)[kCsStride], int& cnt_out,
+                                            uint8_t* mask_out) {
+  const int lane = threadIdx.x & 31;
+  const int Hb = G.Hb;
+  const Acc tw = Limits<Acc>::lim(G.Wt), th = Limits<Acc>::lim(G.Ht);
   const Acc one = (Acc)1;
-
-  Acc s[kCsStride];
+  const bool split_fn = geo.fnext != geo.frac;
+  constexpr int NS = nsums(MODE);
+  Acc s[NS];
 #pragma unroll
-  for (int k = 0; k < kCsStride; k++) s[k] = (Acc)0;
+  for (int i = 0; i < NS; i++) s[i] = (Acc)0;
   int cnt = 0;
   bool run = true;  // leading run of valid pixels (task_correlation.cu:24-34)
 
+#pragma unroll 2
   for (int r0 = 0; r0 < Hb; r0 += 32) {
     const int r = r0 + lane;
     const bool in = r < Hb;
-    double f = 0, bxv = 0, byv = 0;
+    Acc f = 0, bxv = 0, byv = 0;
     bool bm = false;
     if (in) {
-      f = __ldg(G.frac + colm + r);
-      bxv = __ldg(G.basex + colm + r);
-      byv = __ldg(G.basey + colm + r);
-      bm = __ldg(G.base_mask + colm + r) != 0;
+      f = geo.frac[r];
+      bxv = geo.bx[r];
+      byv = geo.by[r];
+      bm = geo.bm[r] != 0;
     }
-    double x, y;
-    bool mA = warp_pixel(ax0, ax1, ay0, ay1, f, bxv, byv, bm, tw, th, x, y) && in;
+    Acc x, y;
+    const bool mA = warp_pixel<Acc>(k.ax0, k.ax1, k.ay0, k.ay1, f, bxv, byv, bm, tw, th, x, y) && in;
     cnt += mA ? 1 : 0;
 
     if (MODE == kAssemble) {
-      Acc img = in ? (Acc)to_double(ld_frame<FrameT>(G.image, coli + r)) : (Acc)0;
+      Acc img = (mA || (k.dual && in)) ? ld_pixel<Acc, FrameT>(G.image, coli + r) : (Acc)0;
       Acc wx = 0, wy = 0, d = 0;
       if (mA) {
-        Sample<Acc, TplT> sa = sample<Acc, TplT, true>(G, x, y);
+        Sample<Acc> sa = sample<Acc, TplT, true>(G, x, y);
         wx = sa.wx;
         wy = sa.wy;
         d = img - sa.wI;
       }
-      if (dual) {
-        double xb, yb;
-        bool mB = warp_pixel(bx0, bx1, by0, by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
+      if (k.dual) {
+        Acc xb, yb;
+        bool mB = warp_pixel<Acc>(k.bx0, k.bx1, k.by0, k.by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
         d = mB ? img - sample<Acc, TplT, false>(G, xb, yb).wI : (Acc)0;
       }
-      Acc fa = (Acc)f;
-      Acc fn = G.frac_uniform ? fa : (in ? (Acc)__ldg(G.frac + coln + r) : (Acc)0);
-      Acc fsq = fa * fa, csq = (one - fa) * (one - fa), fc = fa - fsq, fnsq = fn * fn;
-      Acc gxx = wx * wx, gyy = wy * wy, gxy = wx * wy;
+      const Acc fn = split_fn ? (in ? geo.fnext[r] : (Acc)0) : f;
+      const Acc fsq = f * f, csq = (one - f) * (one - f), fc = f - fsq, fnsq = fn * fn;
+      const Acc gxx = wx * wx, gyy = wy * wy, gxy = wx * wy;
       s[kCsSsd] = fma(d, d, s[kCsSsd]);
       s[kCsAxx] = fma(gxx, csq, s[kCsAxx]);
       s[kCsAyy] = fma(gyy, csq, s[kCsAyy]);
@@ -187,36 +253,34 @@ __global__ void __launch_bounds__(256) k_eval(const GroupDesc* __restrict__ gds,
       s[kCsOxx] = fma(gxx, fc, s[kCsOxx]);
       s[kCsOyy] = fma(gyy, fc, s[kCsOyy]);
       s[kCsOxy] = fma(gxy, fc, s[kCsOxy]);
-      Acc d1 = d * (one - fa), d2 = d * fa;
+      const Acc d1 = d * (one - f), d2 = d * f;
       s[kCsJ1x] = fma(d1, wx, s[kCsJ1x]);
       s[kCsJ1y] = fma(d1, wy, s[kCsJ1y]);
       s[kCsJ2x] = fma(d2, wx, s[kCsJ2x]);
       s[kCsJ2y] = fma(d2, wy, s[kCsJ2y]);
     } else if (MODE == kTrial) {
       if (mA) {
-        Acc img = (Acc)to_double(ld_frame<FrameT>(G.image, coli + r));
-        Acc d = img - sample<Acc, TplT, false>(G, x, y).wI;
+        Acc d = ld_pixel<Acc, FrameT>(G.image, coli + r) - sample<Acc, TplT, false>(G, x, y).wI;
         s[kCsSsd] = fma(d, d, s[kCsSsd]);
       }
     } else {
       // swapped difference image D' of task_correlation.cu:51-60 over the state (kmask, kdiff)
-      Acc img = in ? (Acc)to_double(ld_frame<FrameT>(G.image, coli + r)) : (Acc)0;
+      Acc img = in ? ld_pixel<Acc, FrameT>(G.image, coli + r) : (Acc)0;
       Acc wA = 0;
       if (mA) wA = sample<Acc, TplT, false>(G, x, y).wI;
       bool mB = mA;
       Acc wB = wA;
-      if (dual) {
-        double xb, yb;
-        mB = warp_pixel(bx0, bx1, by0, by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
+      if (k.dual) {
+        Acc xb, yb;
+        mB = warp_pixel<Acc>(k.bx0, k.bx1, k.by0, k.by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
         wB = mB ? sample<Acc, TplT, false>(G, xb, yb).wI : (Acc)0;
       }
-      Acc dstate = mB ? img - wB : (Acc)0;         // differenceImage
-      Acc dp = mA ? img - dstate : dstate;         // after d_swapWIDiff
+      Acc dstate = mB ? img - wB : (Acc)0;  // differenceImage
+      Acc dp = mA ? img - dstate : dstate;  // after d_swapWIDiff
       s[kCsSumD] += dp;
       unsigned bal = __ballot_sync(0xffffffffu, mA);
       unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
-      bool inset = run && ((~bal & le) == 0u) && mA;
-      if (inset) {
+      if (run && ((~bal & le) == 0u) && mA) {
         s[kCsSetN] += one;
         s[kCsSetD] += dp;
         s[kCsSetDD] = fma(dp, dp, s[kCsSetDD]);
@@ -236,23 +300,274 @@ __global__ void __launch_bounds__(256) k_eval(const GroupDesc* __restrict__ gds,
           s[kCsFinalSsd] = fma(dA, dA, s[kCsFinalSsd]);
         }
       }
-      if (MODE == kFinal && G.o_mask && in) G.o_mask[coli + r] = mA ? 1 : 0;
+      if (MODE == kFinal && mask_out && in) mask_out[r] = mA ? 1 : 0;
     }
   }
+  cnt_out = warp_sum(cnt);
+#pragma unroll
+  for (int i = 0; i < NS; i++) out[i] = warp_sum((double)s[i]);
+}
 
-  // Leading-run rows past Hb do not exist; the run simply ends at Hb.
-  cnt = warp_sum(cnt);
-  const int nsum = (MODE == kAssemble) ? kCsAssemble : (MODE == kTrial ? 1 : kCsStride - 2);
-  double out[kCsStride];
-#pragma unroll
-  for (int k = 0; k < kCsStride; k++) out[k] = (k < nsum) ? warp_sum((double)s[k]) : 0.0;
-  if (lane == 0) {
-    double* dst = G.colsum + (size_t)c * kCsStride;
-#pragma unroll
-    for (int k = 0; k < kCsStride; k++)
-      if (k < nsum) dst[k] = out[k];
-    G.colcnt[c] = cnt;
+// Assembly (at p) and final (at kmask) passes. A CTA takes one block column index cc of one group
+// and G.frames_per_cta of its frames, a warp per frame at a time; the column's geometry is staged in
+// shared memory once for all of them, and the frames share the template rows around the column in L1.
+template <class Acc, class FrameT, class TplT, int MODE>
+__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval(const GroupDesc* __restrict__ gds,
+                                                          const int* __restrict__ tile_group,
+                                                          const GroupCtl* __restrict__ ctl, int stage_rows) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int g = tile_group[blockIdx.x];
+  const GroupDesc& G = gds[g];
+  const GroupCtl& C = ctl[g];
+  if (C.phase != (MODE == kFinal ? kPhFinal : kPhHalf)) return;
+  const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
+  const int nfb = (G.nF + fpc - 1) / fpc;
+  const int local = blockIdx.x - G.tile_base;
+  const int cc = local / nfb, fb = local - cc * nfb;
+  const int warp = threadIdx.x >> 5;
+
+  ColGeo<Acc> geo = global_geo<Acc>(G, cc);
+  if (Hb <= stage_rows) {
+    Acc* sf = reinterpret_cast<Acc*>(smem);
+    Acc* sx = sf + Hb;
+    Acc* sy = sx + Hb;
+    Acc* sn = sy + Hb;
+    uint8_t* sm = reinterpret_cast<uint8_t*>(sn + Hb);
+    const bool split_fn = geo.fnext != geo.frac;
+    for (int r = threadIdx.x; r < Hb; r += blockDim.x) {
+      sf[r] = __ldg(geo.frac + r);
+      sx[r] = __ldg(geo.bx + r);
+      sy[r] = __ldg(geo.by + r);
+      sm[r] = __ldg(geo.bm + r);
+      if (split_fn) sn[r] = __ldg(geo.fnext + r);
+    }
+    __syncthreads();
+    geo = {sf, sx, sy, sm, split_fn ? sn : sf};
   }
+  const int f_end = min(G.nF, (fb + 1) * fpc);
+  for (int f = fb * fpc + warp; f < f_end; f += kEvalWarps) {
+    const int c = f * W + cc;
+    ColKnots<Acc> k;
+    if (MODE == kAssemble) {
+      const double ax0 = G.p[c], ax1 = G.p[c + 1], ay0 = G.p[N + c], ay1 = G.p[N + c + 1];
+      if (frame_active(G, f, C.shift)) {
+        set_knots(k, ax0, ax1, ay0, ay1, ax0, ax1, ay0, ay1);
+      } else {  // the difference image of an inactive frame is stale
+        const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
+        set_knots(k, ax0, ax1, ay0, ay1, kd[cc], kd[cc + 1], kd[W + 1 + cc], kd[W + 1 + cc + 1]);
+      }
+    } else {
+      const double* km = G.kmask + (size_t)f * 2 * (W + 1);
+      const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
+      set_knots(k, km[cc], km[cc + 1], km[W + 1 + cc], km[W + 1 + cc + 1], kd[cc], kd[cc + 1], kd[W + 1 + cc],
+                kd[W + 1 + cc + 1]);
+    }
+    const size_t coli = (size_t)c * Hb;
+    double out[kCsStride];
+    int cnt;
+    eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, G.o_mask ? G.o_mask + coli : nullptr);
+    if ((threadIdx.x & 31) == 0) {
+      double* dst = G.colsum + (size_t)c * kCsStride;
+#pragma unroll
+      for (int i = 0; i < nsums(MODE); i++) dst[i] = out[i];
+      G.colcnt[c] = cnt;
+    }
+  }
+}
+
+// Line search of one frame per thread-block cluster (task_linesearch.cu:76-149), for every frame of
+// every group in kPhHalf. The cluster's CTAs split the frame's block columns; each trial's SSD,
+// valid count, block presence and largest step are reduced across the cluster through distributed
+// shared memory, rank 0 decides, and every CTA applies the decision to its own copy of the knots, so
+// the frame's whole search runs without leaving the kernel. The frame's right boundary knot is the
+// committed knot at line-search start (p_snap), or the never-written 1e6 for the last frame.
+// After shift 1 the cluster also evaluates the frame's correlation sums (the iteration-end state).
+template <class Acc, class FrameT, class TplT>
+__global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearch(const GroupDesc* __restrict__ gds,
+                                                           const int* __restrict__ frame_group,
+                                                           GroupCtl* __restrict__ ctl) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int gf = blockIdx.x / kLsCluster;
+  const int g = frame_group[gf];
+  const GroupDesc& G = gds[g];
+  GroupCtl& C = ctl[g];
+  if (C.phase != kPhHalf) return;  // uniform over the cluster
+  const int f = gf - G.frame_base;
+  const int W = G.W, N = G.N, Hb = G.Hb, b0 = f * W;
+  const int shift = C.shift;
+  const bool searching = G.fstate[f] & 2;
+  if (!searching && shift == 0) return;
+
+  const int cpc = (W + kLsCluster - 1) / kLsCluster;
+  const int lo = min(W, rank * cpc), hi = min(W, lo + cpc);  // own knots [lo, hi); copies [lo, hi]
+  const int nk = hi - lo + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = kLsThreads / 32;
+  const bool last_frame = f + 1 == G.nF;
+
+  // knot copies: p, deltaP, kmask, kdiff over [lo, hi] for x (first) and y (second)
+  __shared__ double s_p[2][kLsMaxKnots + 1], s_dp[2][kLsMaxKnots + 1], s_km[2][kLsMaxKnots + 1],
+      s_kd[2][kLsMaxKnots + 1];
+  __shared__ double s_part[5][kLsThreads / 32];
+  __shared__ double s_red[5];      // this CTA's partials: ssd, cnt, present, max|dp|, regulariser
+  __shared__ double s_dec[2];      // rank 0's decision: action, errval
+  const double bxv = last_frame ? kPnewFill : G.p_snap[b0 + W];
+  const double byv = last_frame ? kPnewFill : G.p_snap[N + b0 + W];
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+    const int t = lo + i;
+    for (int d = 0; d < 2; d++) {
+      const size_t o = (size_t)d * N + b0 + t;
+      if (t < W) {
+        s_p[d][i] = G.p[o];
+        s_dp[d][i] = G.delta_p[o];
+      } else {  // the frame's boundary knot: fixed trial value, no step
+        s_p[d][i] = d ? byv : bxv;
+        s_dp[d][i] = 0.0;
+      }
+      s_km[d][i] = G.kmask[(size_t)f * 2 * (W + 1) + d * (W + 1) + t];
+      s_kd[d][i] = G.kdiff[(size_t)f * 2 * (W + 1) + d * (W + 1) + t];
+    }
+  }
+  __syncthreads();
+
+  const double thr = G.move_thresh, rho = G.ls_mult;
+  int trials = 0;
+  while (searching) {
+    // trial knots: pnew = p + deltaP for own knots (task_linesearch.cu:50-54), boundary as is
+    double ssd = 0, maxabs = 0, reg = 0;
+    long long cnt = 0;
+    bool present = false;
+    for (int t = lo + warp; t < hi; t += nw) {
+      const int i = t - lo;
+      const double x0 = s_p[0][i] + s_dp[0][i], y0 = s_p[1][i] + s_dp[1][i];
+      const double x1 = (t + 1 < W) ? s_p[0][i + 1] + s_dp[0][i + 1] : s_p[0][i + 1];
+      const double y1 = (t + 1 < W) ? s_p[1][i + 1] + s_dp[1][i + 1] : s_p[1][i + 1];
+      ColKnots<Acc> k;
+      set_knots(k, x0, x1, y0, y1, x0, x1, y0, y1);
+      double out[kCsStride];
+      int c;
+      eval_column<Acc, FrameT, TplT, kTrial>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      ssd += out[kCsSsd];
+      cnt += c;
+      present |= c >= G.min_points[t];
+    }
+    for (int i = threadIdx.x; i < hi - lo; i += blockDim.x) {
+      const int t = lo + i;
+      maxabs = fmax(maxabs, fmax(fabs(s_dp[0][i]), fabs(s_dp[1][i])));
+      if (G.lambda != 0.0) {  // knot-difference regulariser of the trial (extension)
+        double x0 = s_p[0][i] + s_dp[0][i], y0 = s_p[1][i] + s_dp[1][i];
+        double x1 = t + 1 < W ? s_p[0][i + 1] + s_dp[0][i + 1] : G.p_snap[b0 + W];
+        double y1 = t + 1 < W ? s_p[1][i + 1] + s_dp[1][i + 1] : G.p_snap[N + b0 + W];
+        reg += (x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxabs = fmax(maxabs, __shfl_xor_sync(0xffffffffu, maxabs, o));
+    reg = warp_sum(reg);
+    if (lane == 0) {
+      s_part[0][warp] = ssd;
+      s_part[1][warp] = (double)cnt;
+      s_part[2][warp] = present ? 1.0 : 0.0;
+      s_part[3][warp] = maxabs;
+      s_part[4][warp] = reg;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0, b = 0, pr = 0, m = 0, rg = 0;
+      for (int w = 0; w < nw; w++) {
+        a += s_part[0][w];
+        b += s_part[1][w];
+        pr = fmax(pr, s_part[2][w]);
+        m = fmax(m, s_part[3][w]);
+        rg += s_part[4][w];
+      }
+      s_red[0] = a; s_red[1] = b; s_red[2] = pr; s_red[3] = m; s_red[4] = rg;
+    }
+    cluster.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+      double a = 0, b = 0, pr = 0, m = 0, rg = 0;
+      for (int q = 0; q < kLsCluster; q++) {
+        const double* r = cluster.map_shared_rank(s_red, q);
+        a += r[0]; b += r[1]; pr = fmax(pr, r[2]); m = fmax(m, r[3]); rg += r[4];
+      }
+      // actions: 0 accept, 1 reduce and retry, 2 stop; bit 4: a block was present (the
+      // difference image was written)
+      int action;
+      double ev = 0;
+      if (pr > 0) {
+        ev = (G.lambda != 0.0) ? (a + G.lambda * rg) / b : a / b;
+        if (ev < G.errval[shift * G.nF + f]) action = 0;
+        else action = (m > thr) ? 1 : 2;  // d_checkMovement before d_reduceDeltaP
+        action |= 16;
+      } else {
+        action = (m * rho > thr) ? 1 : 2;  // d_reduceDeltaP before d_checkMovement
+      }
+      ++trials;
+      atomicAdd((unsigned long long*)&C.n_eval, 1ull);
+      atomicAdd((unsigned long long*)&C.passes[kTrial], 1ull);
+      if ((action & 15) == 1 && trials >= kTrialCap) {
+        action = (action & 16) | 2;
+        C.cap_hit = 1;
+      }
+      if ((action & 15) == 0 && b0 == 0) G.errval[shift * G.nF] = ev;  // only idx == 0 writes (:135)
+      s_dec[0] = (double)action;
+      s_dec[1] = ev;
+    }
+    cluster.sync();
+    const int action = (int)*cluster.map_shared_rank(&s_dec[0], 0);
+    // the reference's buffers now hold this trial's x, y, mask; the difference image only if a
+    // block was present; then p or deltaP change
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+      const int t = lo + i;
+      for (int d = 0; d < 2; d++) {
+        const double v = (t < W) ? s_p[d][i] + s_dp[d][i] : s_p[d][i];
+        s_km[d][i] = v;
+        if (action & 16) s_kd[d][i] = v;
+        if (t < W) {
+          if ((action & 15) == 0) s_p[d][i] = v;
+          else if ((action & 15) == 1) s_dp[d][i] *= rho;
+          else if (!(action & 16)) s_dp[d][i] *= rho;  // absent block: reduced before the stop test
+        }
+      }
+    }
+    __syncthreads();
+    if ((action & 15) != 1) break;
+  }
+
+  if (searching) {  // write back own knots (and the boundary copies) of the search
+    for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+      const int t = lo + i;
+      for (int d = 0; d < 2; d++) {
+        if (t < hi) {
+          G.p[(size_t)d * N + b0 + t] = s_p[d][i];
+          G.delta_p[(size_t)d * N + b0 + t] = s_dp[d][i];
+        }
+        if (t < hi || t == W) {
+          G.kmask[(size_t)f * 2 * (W + 1) + d * (W + 1) + t] = s_km[d][i];
+          G.kdiff[(size_t)f * 2 * (W + 1) + d * (W + 1) + t] = s_kd[d][i];
+        }
+      }
+    }
+    if (rank == 0 && threadIdx.x == 0) G.fstate[f] = 0;
+  }
+
+  if (shift == 1) {  // iteration-end correlation sums of this frame's state (task.cpp:284)
+    for (int t = lo + warp; t < hi; t += nw) {
+      const int i = t - lo;
+      ColKnots<Acc> k;
+      set_knots(k, s_km[0][i], s_km[0][i + 1], s_km[1][i], s_km[1][i + 1], s_kd[0][i], s_kd[0][i + 1], s_kd[1][i],
+                s_kd[1][i + 1]);
+      double out[kCsStride];
+      int c;
+      eval_column<Acc, FrameT, TplT, kCorr>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      if (lane == 0) {
+        double* dst = G.colsum + (size_t)(b0 + t) * kCsStride;
+        for (int q = 0; q < nsums(kCorr); q++) dst[q] = out[q];
+        G.colcnt[b0 + t] = c;
+      }
+    }
+  }
+  cluster.sync();  // no CTA leaves while others may still read its shared memory
 }
 
 }  // namespace ss

@@ -17,6 +17,117 @@ __device__ __forceinline__ void cr_load(const double* n, double& d0, double& d1,
   b0 = n[11]; b1 = n[12];
 }
 
+// Solves a symmetric positive definite block-tridiagonal system with 2x2 blocks in place by block
+// cyclic reduction, with the whole CTA. Node i of cr holds (D_i: xx yy xy, L_i: coupling to its left
+// neighbour, R_i: coupling to its right neighbour, b_i) in kCrStride doubles; on return b_i holds
+// x_i. At stride s every multiple of 2s absorbs its two odd-multiple neighbours (each elimination is
+// a Schur complement on 2x2 blocks), so the reduction takes ceil(log2 h) levels; back substitution
+// runs the levels in reverse. In exact arithmetic this is the LDL^T of the system in a nested
+// dissection order, so it solves the same equations as the reference's exact sparse solvers
+// (eigensolve.cpp:35-38, cusolversolver.cu:53-56).
+__device__ void cr_solve(double* cr, int h) {
+  const int t = threadIdx.x, nt = blockDim.x;
+  int top = 1;
+  while (top < h) top <<= 1;
+  for (int s = 1; s < h; s <<= 1) {
+    for (int j = t * 2 * s; j < h; j += nt * 2 * s) {
+      double* n = cr + (size_t)j * kCrStride;
+      double d0, d1, d2, b0, b1;
+      M2 L, R;
+      cr_load(n, d0, d1, d2, L, R, b0, b1);
+      M2 D = {d0, d2, d2, d1};
+      if (j - s >= 0) {
+        double e0, e1, e2, c0, c1;
+        M2 Ll, Rl;
+        cr_load(cr + (size_t)(j - s) * kCrStride, e0, e1, e2, Ll, Rl, c0, c1);
+        M2 Di = m2_inv({e0, e2, e2, e1});
+        M2 T = m2_mul(L, Di);
+        D = m2_sub(D, m2_mul(T, Rl));
+        b0 -= T.a * c0 + T.b * c1;
+        b1 -= T.c * c0 + T.d * c1;
+        L = m2_neg(m2_mul(T, Ll));
+      }
+      if (j + s < h) {
+        double e0, e1, e2, c0, c1;
+        M2 Lr, Rr;
+        cr_load(cr + (size_t)(j + s) * kCrStride, e0, e1, e2, Lr, Rr, c0, c1);
+        M2 Di = m2_inv({e0, e2, e2, e1});
+        M2 T = m2_mul(R, Di);
+        D = m2_sub(D, m2_mul(T, Lr));
+        b0 -= T.a * c0 + T.b * c1;
+        b1 -= T.c * c0 + T.d * c1;
+        R = m2_neg(m2_mul(T, Rr));
+      }
+      n[0] = D.a; n[1] = D.d; n[2] = 0.5 * (D.b + D.c);
+      n[3] = L.a; n[4] = L.b; n[5] = L.c; n[6] = L.d;
+      n[7] = R.a; n[8] = R.b; n[9] = R.c; n[10] = R.d;
+      n[11] = b0; n[12] = b1;
+    }
+    __syncthreads();
+  }
+  if (t == 0 && h > 0) {
+    double* n = cr;
+    M2 Di = m2_inv({n[0], n[2], n[2], n[1]});
+    double b0 = n[11], b1 = n[12];
+    n[11] = Di.a * b0 + Di.b * b1;
+    n[12] = Di.c * b0 + Di.d * b1;
+  }
+  __syncthreads();
+  for (int s = top >> 1; s >= 1; s >>= 1) {
+    for (int i = s + t * 2 * s; i < h; i += nt * 2 * s) {
+      double* n = cr + (size_t)i * kCrStride;
+      double d0, d1, d2, b0, b1;
+      M2 L, R;
+      cr_load(n, d0, d1, d2, L, R, b0, b1);
+      const double* l = cr + (size_t)(i - s) * kCrStride;
+      b0 -= L.a * l[11] + L.b * l[12];
+      b1 -= L.c * l[11] + L.d * l[12];
+      if (i + s < h) {
+        const double* r = cr + (size_t)(i + s) * kCrStride;
+        b0 -= R.a * r[11] + R.b * r[12];
+        b1 -= R.c * r[11] + R.d * r[12];
+      }
+      M2 Di = m2_inv({d0, d2, d2, d1});
+      n[11] = Di.a * b0 + Di.b * b1;
+      n[12] = Di.c * b0 + Di.d * b1;
+    }
+    __syncthreads();
+  }
+}
+
+// Standalone solve of a block-tridiagonal system given as diag (n x 3: xx yy xy), coupling
+// ((n-1) x 4: [[c0 c2] [c3 c1]] between block i and i+1) and rhs (n x 2) into x (n x 2), with
+// the caller's workspace cr (n x kCrStride doubles). One CTA.
+__global__ void __launch_bounds__(kSolveThreads) k_block_tridiag(int n, const double* __restrict__ diag,
+                                                                 const double* __restrict__ coupling,
+                                                                 const double* __restrict__ rhs,
+                                                                 double* __restrict__ x, double* __restrict__ cr) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double* q = cr + (size_t)i * kCrStride;
+    q[0] = diag[3 * i]; q[1] = diag[3 * i + 1]; q[2] = diag[3 * i + 2];
+    if (i > 0) {  // L_i = R_{i-1}^T
+      const double* c = coupling + 4 * (size_t)(i - 1);
+      q[3] = c[0]; q[4] = c[3]; q[5] = c[2]; q[6] = c[1];
+    } else {
+      q[3] = q[4] = q[5] = q[6] = 0.0;
+    }
+    if (i + 1 < n) {
+      const double* c = coupling + 4 * (size_t)i;
+      q[7] = c[0]; q[8] = c[2]; q[9] = c[3]; q[10] = c[1];
+    } else {
+      q[7] = q[8] = q[9] = q[10] = 0.0;
+    }
+    q[11] = rhs[2 * i];
+    q[12] = rhs[2 * i + 1];
+  }
+  __syncthreads();
+  cr_solve(cr, n);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    x[2 * i] = cr[(size_t)i * kCrStride + 11];
+    x[2 * i + 1] = cr[(size_t)i * kCrStride + 12];
+  }
+}
+
 // Knot-difference regulariser of frame f (extension; lambda = 0 reproduces the reference): sum of
 // |k_{t+1}-k_t|^2 over its W edges, own knots from own (+N for y), right boundary (bx, by).
 __device__ inline double frame_reg(const double* own, int W, int N, double bx, double by) {
@@ -243,74 +354,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
   }
   __syncthreads();
 
-  // (4) block cyclic reduction: at stride s the multiples of 2s absorb their odd-multiple neighbours
-  int top = 1;
-  while (top < h) top <<= 1;
-  for (int s = 1; s < h; s <<= 1) {
-    for (int j = t * 2 * s; j < h; j += nt * 2 * s) {
-      double* n = G.cr + (size_t)j * kCrStride;
-      double d0, d1, d2, b0, b1;
-      M2 L, R;
-      cr_load(n, d0, d1, d2, L, R, b0, b1);
-      M2 D = {d0, d2, d2, d1};
-      if (j - s >= 0) {
-        double e0, e1, e2, c0, c1;
-        M2 Ll, Rl;
-        cr_load(G.cr + (size_t)(j - s) * kCrStride, e0, e1, e2, Ll, Rl, c0, c1);
-        M2 Di = m2_inv({e0, e2, e2, e1});
-        M2 T = m2_mul(L, Di);
-        D = m2_sub(D, m2_mul(T, Rl));
-        b0 -= T.a * c0 + T.b * c1;
-        b1 -= T.c * c0 + T.d * c1;
-        L = m2_neg(m2_mul(T, Ll));
-      }
-      if (j + s < h) {
-        double e0, e1, e2, c0, c1;
-        M2 Lr, Rr;
-        cr_load(G.cr + (size_t)(j + s) * kCrStride, e0, e1, e2, Lr, Rr, c0, c1);
-        M2 Di = m2_inv({e0, e2, e2, e1});
-        M2 T = m2_mul(R, Di);
-        D = m2_sub(D, m2_mul(T, Lr));
-        b0 -= T.a * c0 + T.b * c1;
-        b1 -= T.c * c0 + T.d * c1;
-        R = m2_neg(m2_mul(T, Rr));
-      }
-      n[0] = D.a; n[1] = D.d; n[2] = 0.5 * (D.b + D.c);
-      n[3] = L.a; n[4] = L.b; n[5] = L.c; n[6] = L.d;
-      n[7] = R.a; n[8] = R.b; n[9] = R.c; n[10] = R.d;
-      n[11] = b0; n[12] = b1;
-    }
-    __syncthreads();
-  }
-  // back substitution, coarse to fine; x_i overwrites b_i
-  if (t == 0 && h > 0) {
-    double* n = G.cr;
-    M2 Di = m2_inv({n[0], n[2], n[2], n[1]});
-    double b0 = n[11], b1 = n[12];
-    n[11] = Di.a * b0 + Di.b * b1;
-    n[12] = Di.c * b0 + Di.d * b1;
-  }
-  __syncthreads();
-  for (int s = top >> 1; s >= 1; s >>= 1) {
-    for (int i = s + t * 2 * s; i < h; i += nt * 2 * s) {
-      double* n = G.cr + (size_t)i * kCrStride;
-      double d0, d1, d2, b0, b1;
-      M2 L, R;
-      cr_load(n, d0, d1, d2, L, R, b0, b1);
-      const double* l = G.cr + (size_t)(i - s) * kCrStride;
-      b0 -= L.a * l[11] + L.b * l[12];
-      b1 -= L.c * l[11] + L.d * l[12];
-      if (i + s < h) {
-        const double* r = G.cr + (size_t)(i + s) * kCrStride;
-        b0 -= R.a * r[11] + R.b * r[12];
-        b1 -= R.c * r[11] + R.d * r[12];
-      }
-      M2 Di = m2_inv({d0, d2, d2, d1});
-      n[11] = Di.a * b0 + Di.b * b1;
-      n[12] = Di.c * b0 + Di.d * b1;
-    }
-    __syncthreads();
-  }
+  // (4) FP64 block cyclic reduction
+  cr_solve(G.cr, h);
   // (5) compact step [x_0..x_h-1, y_0..y_h-1]
   for (int i = t; i < h; i += nt) {
     G.ndp[i] = G.cr[(size_t)i * kCrStride + 11];
@@ -349,106 +394,6 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
     bool fixed = (((idx + 1) - shift * half) % G.group_size) == 0;
     if (fixed) continue;
     G.delta_p[idx] = G.params_used[j] ? G.ndp[(idx >= N ? h : 0) + G.list[N + j]] : 0.0;
-  }
-}
-
-// Line-search decision for one frame per warp (task_linesearch.cu:95-149), after k_eval<kTrial>.
-__global__ void __launch_bounds__(256) k_ls_decide(const GroupDesc* __restrict__ gds, const int* __restrict__ frame_group,
-                                                   int n_frames_total, GroupCtl* __restrict__ ctl, int* __restrict__ n_search) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gf = blockIdx.x * 8 + warp;
-  if (gf >= n_frames_total) return;
-  const int g = frame_group[gf];
-  const GroupDesc& G = gds[g];
-  GroupCtl& C = ctl[g];
-  if (C.phase != kPhHalf) return;
-  const int f = gf - G.frame_base;
-  if (!(G.fstate[f] & 2)) return;
-  const int W = G.W, N = G.N, b0 = f * W, shift = C.shift;
-  double ssd = 0;
-  long long cnt = 0;
-  bool present = false;
-  for (int cc = lane; cc < W; cc += 32) {
-    ssd += G.colsum[(size_t)(b0 + cc) * kCsStride + kCsSsd];
-    int k = G.colcnt[b0 + cc];
-    cnt += k;
-    present |= k >= G.min_points[cc];
-  }
-  ssd = warp_sum(ssd);
-  cnt = (long long)warp_sum((int)cnt);
-  present = __any_sync(0xffffffffu, present);
-  const bool last = f + 1 == G.nF;
-  const double bx = last ? kPnewFill : G.p_snap[b0 + W], by = last ? kPnewFill : G.p_snap[N + b0 + W];
-  // the state the reference's buffers now hold: x, y, mask from this trial; the difference image
-  // only if the trial had a block present
-  double* km = G.kmask + (size_t)f * 2 * (W + 1);
-  double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
-  for (int cc = lane; cc <= W; cc += 32) {
-    double vx = cc < W ? G.p[b0 + cc] + G.delta_p[b0 + cc] : bx;
-    double vy = cc < W ? G.p[N + b0 + cc] + G.delta_p[N + b0 + cc] : by;
-    km[cc] = vx;
-    km[W + 1 + cc] = vy;
-    if (present) {
-      kd[cc] = vx;
-      kd[W + 1 + cc] = vy;
-    }
-  }
-  bool done = false;
-  const double thr = G.move_thresh, rho = G.ls_mult;
-  if (present) {
-    double ev = ssd / (double)cnt;
-    if (G.lambda != 0.0) {
-      double r = 0;
-      for (int cc = lane; cc < W; cc += 32) {
-        double x0 = G.p[b0 + cc] + G.delta_p[b0 + cc], y0 = G.p[N + b0 + cc] + G.delta_p[N + b0 + cc];
-        double x1 = cc + 1 < W ? G.p[b0 + cc + 1] + G.delta_p[b0 + cc + 1] : G.p_snap[b0 + W];
-        double y1 = cc + 1 < W ? G.p[N + b0 + cc + 1] + G.delta_p[N + b0 + cc + 1] : G.p_snap[N + b0 + W];
-        r += (x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0);
-      }
-      ev = (ssd + G.lambda * warp_sum(r)) / (double)cnt;
-    }
-    if (ev < G.errval[shift * G.nF + f]) {
-      __syncwarp();
-      for (int cc = lane; cc < W; cc += 32) {
-        G.p[b0 + cc] = G.p[b0 + cc] + G.delta_p[b0 + cc];
-        G.p[N + b0 + cc] = G.p[N + b0 + cc] + G.delta_p[N + b0 + cc];
-      }
-      if (b0 == 0 && lane == 0) G.errval[shift * G.nF] = ev;  // only idx == 0 writes (task_linesearch.cu:135)
-      done = true;
-    } else {
-      bool moving = false;
-      for (int cc = lane; cc < W; cc += 32)
-        moving |= fabs(G.delta_p[b0 + cc]) > thr || fabs(G.delta_p[N + b0 + cc]) > thr;
-      moving = __any_sync(0xffffffffu, moving);
-      if (!moving) {
-        done = true;
-      } else {
-        for (int cc = lane; cc < W; cc += 32) {
-          G.delta_p[b0 + cc] *= rho;
-          G.delta_p[N + b0 + cc] *= rho;
-        }
-      }
-    }
-  } else {
-    bool moving = false;
-    for (int cc = lane; cc < W; cc += 32) {
-      double a = G.delta_p[b0 + cc] * rho, b = G.delta_p[N + b0 + cc] * rho;
-      G.delta_p[b0 + cc] = a;
-      G.delta_p[N + b0 + cc] = b;
-      moving |= fabs(a) > thr || fabs(b) > thr;
-    }
-    done = !__any_sync(0xffffffffu, moving);
-  }
-  if (lane == 0) {
-    int tr = ++G.ls_trials[f];
-    atomicAdd((unsigned long long*)&C.n_eval, 1ull);
-    atomicAdd((unsigned long long*)&C.passes[kTrial], 1ull);
-    if (!done && tr >= kTrialCap) {
-      done = true;
-      C.cap_hit = 1;
-    }
-    if (done) G.fstate[f] = 0;
-    else atomicAdd(n_search, 1);
   }
 }
 
