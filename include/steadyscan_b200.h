@@ -165,6 +165,21 @@ SS_API void ss_batch_destroy(ss_batch* batch);
 SS_API int ss_solve_block_tridiagonal(int32_t n, const double* diag, const double* coupling, const double* rhs,
                                       double* x, void* stream);
 
+/* ss_solve_block_tridiagonal without any device allocation; it has no counterpart in the
+ * reference. It is for callers that cannot allocate GPU memory while they run: an acquisition loop
+ * that aligns frames while the microscope streams, where cudaMalloc and cudaFree synchronize the
+ * device and stall the frames in flight, or a host application whose own allocator has already
+ * reserved the GPU's memory. The caller passes the same device buffers as to
+ * ss_solve_block_tridiagonal; the workspace is a fixed device array inside this library of
+ * 32768 blocks (3.4 MB, held by every GPU that loads the library until the process exits), so
+ * n > 32768 is rejected with SS_ERR_INVALID_ARGUMENT. The first call on a device looks up that
+ * array's device address, so make it before any stream capture. All calls share the one array
+ * per device: calls that overlap on the GPU (different streams or threads at the same time) race
+ * and corrupt each other's results; serialize them. Each call writes every part of the workspace
+ * it reads before reading it. */
+SS_API int ss_solve_block_tridiagonal_noalloc(int32_t n, const double* diag, const double* coupling,
+                                              const double* rhs, double* x, void* stream);
+
 /* Message of the calling thread's last error ("" if none). */
 SS_API const char* ss_last_error(void);
 

@@ -89,6 +89,9 @@ def load(build_if_missing: bool = True):
     lib.ss_solve_block_tridiagonal.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_void_p]
     lib.ss_solve_block_tridiagonal.restype = C.c_int
+    lib.ss_solve_block_tridiagonal_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                       C.c_void_p]
+    lib.ss_solve_block_tridiagonal_noalloc.restype = C.c_int
     _lib = lib
     return lib
 

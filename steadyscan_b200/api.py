@@ -193,6 +193,23 @@ def solve_block_tridiagonal(diag, coupling, rhs, stream: int = 0):
     return x
 
 
+def solve_block_tridiagonal_noalloc(diag, coupling, rhs, stream: int = 0):
+    """The same solve through ss_solve_block_tridiagonal_noalloc, which allocates no device memory:
+    its workspace is a fixed array inside the library (at most 32768 blocks). For callers that
+    cannot allocate while they run, e.g. a streaming acquisition loop in which cudaMalloc would
+    synchronize the device. Calls that overlap on the GPU race on that array."""
+    import torch
+    d = torch.as_tensor(diag, dtype=torch.float64, device="cuda").contiguous()
+    c = torch.as_tensor(coupling, dtype=torch.float64, device="cuda").contiguous()
+    b = torch.as_tensor(rhs, dtype=torch.float64, device="cuda").contiguous()
+    x = torch.empty_like(b)
+    lib = load()
+    torch.cuda.synchronize()
+    check(lib.ss_solve_block_tridiagonal_noalloc(d.shape[0], d.data_ptr(), c.data_ptr() if c.numel() else None,
+                                                 b.data_ptr(), x.data_ptr(), stream or None))
+    return x
+
+
 class Batch:
     """A prepared batch of groups (ss_batch_*): inputs resident on the device, runnable repeatedly."""
 

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -890,6 +891,65 @@ int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats) {
 }
 
 void* ss_batch_stream(const ss_batch* batch) { return batch ? batch->b.stream() : nullptr; }
+
+}  // extern "C"
+
+namespace ss {
+
+// Workspace of ss_solve_block_tridiagonal_noalloc: the cyclic-reduction nodes of up to
+// kNoAllocMaxBlocks blocks (3.4 MB). It is file-scope device memory, so every GPU that loads this
+// library holds it until the process exits. Its host-side name is only a handle; the device
+// address comes from cudaGetSymbolAddress, looked up once per device below.
+constexpr int kNoAllocMaxBlocks = 32768;
+static __device__ __align__(256) double g_noalloc_work[(size_t)kNoAllocMaxBlocks * kCrStride];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_addr[128];  // per device ordinal
+
+// Device address of g_noalloc_work on the current device, looked up on the first call per device.
+static int noalloc_workspace(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= 128) return fail(SS_ERR_NO_DEVICE, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    double* p = nullptr;
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_work);
+    if (e != cudaSuccess || !p)
+      return fail(SS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return SS_OK;
+}
+
+}  // namespace ss
+
+extern "C" {
+
+int ss_solve_block_tridiagonal_noalloc(int32_t n, const double* diag, const double* coupling, const double* rhs,
+                                       double* x, void* stream) {
+  if (n < 1 || !diag || !rhs || !x || (n > 1 && !coupling))
+    return ss::fail(SS_ERR_INVALID_ARGUMENT, "ss_solve_block_tridiagonal_noalloc: bad arguments");
+  if (n > ss::kNoAllocMaxBlocks)
+    return ss::fail(SS_ERR_INVALID_ARGUMENT, "ss_solve_block_tridiagonal_noalloc: n = " + std::to_string(n) +
+                                                 " exceeds the fixed workspace of " +
+                                                 std::to_string(ss::kNoAllocMaxBlocks) + " blocks");
+  double* work = nullptr;
+  int rc = ss::noalloc_workspace(&work);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // every node of the workspace that the solve reads is written first by k_block_tridiag
+  ss::k_block_tridiag<<<1, ss::kSolveThreads, 0, s>>>(n, diag, coupling, rhs, x, work);
+  cudaError_t e = cudaGetLastError();
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return ss::fail(SS_ERR_CUDA, std::string("ss_solve_block_tridiagonal_noalloc: ") +
+                                     cudaGetErrorString(e != cudaSuccess ? e : e2));
+  ss::g_err.clear();
+  return SS_OK;
+}
 
 int ss_solve_block_tridiagonal(int32_t n, const double* diag, const double* coupling, const double* rhs, double* x,
                                void* stream) {
