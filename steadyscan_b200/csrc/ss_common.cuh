@@ -78,6 +78,11 @@ struct GroupDesc {
   const float* frac_f;      // FP32 copies for precision 'S'
   const float* basex_f;
   const float* basey_f;
+  // Affine geometry (precision 'S'; geo_k == 0: use the tables). Row r of block column cc holds
+  // line cc*k + l, pixel j of that line (l = r mod k, j = r div k), with
+  // basex = geo_ax*j + geo_bx, basey = geo_ay*(cc*k + l) + geo_by, tfrac = (l*L + j + 1/2) * geo_fs.
+  int geo_k, geo_L;
+  float geo_ax, geo_bx, geo_ay, geo_by, geo_fs;
   const uint8_t* base_mask;
   const int* min_points;    // W
   const void* image;        // Hb x fW column-major, engine frame type

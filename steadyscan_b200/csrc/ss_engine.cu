@@ -269,6 +269,8 @@ struct HostGroup {
   std::vector<double> p0, templ, xg, yg, frac, bx, by;
   std::vector<float> frac_f, bx_f, by_f;  // precision 'S' geometry
   int frames_per_cta = 32;
+  int geo_k = 0, geo_L = 0;               // affine geometry (0: tables)
+  double geo_ax = 0, geo_bx = 0, geo_ay = 0, geo_by = 0, geo_fs = 0;
   std::vector<uint8_t> bmask;
   std::vector<int32_t> minp;
   const void* frames_dev = nullptr;  // caller device pointer when bm_data is on the device
@@ -281,6 +283,8 @@ struct HostGroup {
   double* d_p0 = nullptr;
   void* d_image = nullptr;
 };
+
+static void detect_affine_geometry(HostGroup& g);
 
 static int validate_group(const ss_inputs* in, HostGroup& g) {
   if (!in) return fail(SS_ERR_INVALID_ARGUMENT, "inputs is NULL");
@@ -384,9 +388,47 @@ static int load_host_inputs(HostGroup& g) {
   for (int c = 1; c < g.W && g.frac_uniform; c++)
     for (int r = 0; r < g.Hb; r++)
       if (std::memcmp(&g.frac[(size_t)c * g.Hb + r], &g.frac[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
+  if (g.compute == 1 && g.frac_uniform) detect_affine_geometry(g);
   g.frame_bytes = (size_t)g.Hb * g.fW * dtype_size(g.frame_dt);
   if (in->bm_data.location == SS_DEVICE) g.frames_dev = in->bm_data.data;
   return SS_OK;
+}
+
+// Recognises the geometry that steady_scan.m:787-827 builds for unidirectional scanning with an
+// integer number of lines per knot dividing 32 and no cropping: block row r = j*k + l is pixel j
+// of line cc*k + l, basex and basey are affine in j and in the line, and tfrac = (l*L + j + 1/2) /
+// (k*L). Every table entry is checked; any mismatch keeps the tables.
+static void detect_affine_geometry(HostGroup& g) {
+  g.geo_k = 0;
+  const int Hb = g.Hb, W = g.W;
+  for (int k = 1; k <= 32; k <<= 1) {
+    if (Hb % k) continue;
+    const int L = Hb / k;
+    if (L < 2 || (k > 1 && W < 1)) continue;
+    const double fs = 1.0 / ((double)k * L);
+    const double bx0 = g.bx[0], ax = g.bx[k] - g.bx[0];
+    const double by0 = g.by[0];
+    const double ay = (k > 1) ? g.by[1] - g.by[0] : (W > 1 ? g.by[Hb] - g.by[0] : 1.0);
+    bool ok = true;
+    for (int cc = 0; cc < W && ok; cc++)
+      for (int r = 0; r < Hb; r++) {
+        const int l = r % k, j = r / k;
+        const size_t i = (size_t)cc * Hb + r;
+        const double f = ((double)l * L + j + 0.5) * fs;
+        const double x = ax * j + bx0, y = ay * ((double)cc * k + l) + by0;
+        auto near = [](double a, double b) { return std::fabs(a - b) <= 1e-9 * std::max(1.0, std::fabs(b)); };
+        if (!g.bmask[i] || !near(f, g.frac[i]) || !near(x, g.bx[i]) || !near(y, g.by[i])) {
+          ok = false;
+          break;
+        }
+      }
+    if (ok) {
+      g.geo_k = k;
+      g.geo_L = L;
+      g.geo_ax = ax; g.geo_bx = bx0; g.geo_ay = ay; g.geo_by = by0; g.geo_fs = fs;
+      return;
+    }
+  }
 }
 
 // Arena carving: every sub-buffer 256-byte aligned.
@@ -482,6 +524,10 @@ static void layout(Batch::Impl* b, char* base) {
     G.group_size = g.group_size; G.n_rg = g.n_rg;
     G.tile_base = b->n_tiles;
     G.frames_per_cta = g.frames_per_cta;
+    G.geo_k = g.geo_k;
+    G.geo_L = g.geo_L;
+    G.geo_ax = (float)g.geo_ax; G.geo_bx = (float)g.geo_bx; G.geo_ay = (float)g.geo_ay; G.geo_by = (float)g.geo_by;
+    G.geo_fs = (float)g.geo_fs;
     b->n_tiles += g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
     b->max_hb = std::max(b->max_hb, g.Hb);
     G.frame_base = b->n_frames_total;

@@ -194,21 +194,31 @@ __host__ __device__ constexpr int nsums(int mode) {
 // Evaluates one block column with one warp and returns the warp-reduced sums (all lanes) and the
 // valid-pixel count. coli is the column's offset in the frame data; mask_out (kFinal) receives the
 // reference's mask output.
-template <class Acc, class FrameT, class TplT, int MODE>
+template <class Acc, class FrameT, class TplT, int MODE, bool AFFINE = false>
 __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, const ColGeo<Acc>& geo,
                                             const ColKnots<Acc>& k, double (&out)[kCsStride], int& cnt_out,
-                                            uint8_t* mask_out) {
+                                            uint8_t* mask_out, int cc = 0) {
   const int lane = threadIdx.x & 31;
   const int Hb = G.Hb;
   const Acc tw = Limits<Acc>::lim(G.Wt), th = Limits<Acc>::lim(G.Ht);
   const Acc one = (Acc)1;
-  const bool split_fn = geo.fnext != geo.frac;
+  const bool split_fn = AFFINE ? false : geo.fnext != geo.frac;
   constexpr int NS = nsums(MODE);
   Acc s[NS];
 #pragma unroll
   for (int i = 0; i < NS; i++) s[i] = (Acc)0;
   int cnt = 0;
   bool run = true;  // leading run of valid pixels (task_correlation.cu:24-34)
+  // affine geometry: the lane's line offset l is fixed (k divides 32) and its pixel index j
+  // advances by 32/k per row step
+  Acc a_j = 0, a_dj = 0, a_f0 = 0, a_by = 0;
+  if (AFFINE) {
+    const int l = lane % G.geo_k;
+    a_j = (Acc)(lane / G.geo_k);
+    a_dj = (Acc)(32 / G.geo_k);
+    a_f0 = ((Acc)(l * G.geo_L) + (Acc)0.5) * (Acc)G.geo_fs;
+    a_by = fma((Acc)G.geo_ay, (Acc)(cc * G.geo_k + l), (Acc)G.geo_by);
+  }
 
 #pragma unroll 2
   for (int r0 = 0; r0 < Hb; r0 += 32) {
@@ -216,7 +226,13 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
     const bool in = r < Hb;
     Acc f = 0, bxv = 0, byv = 0;
     bool bm = false;
-    if (in) {
+    if (AFFINE) {
+      f = fma((Acc)G.geo_fs, a_j, a_f0);
+      bxv = fma((Acc)G.geo_ax, a_j, (Acc)G.geo_bx);
+      byv = a_by;
+      bm = in;
+      a_j += a_dj;
+    } else if (in) {
       f = geo.frac[r];
       bxv = geo.bx[r];
       byv = geo.by[r];
@@ -327,7 +343,8 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
   const int warp = threadIdx.x >> 5;
 
   ColGeo<Acc> geo = global_geo<Acc>(G, cc);
-  if (Hb <= stage_rows) {
+  const bool affine = sizeof(Acc) == 4 && G.geo_k > 0;
+  if (!affine && Hb <= stage_rows) {
     Acc* sf = reinterpret_cast<Acc*>(smem);
     Acc* sx = sf + Hb;
     Acc* sy = sx + Hb;
@@ -365,7 +382,13 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
     const size_t coli = (size_t)c * Hb;
     double out[kCsStride];
     int cnt;
-    eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, G.o_mask ? G.o_mask + coli : nullptr);
+    uint8_t* mo = G.o_mask ? G.o_mask + coli : nullptr;
+    if constexpr (sizeof(Acc) == 4) {
+      if (affine) eval_column<Acc, FrameT, TplT, MODE, true>(G, coli, geo, k, out, cnt, mo, cc);
+      else eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, mo);
+    } else {
+      eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, mo);
+    }
     if ((threadIdx.x & 31) == 0) {
       double* dst = G.colsum + (size_t)c * kCsStride;
 #pragma unroll
@@ -446,7 +469,15 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
       set_knots(k, x0, x1, y0, y1, x0, x1, y0, y1);
       double out[kCsStride];
       int c;
-      eval_column<Acc, FrameT, TplT, kTrial>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      if constexpr (sizeof(Acc) == 4) {
+        if (G.geo_k > 0)
+          eval_column<Acc, FrameT, TplT, kTrial, true>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c,
+                                                       nullptr, t);
+        else
+          eval_column<Acc, FrameT, TplT, kTrial>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      } else {
+        eval_column<Acc, FrameT, TplT, kTrial>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      }
       ssd += out[kCsSsd];
       cnt += c;
       present |= c >= G.min_points[t];
@@ -559,7 +590,15 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
                 s_kd[1][i + 1]);
       double out[kCsStride];
       int c;
-      eval_column<Acc, FrameT, TplT, kCorr>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      if constexpr (sizeof(Acc) == 4) {
+        if (G.geo_k > 0)
+          eval_column<Acc, FrameT, TplT, kCorr, true>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c,
+                                                      nullptr, t);
+        else
+          eval_column<Acc, FrameT, TplT, kCorr>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      } else {
+        eval_column<Acc, FrameT, TplT, kCorr>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+      }
       if (lane == 0) {
         double* dst = G.colsum + (size_t)(b0 + t) * kCsStride;
         for (int q = 0; q < nsums(kCorr); q++) dst[q] = out[q];

@@ -103,6 +103,21 @@ def test_precision_s_within_bound():
     assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([o["dx"], o["dy"]])) <= KNOT_RMS_S
 
 
+def test_precision_s_affine_and_table_geometry_agree():
+    """Precision S computes the default scan geometry in registers when the tables are affine; a
+    1e-7 px perturbation of basex forces the table path. Both stay within the bound of FP64."""
+    args, _, _ = make_args(frame_dtype=np.uint16, seed=13)
+    o = oracle.align_group(args)
+    args["flags"] = "S"
+    g_aff = api.align_group(args)
+    t = dict(args)
+    t["basex"] = args["basex"] + 1e-7
+    g_tab = api.align_group(t)
+    ref = np.concatenate([o["dx"], o["dy"]])
+    for g in (g_aff, g_tab):
+        assert knot_rms(np.concatenate([g["dx"], g["dy"]]), ref) <= KNOT_RMS_S
+
+
 def test_batched_equals_single():
     """Ragged groups in one batched run give the same results as one call each."""
     specs = [dict(seed=31), dict(n_frames=3, seed=32), dict(nlines=24, linewidth=20, nknots=7, seed=33),
