@@ -44,7 +44,16 @@ class DeviceMatrix:
         self.ptr, self.rows, self.cols, self.dtype, self.owner = int(ptr), int(rows), int(cols), int(dtype), owner
 
 
-def _matrix(a, keep: list) -> SSMatrix:
+def _matrix(a, keep: list, memo: dict | None = None) -> SSMatrix:
+    """ss_matrix of ``a``; with ``memo`` the same Python object maps to the same buffer, so groups
+    that share an argument share it in the library too."""
+    if memo is not None:
+        hit = memo.get(id(a))
+        if hit is not None and hit[0] is a:
+            return hit[1]
+        m = _matrix(a, keep)
+        memo[id(a)] = (a, m)
+        return m
     if isinstance(a, DeviceMatrix):
         return SSMatrix(a.ptr, a.rows, a.cols, a.dtype, SS_DEVICE)
     if hasattr(a, "is_cuda") and a.is_cuda:  # torch tensor in column-major memory order
@@ -71,19 +80,21 @@ def _matrix(a, keep: list) -> SSMatrix:
     return SSMatrix(arr.ctypes.data, arr.shape[0], arr.shape[1], _NP_DTYPE[arr.dtype], SS_HOST)
 
 
-def _inputs(args: dict, template_storage=None):
+def _inputs(args: dict, template_storage=None, memo: dict | None = None):
     keep: list = []
     flags = args["flags"].encode() if isinstance(args["flags"], str) else bytes(args["flags"])
     keep.append(flags)
     ts = {None: 0, "f32": SS_F32, "f16": SS_F16, np.float32: SS_F32, np.float16: SS_F16}.get(template_storage,
                                                                                           template_storage)
+    mp = args["min_points_per_block"]
     i = SSInputs(
         flags,
-        _matrix(args["template_image"], keep), _matrix(args["xgrad"], keep), _matrix(args["ygrad"], keep),
-        _matrix(args["tfrac"], keep), _matrix(args["basex"], keep), _matrix(args["basey"], keep),
-        _matrix(args["base_mask"], keep), _matrix(args["bmData"], keep), _matrix(args["est_dx_knots"], keep),
-        _matrix(args["est_dy_knots"], keep), int(args["group_size"]), int(args["nFrames"]),
-        _matrix(np.asarray(args["min_points_per_block"]).reshape(-1), keep), int(args["max_iter"]),
+        _matrix(args["template_image"], keep, memo), _matrix(args["xgrad"], keep, memo),
+        _matrix(args["ygrad"], keep, memo), _matrix(args["tfrac"], keep, memo), _matrix(args["basex"], keep, memo),
+        _matrix(args["basey"], keep, memo), _matrix(args["base_mask"], keep, memo), _matrix(args["bmData"], keep),
+        _matrix(args["est_dx_knots"], keep), _matrix(args["est_dy_knots"], keep), int(args["group_size"]),
+        int(args["nFrames"]), _matrix(mp if np.ndim(mp) == 1 else np.asarray(mp).reshape(-1), keep, memo),
+        int(args["max_iter"]),
         float(args["move_thresh"]), float(args["halt_correlation"]), float(args["correlation_increase_threshold"]),
         float(args["filter_strength"]), int(args["max_filter_iterations"]),
         float(args["filter_deactivation_threshold"]), float(args.get("lambda", 0.0)),
@@ -139,8 +150,9 @@ def align_groups(groups: list, want_mask: bool = True, want_history: bool = Fals
     ins = (SSInputs * n)()
     outs = (SSOutputs * n)()
     keep, arrays, dims = [], [], []
+    memo: dict = {}
     for k, g in enumerate(groups):
-        i, kk = _inputs(g, template_storage)
+        i, kk = _inputs(g, template_storage, memo)
         ins[k] = i
         keep.append(kk)
         o, a, d = _outputs(g, want_mask, want_history)
@@ -220,8 +232,9 @@ class Batch:
         self._ins = (SSInputs * n)()
         self._outs = (SSOutputs * n)()
         self._keep, self._arrays, self._dims = [], [], []
+        memo: dict = {}
         for k, g in enumerate(groups):
-            i, kk = _inputs(g, template_storage)
+            i, kk = _inputs(g, template_storage, memo)
             self._ins[k] = i
             self._keep.append(kk)
             o, a, d = _outputs(g, want_mask, want_history)

@@ -269,6 +269,7 @@ struct HostGroup {
   std::vector<double> p0, templ, xg, yg, frac, bx, by;
   std::vector<float> frac_f, bx_f, by_f;  // precision 'S' geometry
   int frames_per_cta = 32;
+  int tpl_src = -1, geo_src = -1;         // earlier group whose template / geometry buffers are shared
   int geo_k = 0, geo_L = 0;               // affine geometry (0: tables)
   double geo_ax = 0, geo_bx = 0, geo_ay = 0, geo_by = 0, geo_fs = 0;
   std::vector<uint8_t> bmask;
@@ -337,22 +338,49 @@ static int validate_group(const ss_inputs* in, HostGroup& g) {
   return SS_OK;
 }
 
-static int load_host_inputs(HostGroup& g) {
+static bool same_matrix(const ss_matrix& a, const ss_matrix& b) {
+  return a.data == b.data && a.rows == b.rows && a.cols == b.cols && a.dtype == b.dtype && a.location == b.location;
+}
+
+// Groups that pass the same host buffers for template and gradients, or for the scan geometry,
+// share one conversion and one device copy (typically all sets of one recording).
+static void find_shared_inputs(std::vector<HostGroup>& hg) {
+  for (size_t i = 0; i < hg.size(); i++) {
+    const ss_inputs* a = hg[i].in;
+    for (size_t j = 0; j < i; j++) {
+      const ss_inputs* b = hg[j].in;
+      if (hg[i].tpl_src < 0 && hg[j].tpl_src < 0 && same_matrix(a->template_image, b->template_image) &&
+          same_matrix(a->xgrad, b->xgrad) && same_matrix(a->ygrad, b->ygrad))
+        hg[i].tpl_src = (int)j;
+      if (hg[i].geo_src < 0 && hg[j].geo_src < 0 && same_matrix(a->tfrac, b->tfrac) &&
+          same_matrix(a->basex, b->basex) && same_matrix(a->basey, b->basey) &&
+          same_matrix(a->base_mask, b->base_mask) && same_matrix(a->min_points_per_block, b->min_points_per_block))
+        hg[i].geo_src = (int)j;
+    }
+  }
+}
+
+static int load_host_inputs(std::vector<HostGroup>& all, size_t gi) {
+  HostGroup& g = all[gi];
   const ss_inputs* in = g.in;
   int rc;
-  if ((rc = host_doubles(in->template_image, "template_image", g.templ))) return rc;
-  if ((rc = host_doubles(in->xgrad, "xgrad", g.xg))) return rc;
-  if ((rc = host_doubles(in->ygrad, "ygrad", g.yg))) return rc;
-  if ((rc = host_doubles(in->tfrac, "tfrac", g.frac))) return rc;
-  if ((rc = host_doubles(in->basex, "basex", g.bx))) return rc;
-  if ((rc = host_doubles(in->basey, "basey", g.by))) return rc;
+  if (g.tpl_src < 0) {
+    if ((rc = host_doubles(in->template_image, "template_image", g.templ))) return rc;
+    if ((rc = host_doubles(in->xgrad, "xgrad", g.xg))) return rc;
+    if ((rc = host_doubles(in->ygrad, "ygrad", g.yg))) return rc;
+  }
   std::vector<double> tmp;
-  if ((rc = host_doubles(in->base_mask, "base_mask", tmp))) return rc;
-  g.bmask.resize(tmp.size());
-  for (size_t i = 0; i < tmp.size(); i++) g.bmask[i] = tmp[i] != 0.0;
-  if ((rc = host_doubles(in->min_points_per_block, "min_points_per_block", tmp))) return rc;
-  g.minp.resize(g.W);
-  for (int i = 0; i < g.W; i++) g.minp[i] = (int32_t)tmp[i];  // static_cast<int> (mexconverter.cpp:97)
+  if (g.geo_src < 0) {
+    if ((rc = host_doubles(in->tfrac, "tfrac", g.frac))) return rc;
+    if ((rc = host_doubles(in->basex, "basex", g.bx))) return rc;
+    if ((rc = host_doubles(in->basey, "basey", g.by))) return rc;
+    if ((rc = host_doubles(in->base_mask, "base_mask", tmp))) return rc;
+    g.bmask.resize(tmp.size());
+    for (size_t i = 0; i < tmp.size(); i++) g.bmask[i] = tmp[i] != 0.0;
+    if ((rc = host_doubles(in->min_points_per_block, "min_points_per_block", tmp))) return rc;
+    g.minp.resize(g.W);
+    for (int i = 0; i < g.W; i++) g.minp[i] = (int32_t)tmp[i];  // static_cast<int> (mexconverter.cpp:97)
+  }
   std::vector<double> ex, ey;
   if ((rc = host_doubles(in->est_dx_knots, "est_dx_knots", ex))) return rc;
   if ((rc = host_doubles(in->est_dy_knots, "est_dy_knots", ey))) return rc;
@@ -372,23 +400,34 @@ static int load_host_inputs(HostGroup& g) {
       g.p0[j + g.N] = ey[(size_t)f * (g.W + 1) + g.W];
     }
   }
-  // gradients that are exactly the template's forward differences are re-derived on the device
-  g.grad_derived = true;
-  for (int c = 0; c + 1 < g.Wt && g.grad_derived; c++)
-    for (int r = 0; r < g.Ht; r++) {
-      double d = g.templ[(size_t)(c + 1) * g.Ht + r] - g.templ[(size_t)c * g.Ht + r];
-      if (!(g.xg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
-    }
-  for (int c = 0; c < g.Wt && g.grad_derived; c++)
-    for (int r = 0; r + 1 < g.Ht; r++) {
-      double d = g.templ[(size_t)c * g.Ht + r + 1] - g.templ[(size_t)c * g.Ht + r];
-      if (!(g.yg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
-    }
-  g.frac_uniform = true;
-  for (int c = 1; c < g.W && g.frac_uniform; c++)
-    for (int r = 0; r < g.Hb; r++)
-      if (std::memcmp(&g.frac[(size_t)c * g.Hb + r], &g.frac[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
-  if (g.compute == 1 && g.frac_uniform) detect_affine_geometry(g);
+  if (g.tpl_src < 0) {
+    // gradients that are exactly the template's forward differences are re-derived on the device
+    g.grad_derived = true;
+    for (int c = 0; c + 1 < g.Wt && g.grad_derived; c++)
+      for (int r = 0; r < g.Ht; r++) {
+        double d = g.templ[(size_t)(c + 1) * g.Ht + r] - g.templ[(size_t)c * g.Ht + r];
+        if (!(g.xg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
+      }
+    for (int c = 0; c < g.Wt && g.grad_derived; c++)
+      for (int r = 0; r + 1 < g.Ht; r++) {
+        double d = g.templ[(size_t)c * g.Ht + r + 1] - g.templ[(size_t)c * g.Ht + r];
+        if (!(g.yg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
+      }
+  } else {
+    g.grad_derived = all[g.tpl_src].grad_derived;
+  }
+  if (g.geo_src < 0) {
+    g.frac_uniform = true;
+    for (int c = 1; c < g.W && g.frac_uniform; c++)
+      for (int r = 0; r < g.Hb; r++)
+        if (std::memcmp(&g.frac[(size_t)c * g.Hb + r], &g.frac[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
+    if (g.compute == 1 && g.frac_uniform) detect_affine_geometry(g);
+  } else {
+    const HostGroup& s = all[g.geo_src];
+    g.frac_uniform = s.frac_uniform;
+    g.geo_k = s.geo_k; g.geo_L = s.geo_L;
+    g.geo_ax = s.geo_ax; g.geo_bx = s.geo_bx; g.geo_ay = s.geo_ay; g.geo_by = s.geo_by; g.geo_fs = s.geo_fs;
+  }
   g.frame_bytes = (size_t)g.Hb * g.fW * dtype_size(g.frame_dt);
   if (in->bm_data.location == SS_DEVICE) g.frames_dev = in->bm_data.data;
   return SS_OK;
@@ -541,26 +580,38 @@ static void layout(Batch::Impl* b, char* base) {
     G.ls_mult = in->linesearch_reduction_multiplier;
     const size_t hbw = (size_t)g.Hb * g.W, npx = (size_t)g.Hb * g.fW, N = g.N, nF = g.nF;
     const size_t nq = (size_t)(g.Ht - 1) * (g.Wt - 1);
-    G.frac = cv.take<double>(hbw);
-    G.basex = cv.take<double>(hbw);
-    G.basey = cv.take<double>(hbw);
-    if (b->compute == 1) {
-      G.frac_f = cv.take<float>(hbw);
-      G.basex_f = cv.take<float>(hbw);
-      G.basey_f = cv.take<float>(hbw);
+    if (g.geo_src >= 0) {  // shared with an earlier group
+      const GroupDesc& S = gd[g.geo_src];
+      G.frac = S.frac; G.basex = S.basex; G.basey = S.basey;
+      G.frac_f = S.frac_f; G.basex_f = S.basex_f; G.basey_f = S.basey_f;
+      G.base_mask = S.base_mask; G.min_points = S.min_points;
     } else {
-      G.frac_f = G.basex_f = G.basey_f = nullptr;
+      G.frac = cv.take<double>(hbw);
+      G.basex = cv.take<double>(hbw);
+      G.basey = cv.take<double>(hbw);
+      if (b->compute == 1) {
+        G.frac_f = cv.take<float>(hbw);
+        G.basex_f = cv.take<float>(hbw);
+        G.basey_f = cv.take<float>(hbw);
+      } else {
+        G.frac_f = G.basex_f = G.basey_f = nullptr;
+      }
+      G.base_mask = cv.take<uint8_t>(hbw);
+      G.min_points = cv.take<int>(g.W);
     }
-    G.base_mask = cv.take<uint8_t>(hbw);
-    G.min_points = cv.take<int>(g.W);
     g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
     G.image = g.frames_dev ? g.frames_dev : g.d_image;
-    G.tquad = cv.take<char>(nq * 4 * tsz);
-    G.gquad = g.grad_derived ? nullptr : cv.take<char>(nq * 4 * tsz);
-    g.d_templ_stage = cv.take<double>((size_t)g.Ht * g.Wt);
-    if (!g.grad_derived) {
-      g.d_xg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
-      g.d_yg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+    if (g.tpl_src >= 0) {
+      G.tquad = gd[g.tpl_src].tquad;
+      G.gquad = gd[g.tpl_src].gquad;
+    } else {
+      G.tquad = cv.take<char>(nq * 4 * tsz);
+      G.gquad = g.grad_derived ? nullptr : cv.take<char>(nq * 4 * tsz);
+      g.d_templ_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+      if (!g.grad_derived) {
+        g.d_xg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+        g.d_yg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
+      }
     }
     g.d_sum = cv.take<double>(1);
     G.sum_image = g.d_sum;
@@ -622,7 +673,10 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
           in[i].gpu_device_id != in[0].gpu_device_id)
         return fail(SS_ERR_INVALID_ARGUMENT, "all groups of a batch need the same precision, frame dtype and device");
     }
-    rc = load_host_inputs(b->hg[i]);
+  }
+  find_shared_inputs(b->hg);
+  for (int i = 0; i < n; i++) {
+    int rc = load_host_inputs(b->hg, i);
     if (rc) return rc;
   }
   b->compute = b->hg[0].compute;
@@ -659,29 +713,35 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     HostGroup& g = b->hg[i];
     GroupDesc& G = b->gd[i];
     const size_t hbw = (size_t)g.Hb * g.W;
-    SS_CK(cudaMemcpyAsync((void*)G.frac, g.frac.data(), hbw * 8, cudaMemcpyHostToDevice, s));
-    SS_CK(cudaMemcpyAsync((void*)G.basex, g.bx.data(), hbw * 8, cudaMemcpyHostToDevice, s));
-    SS_CK(cudaMemcpyAsync((void*)G.basey, g.by.data(), hbw * 8, cudaMemcpyHostToDevice, s));
-    if (b->compute == 1) {
-      g.frac_f.assign(g.frac.begin(), g.frac.end());
-      g.bx_f.assign(g.bx.begin(), g.bx.end());
-      g.by_f.assign(g.by.begin(), g.by.end());
-      SS_CK(cudaMemcpyAsync((void*)G.frac_f, g.frac_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
-      SS_CK(cudaMemcpyAsync((void*)G.basex_f, g.bx_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
-      SS_CK(cudaMemcpyAsync((void*)G.basey_f, g.by_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+    if (g.geo_src < 0) {
+      SS_CK(cudaMemcpyAsync((void*)G.frac, g.frac.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+      SS_CK(cudaMemcpyAsync((void*)G.basex, g.bx.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+      SS_CK(cudaMemcpyAsync((void*)G.basey, g.by.data(), hbw * 8, cudaMemcpyHostToDevice, s));
+      if (b->compute == 1) {
+        g.frac_f.assign(g.frac.begin(), g.frac.end());
+        g.bx_f.assign(g.bx.begin(), g.bx.end());
+        g.by_f.assign(g.by.begin(), g.by.end());
+        SS_CK(cudaMemcpyAsync((void*)G.frac_f, g.frac_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+        SS_CK(cudaMemcpyAsync((void*)G.basex_f, g.bx_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+        SS_CK(cudaMemcpyAsync((void*)G.basey_f, g.by_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+      }
+      SS_CK(cudaMemcpyAsync((void*)G.base_mask, g.bmask.data(), hbw, cudaMemcpyHostToDevice, s));
+      SS_CK(cudaMemcpyAsync((void*)G.min_points, g.minp.data(), g.W * 4, cudaMemcpyHostToDevice, s));
     }
-    SS_CK(cudaMemcpyAsync((void*)G.base_mask, g.bmask.data(), hbw, cudaMemcpyHostToDevice, s));
-    SS_CK(cudaMemcpyAsync((void*)G.min_points, g.minp.data(), g.W * 4, cudaMemcpyHostToDevice, s));
     if (!g.frames_dev)
       SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
-    SS_CK(cudaMemcpyAsync(g.d_templ_stage, g.templ.data(), g.templ.size() * 8, cudaMemcpyHostToDevice, s));
-    if (!g.grad_derived) {
-      SS_CK(cudaMemcpyAsync(g.d_xg_stage, g.xg.data(), g.xg.size() * 8, cudaMemcpyHostToDevice, s));
-      SS_CK(cudaMemcpyAsync(g.d_yg_stage, g.yg.data(), g.yg.size() * 8, cudaMemcpyHostToDevice, s));
-    }
     SS_CK(cudaMemcpyAsync(g.d_p0, g.p0.data(), g.p0.size() * 8, cudaMemcpyHostToDevice, s));
+    if (g.tpl_src < 0) {
+      SS_CK(cudaMemcpyAsync(g.d_templ_stage, g.templ.data(), g.templ.size() * 8, cudaMemcpyHostToDevice, s));
+      if (!g.grad_derived) {
+        SS_CK(cudaMemcpyAsync(g.d_xg_stage, g.xg.data(), g.xg.size() * 8, cudaMemcpyHostToDevice, s));
+        SS_CK(cudaMemcpyAsync(g.d_yg_stage, g.yg.data(), g.yg.size() * 8, cudaMemcpyHostToDevice, s));
+      }
+    }
     const int nb = 148 * 4;
-    if (b->tpl_dt == SS_F64) {
+    if (g.tpl_src >= 0) {
+      // template quads shared with an earlier group
+    } else if (b->tpl_dt == SS_F64) {
       k_build_tquad<double><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (double*)G.tquad);
       if (!g.grad_derived)
         k_build_gquad<double><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (double*)G.gquad);

@@ -324,6 +324,72 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
   for (int i = 0; i < NS; i++) out[i] = warp_sum((double)s[i]);
 }
 
+// Trial SSD and valid count of up to NC block columns of one frame with one warp, their rows
+// interleaved so that the frame loads and template gathers of all columns are in flight together.
+// Loads are predicated by index clamping (a masked pixel reads row 0 / quad 0 and is discarded), so
+// the column loop has no divergent branches. tq: frame-local column indices, nq <= NC of them valid.
+template <class Acc, class FrameT, class TplT, bool AFFINE, int NC>
+__device__ __forceinline__ void trial_columns(const GroupDesc& G, int b0, const int (&tq)[NC], int nq,
+                                              const Acc (&qx0)[NC], const Acc (&qx1)[NC], const Acc (&qy0)[NC],
+                                              const Acc (&qy1)[NC], double (&ssd)[NC], int (&cnt)[NC]) {
+  const int lane = threadIdx.x & 31;
+  const int Hb = G.Hb;
+  const Acc tw = Limits<Acc>::lim(G.Wt), th = Limits<Acc>::lim(G.Ht);
+  Acc s[NC];
+  int c[NC];
+  size_t coli[NC];
+  ColGeo<Acc> geo[NC];
+  Acc aby[NC];
+  Acc a_j = 0, a_dj = 0, a_f0 = 0;
+  if (AFFINE) {
+    const int l = lane % G.geo_k;
+    a_j = (Acc)(lane / G.geo_k);
+    a_dj = (Acc)(32 / G.geo_k);
+    a_f0 = ((Acc)(l * G.geo_L) + (Acc)0.5) * (Acc)G.geo_fs;
+#pragma unroll
+    for (int q = 0; q < NC; q++) aby[q] = fma((Acc)G.geo_ay, (Acc)(tq[q] * G.geo_k + l), (Acc)G.geo_by);
+  }
+#pragma unroll
+  for (int q = 0; q < NC; q++) {
+    s[q] = (Acc)0;
+    c[q] = 0;
+    coli[q] = (size_t)(b0 + tq[q]) * Hb;
+    if (!AFFINE) geo[q] = global_geo<Acc>(G, tq[q]);
+  }
+  for (int r0 = 0; r0 < Hb; r0 += 32) {
+    const int r = r0 + lane;
+    const bool in = r < Hb;
+    const int rr = in ? r : 0;
+    Acc fa = 0, bxa = 0;
+    if (AFFINE) {
+      fa = fma((Acc)G.geo_fs, a_j, a_f0);
+      bxa = fma((Acc)G.geo_ax, a_j, (Acc)G.geo_bx);
+      a_j += a_dj;
+    }
+#pragma unroll
+    for (int q = 0; q < NC; q++) {
+      if (q < nq) {
+        const Acc f = AFFINE ? fa : geo[q].frac[rr];
+        const Acc bx = AFFINE ? bxa : geo[q].bx[rr];
+        const Acc by = AFFINE ? aby[q] : geo[q].by[rr];
+        const bool bm = AFFINE ? in : (in && geo[q].bm[rr] != 0);
+        Acc x, y;
+        const bool m = warp_pixel<Acc>(qx0[q], qx1[q], qy0[q], qy1[q], f, bx, by, bm, tw, th, x, y);
+        const Acc img = ld_pixel<Acc, FrameT>(G.image, coli[q] + rr);
+        const Acc wI = sample<Acc, TplT, false>(G, m ? x : (Acc)0, m ? y : (Acc)0).wI;
+        const Acc d = img - wI;
+        s[q] = m ? fma(d, d, s[q]) : s[q];
+        c[q] += m ? 1 : 0;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NC; q++) {
+    ssd[q] = warp_sum((double)s[q]);
+    cnt[q] = warp_sum(c[q]);
+  }
+}
+
 // Assembly (at p) and final (at kmask) passes. A CTA takes one block column index cc of one group
 // and G.frames_per_cta of its frames, a warp per frame at a time; the column's geometry is staged in
 // shared memory once for all of them, and the frames share the template rows around the column in L1.
@@ -460,27 +526,36 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
     double ssd = 0, maxabs = 0, reg = 0;
     long long cnt = 0;
     bool present = false;
-    for (int t = lo + warp; t < hi; t += nw) {
-      const int i = t - lo;
-      const double x0 = s_p[0][i] + s_dp[0][i], y0 = s_p[1][i] + s_dp[1][i];
-      const double x1 = (t + 1 < W) ? s_p[0][i + 1] + s_dp[0][i + 1] : s_p[0][i + 1];
-      const double y1 = (t + 1 < W) ? s_p[1][i + 1] + s_dp[1][i + 1] : s_p[1][i + 1];
-      ColKnots<Acc> k;
-      set_knots(k, x0, x1, y0, y1, x0, x1, y0, y1);
-      double out[kCsStride];
-      int c;
-      if constexpr (sizeof(Acc) == 4) {
-        if (G.geo_k > 0)
-          eval_column<Acc, FrameT, TplT, kTrial, true>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c,
-                                                       nullptr, t);
-        else
-          eval_column<Acc, FrameT, TplT, kTrial>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
-      } else {
-        eval_column<Acc, FrameT, TplT, kTrial>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+    constexpr int NC = 4;
+    for (int t0 = lo + warp; t0 < hi; t0 += nw * NC) {
+      int tq[NC], nq = 0;
+      Acc qx0[NC], qx1[NC], qy0[NC], qy1[NC];
+#pragma unroll
+      for (int q = 0; q < NC; q++) {
+        int t = t0 + q * nw;
+        if (t >= hi) t = t0;  // padding column, not evaluated (nq excludes it)
+        else nq = q + 1;
+        const int i = t - lo;
+        tq[q] = t;
+        qx0[q] = (Acc)(s_p[0][i] + s_dp[0][i]);
+        qy0[q] = (Acc)(s_p[1][i] + s_dp[1][i]);
+        qx1[q] = (Acc)((t + 1 < W) ? s_p[0][i + 1] + s_dp[0][i + 1] : s_p[0][i + 1]);
+        qy1[q] = (Acc)((t + 1 < W) ? s_p[1][i + 1] + s_dp[1][i + 1] : s_p[1][i + 1]);
       }
-      ssd += out[kCsSsd];
-      cnt += c;
-      present |= c >= G.min_points[t];
+      double qs[NC];
+      int qc[NC];
+      bool aff = false;
+      if constexpr (sizeof(Acc) == 4) aff = G.geo_k > 0;
+      if (aff) trial_columns<Acc, FrameT, TplT, true, NC>(G, b0, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+      else trial_columns<Acc, FrameT, TplT, false, NC>(G, b0, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+#pragma unroll
+      for (int q = 0; q < NC; q++) {
+        if (q < nq) {
+          ssd += qs[q];
+          cnt += qc[q];
+          present |= qc[q] >= G.min_points[tq[q]];
+        }
+      }
     }
     for (int i = threadIdx.x; i < hi - lo; i += blockDim.x) {
       const int t = lo + i;

@@ -118,6 +118,32 @@ def test_precision_s_affine_and_table_geometry_agree():
         assert knot_rms(np.concatenate([g["dx"], g["dy"]]), ref) <= KNOT_RMS_S
 
 
+@pytest.mark.parametrize("flags", ["D", "S"])
+def test_batched_groups_sharing_template_and_geometry(flags):
+    """Sets of one recording pass the same template and geometry arrays; the library converts and
+    uploads them once and every set still gets its single-call result."""
+    args, _, _ = make_args(n_frames=12, seed=41, frame_dtype=np.uint16)
+    args["flags"] = flags
+    w = args["tfrac"].shape[1]
+    groups = []
+    for k in range(3):
+        a = dict(args)
+        a["bmData"] = np.asfortranarray(args["bmData"][:, k * 4 * w:(k + 1) * 4 * w])
+        a["nFrames"] = 4
+        a["est_dx_knots"] = args["est_dx_knots"][:, k * 4:(k + 1) * 4]
+        a["est_dy_knots"] = args["est_dy_knots"][:, k * 4:(k + 1) * 4]
+        groups.append(a)
+    batched = api.align_groups(groups)
+    for a, b in zip(groups, batched):
+        single = api.align_group(a)
+        assert single["iter_used"] == b["iter_used"]
+        np.testing.assert_array_equal(single["dx"], b["dx"])
+        np.testing.assert_array_equal(single["dy"], b["dy"])
+        np.testing.assert_array_equal(single["mask"], b["mask"])
+    if flags == "D":
+        _compare_d(groups[1], g=batched[1])
+
+
 def test_batched_equals_single():
     """Ragged groups in one batched run give the same results as one call each."""
     specs = [dict(seed=31), dict(n_frames=3, seed=32), dict(nlines=24, linewidth=20, nknots=7, seed=33),
