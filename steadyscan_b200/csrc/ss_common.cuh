@@ -83,6 +83,12 @@ struct GroupDesc {
   // basex = geo_ax*j + geo_bx, basey = geo_ay*(cc*k + l) + geo_by, tfrac = (l*L + j + 1/2) * geo_fs.
   int geo_k, geo_L;
   float geo_ax, geo_bx, geo_ay, geo_by, geo_fs;
+  // Precision 'S': the template as FP32 rows of tpitch floats (16-byte aligned rows) for staging
+  // row windows in shared memory, and per block column the [min, max] of basey over valid rows.
+  const float* tplain;
+  int tpitch;
+  const float* col_yrange;  // W x 2
+  int* err;                 // device error word of the batch (bit 0: a staging copy timed out)
   const uint8_t* base_mask;
   const int* min_points;    // W
   const void* image;        // Hb x fW column-major, engine frame type

@@ -57,6 +57,16 @@ __global__ void k_build_tquad(const double* __restrict__ T, int Ht, int Wt, TplT
   }
 }
 
+// FP32 template rows of `pitch` floats (zero padding) from the column-major FP64 template, the
+// source of the shared-memory row windows of precision 'S'.
+__global__ void k_build_tplain(const double* __restrict__ T, int Ht, int Wt, int pitch, float* __restrict__ out) {
+  const size_t n = (size_t)Ht * pitch;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int iy = (int)(i / pitch), ix = (int)(i % pitch);
+    out[i] = ix < Wt ? (float)T[(size_t)ix * Ht + iy] : 0.0f;
+  }
+}
+
 // Gradient quads (xg[iy][ix], xg[iy+1][ix], yg[iy][ix], yg[iy][ix+1]) for caller gradients that
 // are not the template's forward differences.
 template <class TplT>
@@ -97,29 +107,35 @@ __global__ void k_fill(double* p, size_t n, double v) {
 // Dynamic shared memory for staging one block column's geometry (tfrac, basex, basey, the next
 // column's tfrac and base_mask) in k_eval.
 constexpr int kStageBytes = 96 * 1024;
+// Shared memory for one template row window of precision 'S' (26 rows of a 512-pixel template):
+// four resident assembly CTAs per SM.
+constexpr int kWinBytes = 52 * 1024;
 
 using EvalFn = cudaError_t (*)(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
-                               const GroupCtl* ctl, int max_hb);
+                               const GroupCtl* ctl, int max_hb, int win_bytes);
 using LsFn = cudaError_t (*)(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl);
 using SumFn = void (*)(const void* img, size_t n, double* out, cudaStream_t s);
 
 template <class Acc, class FrameT, class TplT>
 static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
-                               const GroupCtl* ctl, int max_hb) {
+                               const GroupCtl* ctl, int max_hb, int win_bytes) {
   if (tiles <= 0) return cudaSuccess;
+  constexpr int kMaxDyn = kStageBytes + kWinBytes + 64;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kAssemble>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
-    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kAssemble>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
+    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
     attr_set = true;
   }
-  const size_t row_bytes = 4 * sizeof(Acc) + 1;
-  const int rows = (size_t)max_hb * row_bytes <= (size_t)kStageBytes ? max_hb : 0;
-  const size_t smem = (size_t)rows * row_bytes + 64;
+  const int rows = stage_bytes<Acc>(max_hb) <= (size_t)kStageBytes ? max_hb : 0;
+  if (sizeof(Acc) != 4) win_bytes = 0;
+  win_bytes = std::min(win_bytes, kWinBytes) & ~15;
+  // geometry staging (16-byte multiple), then the template window and its mbarrier
+  const size_t smem = (rows ? stage_bytes<Acc>(rows) : 0) + (win_bytes ? (size_t)win_bytes + 16 : 0) + 64;
   if (mode == kAssemble)
-    k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows);
+    k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
   else
-    k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows);
+    k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
   return cudaGetLastError();
 }
 
@@ -268,6 +284,7 @@ struct HostGroup {
   bool grad_derived = true, frac_uniform = true;
   std::vector<double> p0, templ, xg, yg, frac, bx, by;
   std::vector<float> frac_f, bx_f, by_f;  // precision 'S' geometry
+  std::vector<float> yrange;              // per block column [min, max] of basey over valid rows
   int frames_per_cta = 32;
   int tpl_src = -1, geo_src = -1;         // earlier group whose template / geometry buffers are shared
   int geo_k = 0, geo_L = 0;               // affine geometry (0: tables)
@@ -498,8 +515,11 @@ struct Batch::Impl {
   int* d_tile_group = nullptr;
   int* d_frame_group = nullptr;
   int* d_counters = nullptr;  // [0] searching frames, [1] finished groups
+  int* d_err = nullptr;       // device error word (bit 0: a shared-memory staging copy timed out)
+  int win_bytes = 0;          // template window bytes per assembly/final CTA (0: no windows)
   int* h_counters = nullptr;  // pinned
-  int n_tiles = 0, n_frames_total = 0, max_hb = 0;
+  int n_tiles = 0, n_frames_total = 0;
+  int max_hb = 0;  // largest block height among groups whose geometry k_eval stages in shared memory
   KernelSet ks = {nullptr, nullptr};
   SumFn sum = nullptr;
   std::vector<GroupCtl> h_ctl;
@@ -525,7 +545,7 @@ struct Batch::Impl {
       cudaEventRecord(events[event_used], stream);
     }
     if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl);
-    else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb);
+    else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb, win_bytes);
     launches++;
     if (timing) {
       cudaEventRecord(events[event_used + 1], stream);
@@ -556,6 +576,8 @@ static void layout(Batch::Impl* b, char* base) {
   b->n_frames_total = 0;
   std::vector<GroupDesc>& gd = b->gd;
   gd.assign(b->hg.size(), GroupDesc{});
+  b->d_err = cv.take<int>(1);
+  b->win_bytes = 0;
   for (size_t i = 0; i < b->hg.size(); i++) {
     HostGroup& g = b->hg[i];
     GroupDesc& G = gd[i];
@@ -568,7 +590,7 @@ static void layout(Batch::Impl* b, char* base) {
     G.geo_ax = (float)g.geo_ax; G.geo_bx = (float)g.geo_bx; G.geo_ay = (float)g.geo_ay; G.geo_by = (float)g.geo_by;
     G.geo_fs = (float)g.geo_fs;
     b->n_tiles += g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
-    b->max_hb = std::max(b->max_hb, g.Hb);
+    if (!(b->compute == 1 && g.geo_k > 0)) b->max_hb = std::max(b->max_hb, g.Hb);  // affine: no tables
     G.frame_base = b->n_frames_total;
     b->n_frames_total += g.nF;
     const ss_inputs* in = g.in;
@@ -585,6 +607,7 @@ static void layout(Batch::Impl* b, char* base) {
       G.frac = S.frac; G.basex = S.basex; G.basey = S.basey;
       G.frac_f = S.frac_f; G.basex_f = S.basex_f; G.basey_f = S.basey_f;
       G.base_mask = S.base_mask; G.min_points = S.min_points;
+      G.col_yrange = S.col_yrange;
     } else {
       G.frac = cv.take<double>(hbw);
       G.basex = cv.take<double>(hbw);
@@ -598,21 +621,32 @@ static void layout(Batch::Impl* b, char* base) {
       }
       G.base_mask = cv.take<uint8_t>(hbw);
       G.min_points = cv.take<int>(g.W);
+      G.col_yrange = b->compute == 1 ? cv.take<float>(2 * (size_t)g.W) : nullptr;
     }
+    G.err = b->d_err;
     g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
     G.image = g.frames_dev ? g.frames_dev : g.d_image;
     if (g.tpl_src >= 0) {
       G.tquad = gd[g.tpl_src].tquad;
       G.gquad = gd[g.tpl_src].gquad;
+      G.tplain = gd[g.tpl_src].tplain;
+      G.tpitch = gd[g.tpl_src].tpitch;
     } else {
       G.tquad = cv.take<char>(nq * 4 * tsz);
       G.gquad = g.grad_derived ? nullptr : cv.take<char>(nq * 4 * tsz);
+      // precision 'S' with an FP32 template and derived gradients samples row windows in shared
+      // memory: rows padded to 16 bytes for the bulk copies
+      G.tpitch = (g.Wt + 3) & ~3;
+      G.tplain = (b->compute == 1 && b->tpl_dt == SS_F32 && g.grad_derived && 2 * G.tpitch * 4 <= kWinBytes)
+                     ? cv.take<float>((size_t)g.Ht * G.tpitch)
+                     : nullptr;
       g.d_templ_stage = cv.take<double>((size_t)g.Ht * g.Wt);
       if (!g.grad_derived) {
         g.d_xg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
         g.d_yg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
       }
     }
+    if (G.tplain) b->win_bytes = kWinBytes;
     g.d_sum = cv.take<double>(1);
     G.sum_image = g.d_sum;
     g.d_p0 = cv.take<double>(2 * N);
@@ -727,6 +761,21 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
       }
       SS_CK(cudaMemcpyAsync((void*)G.base_mask, g.bmask.data(), hbw, cudaMemcpyHostToDevice, s));
       SS_CK(cudaMemcpyAsync((void*)G.min_points, g.minp.data(), g.W * 4, cudaMemcpyHostToDevice, s));
+      if (G.col_yrange) {  // [min, max] of basey over the valid rows of each block column
+        g.yrange.assign(2 * (size_t)g.W, 0.0f);
+        for (int c = 0; c < g.W; c++) {
+          double lo = INFINITY, hi = -INFINITY;
+          for (int r = 0; r < g.Hb; r++) {
+            const size_t i = (size_t)c * g.Hb + r;
+            if (!g.bmask[i]) continue;
+            lo = std::min(lo, g.by[i]);
+            hi = std::max(hi, g.by[i]);
+          }
+          g.yrange[2 * c] = (float)lo;
+          g.yrange[2 * c + 1] = (float)hi;
+        }
+        SS_CK(cudaMemcpyAsync((void*)G.col_yrange, g.yrange.data(), g.yrange.size() * 4, cudaMemcpyHostToDevice, s));
+      }
     }
     if (!g.frames_dev)
       SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
@@ -747,6 +796,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
         k_build_gquad<double><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (double*)G.gquad);
     } else if (b->tpl_dt == SS_F32) {
       k_build_tquad<float><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (float*)G.tquad);
+      if (G.tplain) k_build_tplain<<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, G.tpitch, (float*)G.tplain);
       if (!g.grad_derived)
         k_build_gquad<float><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (float*)G.gquad);
     } else {
@@ -812,6 +862,7 @@ static int reset_state(Batch::Impl* b) {
   }
   SS_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl.data(), b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(int), s));
+  SS_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), s));
   return SS_OK;
 }
 
@@ -857,7 +908,9 @@ int Batch::run() {
   if (rc) return rc;
   SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost,
                         b->stream));
+  SS_CK(cudaMemcpyAsync(b->h_counters + 2, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   SS_CK(cudaStreamSynchronize(b->stream));
+  if (b->h_counters[2] & 1) return fail(SS_ERR_CUDA, "a shared-memory staging copy did not complete in time");
   for (int m = 0; m < 4; m++) b->eval_ms[m] = 0;
   for (size_t k = 0; k < b->event_used; k += 2) {
     float ms = 0;

@@ -123,6 +123,19 @@ __device__ __forceinline__ Sample<Acc> sample(const GroupDesc& G, Acc x, Acc y) 
   return s;
 }
 
+}  // namespace ss
+
+#include "ss_stage.cuh"
+
+namespace ss {
+
+// Template sample from the staged window (kWin, precision 'S'), else from the global template quads.
+template <class Acc, class TplT, bool kGrad, bool kWin>
+__device__ __forceinline__ Sample<Acc> samp(const GroupDesc& G, const TWin& w, Acc x, Acc y) {
+  if constexpr (kWin && sizeof(Acc) == 4) return sample_win<kGrad>(w, x, y);
+  else return sample<Acc, TplT, kGrad>(G, x, y);
+}
+
 template <class FrameT>
 __device__ __forceinline__ FrameT ld_frame(const void* base, size_t i) {
   return __ldg(reinterpret_cast<const FrameT*>(base) + i);
@@ -194,10 +207,10 @@ __host__ __device__ constexpr int nsums(int mode) {
 // Evaluates one block column with one warp and returns the warp-reduced sums (all lanes) and the
 // valid-pixel count. coli is the column's offset in the frame data; mask_out (kFinal) receives the
 // reference's mask output.
-template <class Acc, class FrameT, class TplT, int MODE, bool AFFINE = false>
+template <class Acc, class FrameT, class TplT, int MODE, bool AFFINE = false, bool WIN = false>
 __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, const ColGeo<Acc>& geo,
                                             const ColKnots<Acc>& k, double (&out)[kCsStride], int& cnt_out,
-                                            uint8_t* mask_out, int cc = 0) {
+                                            uint8_t* mask_out, int cc = 0, const TWin& win = TWin{nullptr, 0, 0, 0}) {
   const int lane = threadIdx.x & 31;
   const int Hb = G.Hb;
   const Acc tw = Limits<Acc>::lim(G.Wt), th = Limits<Acc>::lim(G.Ht);
@@ -246,7 +259,7 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
       Acc img = (mA || (k.dual && in)) ? ld_pixel<Acc, FrameT>(G.image, coli + r) : (Acc)0;
       Acc wx = 0, wy = 0, d = 0;
       if (mA) {
-        Sample<Acc> sa = sample<Acc, TplT, true>(G, x, y);
+        Sample<Acc> sa = samp<Acc, TplT, true, WIN>(G, win, x, y);
         wx = sa.wx;
         wy = sa.wy;
         d = img - sa.wI;
@@ -254,7 +267,7 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
       if (k.dual) {
         Acc xb, yb;
         bool mB = warp_pixel<Acc>(k.bx0, k.bx1, k.by0, k.by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
-        d = mB ? img - sample<Acc, TplT, false>(G, xb, yb).wI : (Acc)0;
+        d = mB ? img - samp<Acc, TplT, false, WIN>(G, win, xb, yb).wI : (Acc)0;
       }
       const Acc fn = split_fn ? (in ? geo.fnext[r] : (Acc)0) : f;
       const Acc fsq = f * f, csq = (one - f) * (one - f), fc = f - fsq, fnsq = fn * fn;
@@ -276,20 +289,20 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
       s[kCsJ2y] = fma(d2, wy, s[kCsJ2y]);
     } else if (MODE == kTrial) {
       if (mA) {
-        Acc d = ld_pixel<Acc, FrameT>(G.image, coli + r) - sample<Acc, TplT, false>(G, x, y).wI;
+        Acc d = ld_pixel<Acc, FrameT>(G.image, coli + r) - samp<Acc, TplT, false, WIN>(G, win, x, y).wI;
         s[kCsSsd] = fma(d, d, s[kCsSsd]);
       }
     } else {
       // swapped difference image D' of task_correlation.cu:51-60 over the state (kmask, kdiff)
       Acc img = in ? ld_pixel<Acc, FrameT>(G.image, coli + r) : (Acc)0;
       Acc wA = 0;
-      if (mA) wA = sample<Acc, TplT, false>(G, x, y).wI;
+      if (mA) wA = samp<Acc, TplT, false, WIN>(G, win, x, y).wI;
       bool mB = mA;
       Acc wB = wA;
       if (k.dual) {
         Acc xb, yb;
         mB = warp_pixel<Acc>(k.bx0, k.bx1, k.by0, k.by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
-        wB = mB ? sample<Acc, TplT, false>(G, xb, yb).wI : (Acc)0;
+        wB = mB ? samp<Acc, TplT, false, WIN>(G, win, xb, yb).wI : (Acc)0;
       }
       Acc dstate = mB ? img - wB : (Acc)0;  // differenceImage
       Acc dp = mA ? img - dstate : dstate;  // after d_swapWIDiff
@@ -390,13 +403,21 @@ __device__ __forceinline__ void trial_columns(const GroupDesc& G, int b0, const 
   }
 }
 
+// Shared-memory bytes of one staged block column of geometry (tfrac, basex, basey, the next
+// column's tfrac, base_mask), rounded up to 16.
+template <class Acc>
+__host__ __device__ constexpr size_t stage_bytes(int hb) {
+  return ((size_t)hb * (4 * sizeof(Acc) + 1) + 15) & ~(size_t)15;
+}
+
 // Assembly (at p) and final (at kmask) passes. A CTA takes one block column index cc of one group
 // and G.frames_per_cta of its frames, a warp per frame at a time; the column's geometry is staged in
 // shared memory once for all of them, and the frames share the template rows around the column in L1.
 template <class Acc, class FrameT, class TplT, int MODE>
 __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval(const GroupDesc* __restrict__ gds,
                                                           const int* __restrict__ tile_group,
-                                                          const GroupCtl* __restrict__ ctl, int stage_rows) {
+                                                          const GroupCtl* __restrict__ ctl, int stage_rows,
+                                                          int win_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int g = tile_group[blockIdx.x];
   const GroupDesc& G = gds[g];
@@ -428,6 +449,51 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
     geo = {sf, sx, sy, sm, split_fn ? sn : sf};
   }
   const int f_end = min(G.nF, (fb + 1) * fpc);
+
+  // Precision 'S': stage the template rows every pixel of this CTA can sample (the column's basey
+  // range widened by its frames' y knots) into shared memory; windows that would not fit fall back
+  // to the global template.
+  TWin win{nullptr, 0, 0, 0};
+  if constexpr (sizeof(Acc) == 4) {
+    const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
+    if (win_cap >= 2 && !G.gquad) {
+      const size_t geo_bytes = (!affine && Hb <= stage_rows) ? stage_bytes<Acc>(Hb) : 0;
+      float* wbuf = reinterpret_cast<float*>(smem + geo_bytes);
+      uint64_t* bar = reinterpret_cast<uint64_t*>(smem + geo_bytes + (size_t)win_bytes);
+      float klo = INFINITY, khi = -INFINITY;
+      for (int f = fb * fpc + threadIdx.x; f < f_end; f += blockDim.x) {
+        const int c = f * W + cc;
+        const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
+        float a0, a1, b0 = NAN, b1 = NAN;
+        if (MODE == kAssemble) {
+          a0 = (float)G.p[N + c];
+          a1 = (float)G.p[N + c + 1];
+          if (!frame_active(G, f, C.shift)) {
+            b0 = (float)kd[W + 1 + cc];
+            b1 = (float)kd[W + 1 + cc + 1];
+          }
+        } else {
+          const double* km = G.kmask + (size_t)f * 2 * (W + 1);
+          a0 = (float)km[W + 1 + cc];
+          a1 = (float)km[W + 1 + cc + 1];
+          b0 = (float)kd[W + 1 + cc];
+          b1 = (float)kd[W + 1 + cc + 1];
+        }
+        klo = fminf(klo, fminf(fminf(a0, a1), fminf(b0, b1)));
+        khi = fmaxf(khi, fmaxf(fmaxf(a0, a1), fmaxf(b0, b1)));
+      }
+      block_minmax(klo, khi);
+      int r0, rows;
+      window_rows(G, G.col_yrange[2 * cc] + klo, G.col_yrange[2 * cc + 1] + khi, win_cap, r0, rows);
+      if (rows > 0) {
+        if (threadIdx.x == 0) mbar_init(bar);
+        __syncthreads();
+        unsigned phase = 0;
+        if (stage_window(G, wbuf, r0, rows, bar, phase)) win = {wbuf, r0, rows, G.tpitch};
+      }
+    }
+  }
+
   for (int f = fb * fpc + warp; f < f_end; f += kEvalWarps) {
     const int c = f * W + cc;
     ColKnots<Acc> k;
@@ -450,8 +516,13 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
     int cnt;
     uint8_t* mo = G.o_mask ? G.o_mask + coli : nullptr;
     if constexpr (sizeof(Acc) == 4) {
-      if (affine) eval_column<Acc, FrameT, TplT, MODE, true>(G, coli, geo, k, out, cnt, mo, cc);
-      else eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, mo);
+      if (win.p) {
+        if (affine) eval_column<Acc, FrameT, TplT, MODE, true, true>(G, coli, geo, k, out, cnt, mo, cc, win);
+        else eval_column<Acc, FrameT, TplT, MODE, false, true>(G, coli, geo, k, out, cnt, mo, cc, win);
+      } else {
+        if (affine) eval_column<Acc, FrameT, TplT, MODE, true>(G, coli, geo, k, out, cnt, mo, cc);
+        else eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, mo);
+      }
     } else {
       eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, mo);
     }

@@ -306,11 +306,14 @@ def frames_to_blockmatrix(frames: np.ndarray, layout: BlockLayout, dtype=None) -
 
 
 def boundary_arguments(settings: dict, template: np.ndarray, bm_data: np.ndarray, n_frames: int,
-                       est_dx_knots=None, est_dy_knots=None, layout: BlockLayout | None = None):
+                       est_dx_knots=None, est_dy_knots=None, layout: BlockLayout | None = None,
+                       gradients=None):
     """The 26 ``align_group_to_template`` arguments in MEX order (steady_scan.m:195-242), as a dict
-    keyed by the reference's variable names."""
+    keyed by the reference's variable names. ``gradients`` = (xgrad, ygrad) of ``template`` reuses
+    arrays already made, so the groups of one recording pass the same template objects and the
+    library uploads them once."""
     lay = layout or block_layout(settings)
-    xg, yg = template_gradients(template)
+    xg, yg = gradients if gradients is not None else template_gradients(template)
     nk = lay.nknots
     if est_dx_knots is None or est_dy_knots is None:
         est_dx_knots = np.zeros((nk, n_frames))
