@@ -283,7 +283,7 @@ def main():
                 "traffic": tr.get("bytes_per_frame_pass") if tr else None,
                 "algorithmic_bytes_per_frame_pass": frame_bytes,
                 "frame_passes": passes, "eval_ms_by_pass": rs["eval_ms"], "eval_share_of_step":
-                    eval_ms / rs["run_ms"] if rs["run_ms"] else None}
+                    eval_ms / rs["run_ms"] if rs["run_ms"] else None, "staging": rs["staging"]}
 
     # end to end through the public C ABI from pinned host memory
     e2e = None

@@ -142,6 +142,10 @@ typedef struct ss_batch_stats {
   double eval_ms[4];          /* device time of the evaluation kernels per pass kind (timing on) */
   int64_t arena_bytes;        /* device memory held by the batch */
   double run_ms;              /* wall time of the last run */
+  /* shared-memory staging of the last run: assembly/final CTAs, of them with a template row window,
+   * line-search CTAs, of them with a window, of them on the packed pixel-pair path, and assembly
+   * block columns evaluated as pixel pairs */
+  int64_t staging[6];
 } ss_batch_stats;
 
 SS_API int ss_batch_create(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_batch** batch);

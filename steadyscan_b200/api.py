@@ -261,7 +261,9 @@ class Batch:
         check(self._lib.ss_batch_stats_get(self._h, C.byref(st)))
         return dict(n_groups=st.n_groups, cycles=st.cycles, linesearch_rounds=st.linesearch_rounds,
                     kernel_launches=st.kernel_launches, frame_passes=list(st.frame_passes),
-                    eval_ms=list(st.eval_ms), arena_bytes=st.arena_bytes, run_ms=st.run_ms)
+                    eval_ms=list(st.eval_ms), arena_bytes=st.arena_bytes, run_ms=st.run_ms,
+                    staging=dict(zip(("eval_ctas", "eval_windowed", "ls_ctas", "ls_windowed", "ls_pairs",
+                                      "eval_pair_columns"), list(st.staging))))
 
     @property
     def stream_ptr(self) -> int:

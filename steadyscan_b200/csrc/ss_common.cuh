@@ -89,6 +89,8 @@ struct GroupDesc {
   int tpitch;
   const float* col_yrange;  // W x 2
   int* err;                 // device error word of the batch (bit 0: a staging copy timed out)
+  int pair_ok;              // precision 'S' pixel pairs: affine geometry, Hb % 64 == 0, aligned frames
+  unsigned long long* staging;  // batch counters of shared-memory staging (ss_batch_stats.staging)
   const uint8_t* base_mask;
   const int* min_points;    // W
   const void* image;        // Hb x fW column-major, engine frame type

@@ -82,19 +82,38 @@ __global__ void k_build_gquad(const double* __restrict__ xg, const double* __res
   }
 }
 
-template <class FrameT>
-__global__ void __launch_bounds__(1024) k_sum_image(const void* __restrict__ img, size_t n, double* __restrict__ out) {
+// Sum of all frame samples of a group in two deterministic passes: kSumBlocks CTA partials over
+// fixed contiguous ranges, then one CTA adds the partials in a fixed order.
+constexpr int kSumBlocks = 296;
+
+__device__ __forceinline__ double block_sum(double s) {
   __shared__ double sh[32];
-  double s = 0;
-  for (size_t i = threadIdx.x; i < n; i += blockDim.x) s += to_double(ld_frame<FrameT>(img, i));
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
   __syncthreads();
+  double v = 0;
   if (threadIdx.x < 32) {
-    double v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
     v = warp_sum(v);
-    if (threadIdx.x == 0) *out = v;
   }
+  return v;
+}
+
+template <class FrameT>
+__global__ void __launch_bounds__(1024) k_sum_image(const void* __restrict__ img, size_t n, double* __restrict__ parts) {
+  const size_t per = (n + gridDim.x - 1) / gridDim.x;
+  const size_t a = blockIdx.x * per, e = a + per < n ? a + per : n;
+  double s = 0;
+  for (size_t i = a + threadIdx.x; i < e; i += blockDim.x) s += to_double(ld_frame<FrameT>(img, i));
+  s = block_sum(s);
+  if (threadIdx.x == 0) parts[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) k_sum_parts(const double* __restrict__ parts, int n, double* __restrict__ out) {
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += parts[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) *out = s;
 }
 
 __global__ void k_fill(double* p, size_t n, double v) {
@@ -110,11 +129,15 @@ constexpr int kStageBytes = 96 * 1024;
 // Shared memory for one template row window of precision 'S' (26 rows of a 512-pixel template):
 // four resident assembly CTAs per SM.
 constexpr int kWinBytes = 52 * 1024;
+// Shared memory for the template rows of one line-search CTA (98 rows of a 512-pixel template;
+// with the kernel's static shared memory one 1024-thread CTA per SM).
+constexpr int kLsWinBytes = 196 * 1024;
 
 using EvalFn = cudaError_t (*)(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
                                const GroupCtl* ctl, int max_hb, int win_bytes);
-using LsFn = cudaError_t (*)(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl);
-using SumFn = void (*)(const void* img, size_t n, double* out, cudaStream_t s);
+using LsFn = cudaError_t (*)(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl,
+                             int win_bytes);
+using SumFn = void (*)(const void* img, size_t n, double* parts, double* out, cudaStream_t s);
 
 template <class Acc, class FrameT, class TplT>
 static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
@@ -140,12 +163,21 @@ static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupD
 }
 
 template <class Acc, class FrameT, class TplT>
-static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl) {
+static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl,
+                             int win_bytes) {
   if (frames <= 0) return cudaSuccess;
+  if (sizeof(Acc) != 4) win_bytes = 0;
+  win_bytes = std::min(win_bytes, kLsWinBytes) & ~15;
+  static bool attr_set = false;
+  if (!attr_set && sizeof(Acc) == 4) {
+    cudaFuncSetAttribute(k_linesearch<Acc, FrameT, TplT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kLsWinBytes + 16);
+    attr_set = true;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(frames * kLsCluster, 1, 1);
-  cfg.blockDim = dim3(kLsThreads, 1, 1);
-  cfg.dynamicSmemBytes = 0;
+  cfg.blockDim = dim3(LsShape<Acc>::threads, 1, 1);
+  cfg.dynamicSmemBytes = win_bytes ? (size_t)win_bytes + 16 : 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -154,7 +186,7 @@ static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, co
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_linesearch<Acc, FrameT, TplT>, gd, fg, ctl);
+  return cudaLaunchKernelEx(&cfg, k_linesearch<Acc, FrameT, TplT>, gd, fg, ctl, win_bytes);
 }
 
 struct KernelSet {
@@ -162,8 +194,9 @@ struct KernelSet {
   LsFn ls;
 };
 template <class FrameT>
-static void sum_launch(const void* img, size_t n, double* out, cudaStream_t s) {
-  k_sum_image<FrameT><<<1, 1024, 0, s>>>(img, n, out);
+static void sum_launch(const void* img, size_t n, double* parts, double* out, cudaStream_t s) {
+  k_sum_image<FrameT><<<kSumBlocks, 1024, 0, s>>>(img, n, parts);
+  k_sum_parts<<<1, 256, 0, s>>>(parts, kSumBlocks, out);
 }
 
 template <class Acc, class FrameT, class TplT>
@@ -516,7 +549,11 @@ struct Batch::Impl {
   int* d_frame_group = nullptr;
   int* d_counters = nullptr;  // [0] searching frames, [1] finished groups
   int* d_err = nullptr;       // device error word (bit 0: a shared-memory staging copy timed out)
+  unsigned long long* d_staging = nullptr;  // staging counters of the run
+  double* d_sum_parts = nullptr;            // partial sums of k_sum_image
+  unsigned long long h_staging[6] = {0, 0, 0, 0, 0, 0};
   int win_bytes = 0;          // template window bytes per assembly/final CTA (0: no windows)
+  int ls_win_bytes = 0;       // template window bytes per line-search CTA (0: no windows)
   int* h_counters = nullptr;  // pinned
   int n_tiles = 0, n_frames_total = 0;
   int max_hb = 0;  // largest block height among groups whose geometry k_eval stages in shared memory
@@ -544,7 +581,7 @@ struct Batch::Impl {
       }
       cudaEventRecord(events[event_used], stream);
     }
-    if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl);
+    if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl, ls_win_bytes);
     else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb, win_bytes);
     launches++;
     if (timing) {
@@ -577,7 +614,10 @@ static void layout(Batch::Impl* b, char* base) {
   std::vector<GroupDesc>& gd = b->gd;
   gd.assign(b->hg.size(), GroupDesc{});
   b->d_err = cv.take<int>(1);
+  b->d_staging = cv.take<unsigned long long>(6);
+  b->d_sum_parts = cv.take<double>(kSumBlocks);
   b->win_bytes = 0;
+  b->ls_win_bytes = 0;
   for (size_t i = 0; i < b->hg.size(); i++) {
     HostGroup& g = b->hg[i];
     GroupDesc& G = gd[i];
@@ -624,8 +664,14 @@ static void layout(Batch::Impl* b, char* base) {
       G.col_yrange = b->compute == 1 ? cv.take<float>(2 * (size_t)g.W) : nullptr;
     }
     G.err = b->d_err;
+    G.staging = b->d_staging;
     g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
     G.image = g.frames_dev ? g.frames_dev : g.d_image;
+    {
+      const size_t fsz = dtype_size(g.frame_dt);
+      G.pair_ok = (b->compute == 1 && g.geo_k > 0 && g.Hb % 64 == 0 &&
+                   reinterpret_cast<uintptr_t>(G.image) % (2 * fsz) == 0) ? 1 : 0;
+    }
     if (g.tpl_src >= 0) {
       G.tquad = gd[g.tpl_src].tquad;
       G.gquad = gd[g.tpl_src].gquad;
@@ -646,7 +692,7 @@ static void layout(Batch::Impl* b, char* base) {
         g.d_yg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
       }
     }
-    if (G.tplain) b->win_bytes = kWinBytes;
+    if (G.tplain) b->win_bytes = kWinBytes;  // the line search runs from the global template
     g.d_sum = cv.take<double>(1);
     G.sum_image = g.d_sum;
     g.d_p0 = cv.take<double>(2 * N);
@@ -805,7 +851,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
         k_build_gquad<__half><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (__half*)G.gquad);
     }
     SS_CK(cudaGetLastError());
-    b->sum(G.image, (size_t)g.Hb * g.fW, g.d_sum, s);
+    b->sum(G.image, (size_t)g.Hb * g.fW, b->d_sum_parts, g.d_sum, s);
     SS_CK(cudaGetLastError());
     const int ntiles = g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
     for (int t = 0; t < ntiles; t++) tile_group[G.tile_base + t] = (int)i;
@@ -863,6 +909,7 @@ static int reset_state(Batch::Impl* b) {
   SS_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl.data(), b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(int), s));
   SS_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), s));
+  SS_CK(cudaMemsetAsync(b->d_staging, 0, 6 * sizeof(unsigned long long), s));
   return SS_OK;
 }
 
@@ -909,6 +956,7 @@ int Batch::run() {
   SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost,
                         b->stream));
   SS_CK(cudaMemcpyAsync(b->h_counters + 2, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  SS_CK(cudaMemcpyAsync(b->h_staging, b->d_staging, sizeof(b->h_staging), cudaMemcpyDeviceToHost, b->stream));
   SS_CK(cudaStreamSynchronize(b->stream));
   if (b->h_counters[2] & 1) return fail(SS_ERR_CUDA, "a shared-memory staging copy did not complete in time");
   for (int m = 0; m < 4; m++) b->eval_ms[m] = 0;
@@ -934,6 +982,7 @@ void Batch::stats(ss_batch_stats* st) const {
   for (int m = 0; m < 4; m++) st->eval_ms[m] = d->eval_ms[m];
   st->arena_bytes = (int64_t)d->arena_bytes;
   st->run_ms = d->run_ms;
+  for (int i = 0; i < 6; i++) st->staging[i] = (int64_t)d->h_staging[i];
 }
 
 int Batch::collect() {

@@ -30,7 +30,6 @@ namespace cg = cooperative_groups;
 
 constexpr int kEvalWarps = 8;       // warps per assembly/final CTA
 constexpr int kLsCluster = 8;       // CTAs per frame in the line-search cluster
-constexpr int kLsThreads = 256;
 constexpr int kLsMaxKnots = 256;    // knots per cluster CTA: frame_w <= kLsCluster * kLsMaxKnots
 constexpr int kMaxFrameW = kLsCluster * kLsMaxKnots;
 
@@ -43,7 +42,18 @@ struct MinBlocks {
 };
 template <>
 struct MinBlocks<float> {
-  static constexpr int value = 4;
+  static constexpr int value = 3;
+};
+
+// Line-search CTA: 256 threads; two (FP64) or four (FP32) CTAs per SM. A launch given window bytes
+// keeps the template rows of the CTA's knot range in shared memory for the whole search.
+template <class Acc>
+struct LsShape {
+  static constexpr int threads = 256, min_blocks = 2;
+};
+template <>
+struct LsShape<float> {
+  static constexpr int threads = 256, min_blocks = 4;
 };
 
 __device__ __forceinline__ bool frame_active(const GroupDesc& G, int f, int shift) {
@@ -125,7 +135,7 @@ __device__ __forceinline__ Sample<Acc> sample(const GroupDesc& G, Acc x, Acc y) 
 
 }  // namespace ss
 
-#include "ss_stage.cuh"
+#include "ss_pairs.cuh"
 
 namespace ss {
 
@@ -341,8 +351,8 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
 // interleaved so that the frame loads and template gathers of all columns are in flight together.
 // Loads are predicated by index clamping (a masked pixel reads row 0 / quad 0 and is discarded), so
 // the column loop has no divergent branches. tq: frame-local column indices, nq <= NC of them valid.
-template <class Acc, class FrameT, class TplT, bool AFFINE, int NC>
-__device__ __forceinline__ void trial_columns(const GroupDesc& G, int b0, const int (&tq)[NC], int nq,
+template <class Acc, class FrameT, class TplT, bool AFFINE, int NC, bool WIN = false>
+__device__ __forceinline__ void trial_columns(const GroupDesc& G, int b0, const TWin& win, const int (&tq)[NC], int nq,
                                               const Acc (&qx0)[NC], const Acc (&qx1)[NC], const Acc (&qy0)[NC],
                                               const Acc (&qy1)[NC], double (&ssd)[NC], int (&cnt)[NC]) {
   const int lane = threadIdx.x & 31;
@@ -389,7 +399,7 @@ __device__ __forceinline__ void trial_columns(const GroupDesc& G, int b0, const 
         Acc x, y;
         const bool m = warp_pixel<Acc>(qx0[q], qx1[q], qy0[q], qy1[q], f, bx, by, bm, tw, th, x, y);
         const Acc img = ld_pixel<Acc, FrameT>(G.image, coli[q] + rr);
-        const Acc wI = sample<Acc, TplT, false>(G, m ? x : (Acc)0, m ? y : (Acc)0).wI;
+        const Acc wI = samp<Acc, TplT, false, WIN>(G, win, m ? x : (Acc)0, m ? y : (Acc)0).wI;
         const Acc d = img - wI;
         s[q] = m ? fma(d, d, s[q]) : s[q];
         c[q] += m ? 1 : 0;
@@ -494,6 +504,10 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
     }
   }
 
+  if (threadIdx.x == 0) {
+    atomicAdd(G.staging + 0, 1ull);
+    if (win.p) atomicAdd(G.staging + 1, 1ull);
+  }
   for (int f = fb * fpc + warp; f < f_end; f += kEvalWarps) {
     const int c = f * W + cc;
     ColKnots<Acc> k;
@@ -516,7 +530,10 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
     int cnt;
     uint8_t* mo = G.o_mask ? G.o_mask + coli : nullptr;
     if constexpr (sizeof(Acc) == 4) {
-      if (win.p) {
+      if (MODE == kAssemble && win.p && G.pair_ok && !k.dual) {
+        assemble_pairs<FrameT>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt);
+        if ((threadIdx.x & 31) == 0) atomicAdd(G.staging + 5, 1ull);
+      } else if (win.p) {
         if (affine) eval_column<Acc, FrameT, TplT, MODE, true, true>(G, coli, geo, k, out, cnt, mo, cc, win);
         else eval_column<Acc, FrameT, TplT, MODE, false, true>(G, coli, geo, k, out, cnt, mo, cc, win);
       } else {
@@ -543,9 +560,11 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
 // committed knot at line-search start (p_snap), or the never-written 1e6 for the last frame.
 // After shift 1 the cluster also evaluates the frame's correlation sums (the iteration-end state).
 template <class Acc, class FrameT, class TplT>
-__global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearch(const GroupDesc* __restrict__ gds,
-                                                           const int* __restrict__ frame_group,
-                                                           GroupCtl* __restrict__ ctl) {
+__global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_blocks)
+    k_linesearch(const GroupDesc* __restrict__ gds, const int* __restrict__ frame_group, GroupCtl* __restrict__ ctl,
+                 int win_bytes) {
+  constexpr int kLsThreads = LsShape<Acc>::threads;
+  extern __shared__ __align__(16) unsigned char ls_smem[];
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int gf = blockIdx.x / kLsCluster;
@@ -590,6 +609,47 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
   }
   __syncthreads();
 
+  // Precision 'S': stage the template rows of this CTA's lines for every knot vector the search
+  // and the correlation pass can evaluate (trial knots lie between p and p + deltaP; kmask and
+  // kdiff are earlier states); a range that does not fit uses the global template.
+  TWin win{nullptr, 0, 0, 0};
+  if constexpr (sizeof(Acc) == 4) {
+    const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
+    if (win_cap >= 2 && !G.gquad && hi > lo) {
+      float klo = INFINITY, khi = -INFINITY;
+      for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+        const float a = (float)s_p[1][i], b = (float)(s_p[1][i] + s_dp[1][i]);
+        const float c = (float)s_km[1][i], d = (float)s_kd[1][i];
+        klo = fminf(klo, fminf(fminf(a, b), fminf(c, d)));
+        khi = fmaxf(khi, fmaxf(fmaxf(a, b), fmaxf(c, d)));
+      }
+      float ylo = INFINITY, yhi = -INFINITY;
+      for (int t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+        ylo = fminf(ylo, G.col_yrange[2 * t]);
+        yhi = fmaxf(yhi, G.col_yrange[2 * t + 1]);
+      }
+      block_minmax(klo, khi);
+      block_minmax(ylo, yhi);
+      int r0, rows;
+      window_rows(G, ylo + klo, yhi + khi, win_cap, r0, rows);
+      if (rows > 0) {
+        float* wbuf = reinterpret_cast<float*>(ls_smem);
+        uint64_t* bar = reinterpret_cast<uint64_t*>(ls_smem + (size_t)win_bytes);
+        if (threadIdx.x == 0) mbar_init(bar);
+        __syncthreads();
+        unsigned phase = 0;
+        if (stage_window(G, wbuf, r0, rows, bar, phase)) win = {wbuf, r0, rows, G.tpitch};
+      }
+    }
+  }
+  bool pairs = false;
+  if constexpr (sizeof(Acc) == 4) pairs = win.p && G.pair_ok;
+  if (threadIdx.x == 0) {
+    atomicAdd(G.staging + 2, 1ull);
+    if (win.p) atomicAdd(G.staging + 3, 1ull);
+    if (pairs) atomicAdd(G.staging + 4, 1ull);
+  }
+
   const double thr = G.move_thresh, rho = G.ls_mult;
   int trials = 0;
   while (searching) {
@@ -598,7 +658,21 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
     long long cnt = 0;
     bool present = false;
     constexpr int NC = 4;
-    for (int t0 = lo + warp; t0 < hi; t0 += nw * NC) {
+    if (pairs) {
+      for (int t = lo + warp; t < hi; t += nw) {
+        const int i = t - lo;
+        const float x0 = (float)(s_p[0][i] + s_dp[0][i]), y0 = (float)(s_p[1][i] + s_dp[1][i]);
+        const float x1 = (float)((t + 1 < W) ? s_p[0][i + 1] + s_dp[0][i + 1] : s_p[0][i + 1]);
+        const float y1 = (float)((t + 1 < W) ? s_p[1][i + 1] + s_dp[1][i + 1] : s_p[1][i + 1]);
+        double qs;
+        int qc;
+        trial_pairs<FrameT>(G, (size_t)(b0 + t) * Hb, pair_col(G, t, x0, x1, y0, y1), pair_win(win), qs, qc);
+        ssd += qs;
+        cnt += qc;
+        present |= qc >= G.min_points[t];
+      }
+    }
+    for (int t0 = lo + warp; !pairs && t0 < hi; t0 += nw * NC) {
       int tq[NC], nq = 0;
       Acc qx0[NC], qx1[NC], qy0[NC], qy1[NC];
 #pragma unroll
@@ -617,8 +691,13 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
       int qc[NC];
       bool aff = false;
       if constexpr (sizeof(Acc) == 4) aff = G.geo_k > 0;
-      if (aff) trial_columns<Acc, FrameT, TplT, true, NC>(G, b0, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
-      else trial_columns<Acc, FrameT, TplT, false, NC>(G, b0, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+      if (win.p) {
+        if (aff) trial_columns<Acc, FrameT, TplT, true, NC, true>(G, b0, win, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+        else trial_columns<Acc, FrameT, TplT, false, NC, true>(G, b0, win, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+      } else {
+        if (aff) trial_columns<Acc, FrameT, TplT, true, NC>(G, b0, win, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+        else trial_columns<Acc, FrameT, TplT, false, NC>(G, b0, win, tq, nq, qx0, qx1, qy0, qy1, qs, qc);
+      }
 #pragma unroll
       for (int q = 0; q < NC; q++) {
         if (q < nq) {
@@ -737,11 +816,18 @@ __global__ void __launch_bounds__(kLsThreads, MinBlocks<Acc>::value) k_linesearc
       double out[kCsStride];
       int c;
       if constexpr (sizeof(Acc) == 4) {
-        if (G.geo_k > 0)
-          eval_column<Acc, FrameT, TplT, kCorr, true>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c,
-                                                      nullptr, t);
-        else
-          eval_column<Acc, FrameT, TplT, kCorr>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
+        const size_t coli = (size_t)(b0 + t) * Hb;
+        if (win.p) {
+          if (G.geo_k > 0)
+            eval_column<Acc, FrameT, TplT, kCorr, true, true>(G, coli, global_geo<Acc>(G, t), k, out, c, nullptr, t, win);
+          else
+            eval_column<Acc, FrameT, TplT, kCorr, false, true>(G, coli, global_geo<Acc>(G, t), k, out, c, nullptr, t,
+                                                               win);
+        } else if (G.geo_k > 0) {
+          eval_column<Acc, FrameT, TplT, kCorr, true>(G, coli, global_geo<Acc>(G, t), k, out, c, nullptr, t);
+        } else {
+          eval_column<Acc, FrameT, TplT, kCorr>(G, coli, global_geo<Acc>(G, t), k, out, c, nullptr);
+        }
       } else {
         eval_column<Acc, FrameT, TplT, kCorr>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k, out, c, nullptr);
       }

@@ -1,0 +1,240 @@
+// Pixel-pair evaluation of precision 'S' on the packed FP32 pipe (f32x2 fma/add/mul of sm_100).
+//
+// Applies to a block column with the default scan geometry (affine in the pixel index, k lines per
+// knot, k dividing 32, Hb a multiple of 64) whose template rows are staged in a shared-memory
+// window. Lane `lane` of a warp takes rows 64 t + 2 lane and 64 t + 2 lane + 1 of step t as the
+// two halves of float2 values, so every arithmetic instruction serves two pixels; the two frame
+// samples are one 32-bit (16-bit storage) or 64-bit (FP32 storage) load.
+//
+// The warp model is the reference's (task_applyparameters.cuh:33-62): with f = fs (l L + j + 1/2)
+// and basex = ax j + bx0, basey = ay (cc k + l) + by0 for pixel j of line l of knot span cc,
+//   x = basex + kx0 (1 - f) + kx1 f = (ax + (kx1 - kx0) fs) j + (bx0 + kx0 + (kx1 - kx0) f0(l)),
+// and y likewise: one fma per coordinate. Bilinear values and gradients follow
+// task_differenceimage.cuh:118-126 and task_updategradients.cu:12-20 in lerp form. The FP32 results
+// differ from the FP64 path by rounding only.
+#pragma once
+
+#include "ss_stage.cuh"
+
+namespace ss {
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  float2 r;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n sub.rn.f32x2 rd, ra, rb;\n"
+      " mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+// Two frame samples of rows (2i, 2i + 1) of a column as floats.
+template <class FrameT>
+struct PairLoad;
+template <>
+struct PairLoad<uint16_t> {
+  using W = uint32_t;
+  __device__ static W load(const void* col, int i) { return __ldg(reinterpret_cast<const uint32_t*>(col) + i); }
+  __device__ static float2 cvt(W w) {
+    // 2^23 + v has v in its mantissa: exact for 16-bit v
+    const float lo = __uint_as_float(0x4B000000u | (w & 0xFFFFu)) - 8388608.0f;
+    const float hi = __uint_as_float(0x4B000000u | (w >> 16)) - 8388608.0f;
+    return make_float2(lo, hi);
+  }
+};
+template <>
+struct PairLoad<__half> {
+  using W = uint32_t;
+  __device__ static W load(const void* col, int i) { return __ldg(reinterpret_cast<const uint32_t*>(col) + i); }
+  __device__ static float2 cvt(W w) {
+    __half2 h = *reinterpret_cast<__half2*>(&w);
+    return __half22float2(h);
+  }
+};
+template <>
+struct PairLoad<float> {
+  using W = float2;
+  __device__ static W load(const void* col, int i) { return __ldg(reinterpret_cast<const float2*>(col) + i); }
+  __device__ static float2 cvt(W w) { return w; }
+};
+template <>
+struct PairLoad<double> {
+  using W = double2;
+  __device__ static W load(const void* col, int i) { return __ldg(reinterpret_cast<const double2*>(col) + i); }
+  __device__ static float2 cvt(W w) { return make_float2((float)w.x, (float)w.y); }
+};
+
+// Per-warp constants of one block column for the pair loop.
+struct PairCol {
+  float2 bxj, cx, byj, cy;  // x = bxj * j + cx, y = byj * j + cy (both halves)
+  float2 fsj, f0;           // f = fsj * j + f0
+  float2 j0;                // j of step 0 for both halves
+  float dj;                 // j advance per step (64 / k)
+};
+
+// Column constants for knots (kx0, kx1, ky0, ky1) of block column cc (lane-dependent halves).
+__device__ __forceinline__ PairCol pair_col(const GroupDesc& G, int cc, float kx0, float kx1, float ky0, float ky1) {
+  const int lane = threadIdx.x & 31, k = G.geo_k, L = G.geo_L;
+  const int rA = 2 * lane, rB = 2 * lane + 1;
+  const int lA = rA % k, lB = rB % k;
+  const float fs = G.geo_fs;
+  const float f0A = ((float)(lA * L) + 0.5f) * fs, f0B = ((float)(lB * L) + 0.5f) * fs;
+  const float dkx = kx1 - kx0, dky = ky1 - ky0;
+  PairCol p;
+  p.bxj = f2(fmaf(dkx, fs, G.geo_ax));
+  p.cx = f2(fmaf(dkx, f0A, G.geo_bx + kx0), fmaf(dkx, f0B, G.geo_bx + kx0));
+  p.byj = f2(dky * fs);
+  p.cy = f2(fmaf(dky, f0A, fmaf(G.geo_ay, (float)(cc * k + lA), G.geo_by) + ky0),
+            fmaf(dky, f0B, fmaf(G.geo_ay, (float)(cc * k + lB), G.geo_by) + ky0));
+  p.fsj = f2(fs);
+  p.f0 = f2(f0A, f0B);
+  p.j0 = f2((float)(rA / k), (float)(rB / k));
+  p.dj = (float)(64 / k);
+  return p;
+}
+
+// Window addressing: element (iy, ix) of the template sits at index (iy - r0) pitch + ix of the
+// window; from v = 2^23 + floor(c) (the bits of a round-down add) that index is
+// vy pitch + vx - kbias in wrapping 32-bit arithmetic, clamped so masked pixels stay in bounds.
+struct PairWin {
+  const float* p;
+  unsigned pitch, kbias, emax;
+};
+__device__ __forceinline__ PairWin pair_win(const TWin& w) {
+  PairWin q;
+  q.p = w.p;
+  q.pitch = (unsigned)w.pitch;
+  q.kbias = 0x4B000000u * ((unsigned)w.pitch + 1u) + (unsigned)w.r0 * (unsigned)w.pitch;
+  q.emax = (unsigned)((w.rows - 1) * w.pitch - 2);
+  return q;
+}
+
+// Floor / fraction of both halves (0 <= c < 2^23 for valid pixels) and the window corner values.
+__device__ __forceinline__ void pair_sample(const PairWin& w, float2 x, float2 y, float2& xf, float2& yf, float2& t00,
+                                            float2& t01, float2& t10, float2& t11) {
+  const float2 big = f2(8388608.0f);
+  const float2 vx = __fadd2_rd(x, big), vy = __fadd2_rd(y, big);
+  xf = sub2(x, sub2(vx, big));
+  yf = sub2(y, sub2(vy, big));
+  unsigned eA = __float_as_uint(vy.x) * w.pitch + __float_as_uint(vx.x) - w.kbias;
+  unsigned eB = __float_as_uint(vy.y) * w.pitch + __float_as_uint(vx.y) - w.kbias;
+  eA = min(eA, w.emax);
+  eB = min(eB, w.emax);
+  const float* qA = w.p + eA;
+  const float* qB = w.p + eB;
+  t00 = f2(qA[0], qB[0]);
+  t01 = f2(qA[1], qB[1]);
+  t10 = f2(qA[w.pitch], qB[w.pitch]);
+  t11 = f2(qA[w.pitch + 1], qB[w.pitch + 1]);
+}
+
+// Validity of both halves: 0 <= c < lim as an unsigned compare of the bit patterns (negative
+// values and NaN have larger patterns).
+__device__ __forceinline__ bool in_range(float c, unsigned lim_bits) { return __float_as_uint(c) < lim_bits; }
+
+// Assembly sums (kCsSsd .. kCsJ2y) and valid count of one block column at knots that are both the
+// mask and the difference-image knots. out/cnt are warp-reduced (all lanes).
+template <class FrameT>
+__device__ __forceinline__ void assemble_pairs(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
+                                               double (&out)[kCsStride], int& cnt_out) {
+  using PL = PairLoad<FrameT>;
+  const int lane = threadIdx.x & 31;
+  const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
+  const FrameT* col = reinterpret_cast<const FrameT*>(G.image) + coli;
+  const int steps = G.Hb >> 6;
+  float2 ssd = f2(0.f), axx = f2(0.f), ayy = f2(0.f), axy = f2(0.f), bxx = f2(0.f), byy = f2(0.f), bxy = f2(0.f),
+         oxx = f2(0.f), oyy = f2(0.f), oxy = f2(0.f), j1x = f2(0.f), j1y = f2(0.f), j2x = f2(0.f), j2y = f2(0.f);
+  int cnt = 0;
+  float2 j = pc.j0;
+  const float2 dj = f2(pc.dj), one = f2(1.0f);
+  typename PL::W nxt = PL::load(col, lane);
+#pragma unroll 1
+  for (int t = 0; t < steps; t++) {
+    const typename PL::W cur = nxt;
+    if (t + 1 < steps) nxt = PL::load(col, (t + 1) * 32 + lane);
+    const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy), f = fma2(pc.fsj, j, pc.f0);
+    j = add2(j, dj);
+    const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+    const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+    cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+    float2 xf, yf, t00, t01, t10, t11;
+    pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+    const float2 gy0 = sub2(t10, t00), gy1 = sub2(t11, t01);
+    const float2 gx0 = sub2(t01, t00), gx1 = sub2(t11, t10);
+    const float2 a = fma2(yf, gy0, t00), b = fma2(yf, gy1, t01);
+    const float2 wI = fma2(xf, sub2(b, a), a);
+    float2 wx = fma2(yf, sub2(gx1, gx0), gx0);
+    float2 wy = fma2(xf, sub2(gy1, gy0), gy0);
+    float2 d = sub2(PL::cvt(cur), wI);
+    d = f2(mA ? d.x : 0.f, mB ? d.y : 0.f);
+    wx = f2(mA ? wx.x : 0.f, mB ? wx.y : 0.f);
+    wy = f2(mA ? wy.x : 0.f, mB ? wy.y : 0.f);
+    const float2 c = sub2(one, f);
+    const float2 csq = mul2(c, c), fsq = mul2(f, f), fc = mul2(f, c);
+    const float2 gxx = mul2(wx, wx), gyy = mul2(wy, wy), gxy = mul2(wx, wy);
+    ssd = fma2(d, d, ssd);
+    axx = fma2(gxx, csq, axx);
+    ayy = fma2(gyy, csq, ayy);
+    axy = fma2(gxy, csq, axy);
+    bxx = fma2(gxx, fsq, bxx);
+    byy = fma2(gyy, fsq, byy);
+    bxy = fma2(gxy, fsq, bxy);
+    oxx = fma2(gxx, fc, oxx);
+    oyy = fma2(gyy, fc, oyy);
+    oxy = fma2(gxy, fc, oxy);
+    const float2 d1 = mul2(d, c), d2 = mul2(d, f);
+    j1x = fma2(d1, wx, j1x);
+    j1y = fma2(d1, wy, j1y);
+    j2x = fma2(d2, wx, j2x);
+    j2y = fma2(d2, wy, j2y);
+  }
+  cnt_out = warp_sum(cnt);
+  const float2 v[kCsAssemble] = {ssd, axx, ayy, axy, bxx, byy, bxy, oxx, oyy, oxy, j1x, j1y, j2x, j2y};
+#pragma unroll
+  for (int i = 0; i < kCsAssemble; i++) out[i] = warp_sum((double)(v[i].x + v[i].y));
+}
+
+// Trial SSD and valid count of one block column (task_linesearch.cu:50-74 with the SSD of
+// task_calcerrval.cu:6-18); out values are warp-reduced (all lanes).
+template <class FrameT>
+__device__ __forceinline__ void trial_pairs(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
+                                            double& ssd_out, int& cnt_out) {
+  using PL = PairLoad<FrameT>;
+  const int lane = threadIdx.x & 31;
+  const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
+  const FrameT* col = reinterpret_cast<const FrameT*>(G.image) + coli;
+  const int steps = G.Hb >> 6;
+  float2 ssd = f2(0.f);
+  int cnt = 0;
+  float2 j = pc.j0;
+  const float2 dj = f2(pc.dj);
+  // two steps of frame samples in flight
+  typename PL::W w0 = PL::load(col, lane);
+  typename PL::W w1 = steps > 1 ? PL::load(col, 32 + lane) : w0;
+#pragma unroll 1
+  for (int t = 0; t < steps; t++) {
+    const typename PL::W cur = w0;
+    w0 = w1;
+    if (t + 2 < steps) w1 = PL::load(col, (t + 2) * 32 + lane);
+    const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
+    j = add2(j, dj);
+    const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+    const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+    cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+    float2 xf, yf, t00, t01, t10, t11;
+    pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+    const float2 a = fma2(yf, sub2(t10, t00), t00), b = fma2(yf, sub2(t11, t01), t01);
+    const float2 wI = fma2(xf, sub2(b, a), a);
+    float2 d = sub2(PL::cvt(cur), wI);
+    d = f2(mA ? d.x : 0.f, mB ? d.y : 0.f);
+    ssd = fma2(d, d, ssd);
+  }
+  cnt_out = warp_sum(cnt);
+  ssd_out = warp_sum((double)(ssd.x + ssd.y));
+}
+
+}  // namespace ss

@@ -103,6 +103,19 @@ def test_precision_s_within_bound():
     assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([o["dx"], o["dy"]])) <= KNOT_RMS_S
 
 
+@pytest.mark.parametrize("dtype", [np.uint16, np.float16, np.float32, np.float64])
+def test_precision_s_pixel_pairs_per_frame_type(dtype):
+    """Precision S on the default scan geometry with 2 lines per knot (Hb a multiple of 64: the
+    packed pixel-pair assembly) stays within the bound of the FP64 oracle on the same frames for
+    every frame storage type; valid-pixel counts differ at most at boundary ties."""
+    args, _, _ = make_args(nlines=64, linewidth=64, nknots=33, n_frames=4, seed=51, frame_dtype=dtype, n_blobs=30)
+    o = oracle.align_group(args)
+    args["flags"] = "S"
+    g = api.align_group(args)
+    assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([o["dx"], o["dy"]])) <= KNOT_RMS_S
+    assert abs(int(g["mask"].sum()) - int(o["mask"].sum())) <= 0.001 * g["mask"].size
+
+
 def test_precision_s_affine_and_table_geometry_agree():
     """Precision S computes the default scan geometry in registers when the tables are affine; a
     1e-7 px perturbation of basex forces the table path. Both stay within the bound of FP64."""
