@@ -91,6 +91,8 @@ struct GroupDesc {
   int* err;                 // device error word of the batch (bit 0: a staging copy timed out)
   int pair_ok;              // precision 'S' pixel pairs: affine geometry, Hb % 64 == 0, aligned frames
   unsigned long long* staging;  // batch counters of shared-memory staging (ss_batch_stats.staging)
+  int* searching;           // batch count of frames whose line search runs (trial rounds)
+  int* ls_done;             // nF: columns of the frame evaluated in the current trial round
   const uint8_t* base_mask;
   const int* min_points;    // W
   const void* image;        // Hb x fW column-major, engine frame type
@@ -163,6 +165,11 @@ __device__ __forceinline__ void load_quad<float, __half>(const void* base, size_
 // warp reductions
 
 __device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;

@@ -126,9 +126,9 @@ __global__ void k_fill(double* p, size_t n, double v) {
 // Dynamic shared memory for staging one block column's geometry (tfrac, basex, basey, the next
 // column's tfrac and base_mask) in k_eval.
 constexpr int kStageBytes = 96 * 1024;
-// Shared memory for one template row window of precision 'S' (26 rows of a 512-pixel template):
-// four resident assembly CTAs per SM.
-constexpr int kWinBytes = 52 * 1024;
+// Shared memory for one template row window of precision 'S' (36 rows of a 512-pixel template):
+// three resident assembly / trial CTAs per SM, the register limit of those kernels.
+constexpr int kWinBytes = 72 * 1024;
 // Shared memory for the template rows of one line-search CTA (98 rows of a 512-pixel template;
 // with the kernel's static shared memory one 1024-thread CTA per SM).
 constexpr int kLsWinBytes = 196 * 1024;
@@ -148,6 +148,7 @@ static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupD
   if (!attr_set) {
     cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kAssemble>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
     cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
+    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kCorr>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
     attr_set = true;
   }
   const int rows = stage_bytes<Acc>(max_hb) <= (size_t)kStageBytes ? max_hb : 0;
@@ -157,6 +158,8 @@ static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupD
   const size_t smem = (rows ? stage_bytes<Acc>(rows) : 0) + (win_bytes ? (size_t)win_bytes + 16 : 0) + 64;
   if (mode == kAssemble)
     k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
+  else if (mode == kCorr)
+    k_eval<Acc, FrameT, TplT, kCorr><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
   else
     k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
   return cudaGetLastError();
@@ -189,9 +192,29 @@ static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, co
   return cudaLaunchKernelEx(&cfg, k_linesearch<Acc, FrameT, TplT>, gd, fg, ctl, win_bytes);
 }
 
+using RoundFn = cudaError_t (*)(int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, GroupCtl* ctl,
+                                int win_bytes);
+
+// One line-search trial round of precision 'S' over the assembly tiles.
+template <class FrameT, class TplT>
+static cudaError_t round_launch(int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, GroupCtl* ctl,
+                                int win_bytes) {
+  if (tiles <= 0) return cudaSuccess;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_trial_round<FrameT, TplT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWinBytes + 16);
+    attr_set = true;
+  }
+  win_bytes = std::min(win_bytes, kWinBytes) & ~15;
+  k_trial_round<FrameT, TplT><<<tiles, 32 * kEvalWarps, win_bytes ? (size_t)win_bytes + 16 : 0, s>>>(gd, tg, ctl,
+                                                                                                      win_bytes);
+  return cudaGetLastError();
+}
+
 struct KernelSet {
   EvalFn eval;
   LsFn ls;
+  RoundFn round;  // precision 'S' only
 };
 template <class FrameT>
 static void sum_launch(const void* img, size_t n, double* parts, double* out, cudaStream_t s) {
@@ -201,7 +224,10 @@ static void sum_launch(const void* img, size_t n, double* parts, double* out, cu
 
 template <class Acc, class FrameT, class TplT>
 static KernelSet kset() {
-  return {eval_launch<Acc, FrameT, TplT>, ls_launch<Acc, FrameT, TplT>};
+  if constexpr (sizeof(Acc) == 4)
+    return {eval_launch<Acc, FrameT, TplT>, ls_launch<Acc, FrameT, TplT>, round_launch<FrameT, TplT>};
+  else
+    return {eval_launch<Acc, FrameT, TplT>, ls_launch<Acc, FrameT, TplT>, nullptr};
 }
 
 static KernelSet pick_kernels(int compute, int fdt, int tdt) {
@@ -557,7 +583,7 @@ struct Batch::Impl {
   int* h_counters = nullptr;  // pinned
   int n_tiles = 0, n_frames_total = 0;
   int max_hb = 0;  // largest block height among groups whose geometry k_eval stages in shared memory
-  KernelSet ks = {nullptr, nullptr};
+  KernelSet ks = {nullptr, nullptr, nullptr};
   SumFn sum = nullptr;
   std::vector<GroupCtl> h_ctl;
   double init_ms = 0, run_ms = 0;
@@ -581,7 +607,8 @@ struct Batch::Impl {
       }
       cudaEventRecord(events[event_used], stream);
     }
-    if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl, ls_win_bytes);
+    if (mode == kTrial && ks.round) ks.round(n_tiles, stream, d_gd, d_tile_group, d_ctl, win_bytes);
+    else if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl, ls_win_bytes);
     else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb, win_bytes);
     launches++;
     if (timing) {
@@ -614,6 +641,7 @@ static void layout(Batch::Impl* b, char* base) {
   std::vector<GroupDesc>& gd = b->gd;
   gd.assign(b->hg.size(), GroupDesc{});
   b->d_err = cv.take<int>(1);
+  b->d_counters = cv.take<int>(4);
   b->d_staging = cv.take<unsigned long long>(6);
   b->d_sum_parts = cv.take<double>(kSumBlocks);
   b->win_bytes = 0;
@@ -664,6 +692,7 @@ static void layout(Batch::Impl* b, char* base) {
       G.col_yrange = b->compute == 1 ? cv.take<float>(2 * (size_t)g.W) : nullptr;
     }
     G.err = b->d_err;
+    G.searching = b->d_counters;
     G.staging = b->d_staging;
     g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
     G.image = g.frames_dev ? g.frames_dev : g.d_image;
@@ -711,6 +740,7 @@ static void layout(Batch::Impl* b, char* base) {
     G.kdiff = cv.take<double>(nF * 2 * (g.W + 1));
     G.fstate = cv.take<uint8_t>(nF);
     G.ls_trials = cv.take<int>(nF);
+    G.ls_done = cv.take<int>(nF);
     G.eig_c = cv.take<double>(4 * N);
     G.eig_valid = cv.take<uint8_t>(N);
     G.list = cv.take<int>(2 * N);
@@ -733,7 +763,6 @@ static void layout(Batch::Impl* b, char* base) {
   b->d_ctl = cv.take<GroupCtl>(gd.size());
   b->d_tile_group = cv.take<int>(std::max(1, b->n_tiles));
   b->d_frame_group = cv.take<int>(std::max(1, b->n_frames_total));
-  b->d_counters = cv.take<int>(4);
   b->arena_bytes = cv.off + 256;
 }
 
@@ -881,6 +910,7 @@ static int reset_state(Batch::Impl* b) {
     SS_CK(cudaMemsetAsync(G.grp_active + 2 * (size_t)g.n_rg, 0, 1, s));
     SS_CK(cudaMemsetAsync(G.o_frame_corr, 0, nF * 8, s));
     SS_CK(cudaMemsetAsync(G.eig_valid, 0, N, s));
+    SS_CK(cudaMemsetAsync(G.ls_done, 0, nF * sizeof(int), s));
     k_fill<<<64, 256, 0, s>>>(G.errval, 2 * nF, kErrvalFill);
     // the reference's x/y/mask/difference buffers start zero-filled: NaN knots give an all-invalid
     // mask and a zero difference image
@@ -925,8 +955,26 @@ static int run_cycles(Batch::Impl* b) {
     k_solve<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
     b->launches++;
     SS_CK(cudaGetLastError());
-    b->rounds++;
-    b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
+    if (b->ks.round) {
+      // trial rounds until no frame searches: a first block of rounds, then the searching count
+      int block = 6;
+      for (int guard = 0;; guard++) {
+        for (int r = 0; r < block; r++) {
+          b->rounds++;
+          b->eval_timed(kTrial);
+        }
+        SS_CK(cudaGetLastError());
+        SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SS_CK(cudaStreamSynchronize(s));
+        if (b->h_counters[0] <= 0) break;
+        if (guard > kTrialCap) return fail(SS_ERR_CUDA, "line search did not finish within the trial bound");
+        block = 4;
+      }
+      b->eval_timed(kCorr);  // correlation sums after the second half-step
+    } else {
+      b->rounds++;
+      b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
+    }
     SS_CK(cudaGetLastError());
     k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
     k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);

@@ -433,6 +433,7 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
   const GroupDesc& G = gds[g];
   const GroupCtl& C = ctl[g];
   if (C.phase != (MODE == kFinal ? kPhFinal : kPhHalf)) return;
+  if (MODE == kCorr && C.shift != 1) return;  // correlation sums after the second half-step
   const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
   const int nfb = (G.nF + fpc - 1) / fpc;
   const int local = blockIdx.x - G.tile_base;
@@ -533,6 +534,8 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
       if (MODE == kAssemble && win.p && G.pair_ok && !k.dual) {
         assemble_pairs<FrameT>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt);
         if ((threadIdx.x & 31) == 0) atomicAdd(G.staging + 5, 1ull);
+      } else if (MODE != kAssemble && win.p && G.pair_ok && !k.dual) {
+        corr_pairs<FrameT, MODE>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt, mo);
       } else if (win.p) {
         if (affine) eval_column<Acc, FrameT, TplT, MODE, true, true>(G, coli, geo, k, out, cnt, mo, cc, win);
         else eval_column<Acc, FrameT, TplT, MODE, false, true>(G, coli, geo, k, out, cnt, mo, cc, win);
@@ -839,6 +842,222 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
     }
   }
   cluster.sync();  // no CTA leaves while others may still read its shared memory
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// Line search in trial rounds (precision 'S')
+//
+// A round evaluates one trial (pnew = p + deltaP on the frame's own knots, the right boundary knot
+// fixed: task_linesearch.cu:50-54) of every frame still searching, over the assembly tiles (block
+// column cc x a chunk of frames) with the template rows of the tile in shared memory. Each column
+// writes its SSD and valid count; the warp that completes a frame's last column (a device-wide
+// arrival count per frame) makes the frame's decision of task_linesearch.cu:95-149: accept, halve
+// deltaP and search on, or stop. Rounds repeat until no frame searches.
+
+constexpr int kMaxChunk = 64;       // frames_per_cta bound
+
+// Device-scope fetch-and-add with acquire-release order: the writes before it are visible to a
+// thread that observes the new count, and the caller sees every write released before the count
+// it read.
+__device__ __forceinline__ int atomic_add_acq_rel(int* p, int v) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+constexpr int kMinWinFrames = 4;    // searching frames of a tile worth staging a window for
+
+// Decision for frame f after all its columns of the round were evaluated (one warp).
+__device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f) {
+  const int lane = threadIdx.x & 31;
+  const int W = G.W, N = G.N, b0 = f * W, shift = C.shift;
+  const bool last_frame = f + 1 == G.nF;
+  const double bx = G.p_snap[b0 + W], by = G.p_snap[N + b0 + W];
+  double a = 0, m = 0, rg = 0, b = 0;
+  bool pr = false;
+  for (int t = lane; t < W; t += 32) {
+    const int c = b0 + t;
+    a += __ldcg(G.colsum + (size_t)c * kCsStride + kCsSsd);
+    const int n = __ldcg(G.colcnt + c);
+    b += (double)n;
+    pr |= n >= G.min_points[t];
+    const double dx = G.delta_p[c], dy = G.delta_p[N + c];
+    m = fmax(m, fmax(fabs(dx), fabs(dy)));
+    if (G.lambda != 0.0) {  // knot-difference regulariser of the trial (extension)
+      const double x0 = G.p[c] + dx, y0 = G.p[N + c] + dy;
+      const double x1 = t + 1 < W ? G.p[c + 1] + G.delta_p[c + 1] : bx;
+      const double y1 = t + 1 < W ? G.p[N + c + 1] + G.delta_p[N + c + 1] : by;
+      rg += (x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0);
+    }
+  }
+  a = warp_sum(a);
+  b = warp_sum(b);
+  rg = warp_sum(rg);
+  pr = __any_sync(0xffffffffu, pr);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  // actions: 0 accept, 1 reduce and retry, 2 stop; bit 4: a block was present (the difference
+  // image was written)
+  int action = 0;
+  if (lane == 0) {
+    const double thr = G.move_thresh, rho = G.ls_mult;
+    double ev = 0;
+    if (pr) {
+      ev = (G.lambda != 0.0) ? (a + G.lambda * rg) / b : a / b;
+      if (ev < G.errval[shift * G.nF + f]) action = 0;
+      else action = (m > thr) ? 1 : 2;  // d_checkMovement before d_reduceDeltaP
+      action |= 16;
+    } else {
+      action = (m * rho > thr) ? 1 : 2;  // d_reduceDeltaP before d_checkMovement
+    }
+    const int trials = ++G.ls_trials[f];
+    atomicAdd((unsigned long long*)&C.n_eval, 1ull);
+    atomicAdd((unsigned long long*)&C.passes[kTrial], 1ull);
+    if ((action & 15) == 1 && trials >= kTrialCap) {
+      action = (action & 16) | 2;
+      C.cap_hit = 1;
+    }
+    if ((action & 15) == 0 && b0 == 0) G.errval[shift * G.nF] = ev;  // only idx == 0 writes (:135)
+  }
+  action = __shfl_sync(0xffffffffu, action, 0);
+  const double rho = G.ls_mult;
+  double* km = G.kmask + (size_t)f * 2 * (W + 1);
+  double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
+  for (int t = lane; t <= W; t += 32) {
+    for (int d = 0; d < 2; d++) {
+      const size_t o = (size_t)d * N + b0 + t;
+      const double v = t < W ? G.p[o] + G.delta_p[o] : (last_frame ? kPnewFill : (d ? by : bx));
+      km[d * (W + 1) + t] = v;
+      if (action & 16) kd[d * (W + 1) + t] = v;
+      if (t < W) {
+        if ((action & 15) == 0) G.p[o] = v;
+        else if ((action & 15) == 1) G.delta_p[o] *= rho;
+        else if (!(action & 16)) G.delta_p[o] *= rho;  // absent block: reduced before the stop test
+      }
+    }
+  }
+  if (lane == 0) {
+    G.ls_done[f] = 0;
+    if ((action & 15) != 1) {
+      G.fstate[f] = 0;
+      atomicSub(G.searching, 1);
+    }
+  }
+}
+
+template <class FrameT, class TplT>
+__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
+    k_trial_round(const GroupDesc* __restrict__ gds, const int* __restrict__ tile_group, GroupCtl* __restrict__ ctl,
+                  int win_bytes) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_list[kMaxChunk];
+  __shared__ int s_n;
+  const int g = tile_group[blockIdx.x];
+  const GroupDesc& G = gds[g];
+  GroupCtl& C = ctl[g];
+  if (C.phase != kPhHalf) return;
+  const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
+  const int nfb = (G.nF + fpc - 1) / fpc;
+  const int local = blockIdx.x - G.tile_base;
+  const int cc = local / nfb, fb = local - cc * nfb;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int f0 = fb * fpc, f_end = min(G.nF, f0 + fpc);
+
+  // the chunk's searching frames; fstate of a frame changes only in its decision, which follows
+  // the evaluation of all its columns of the round
+  if (warp == 0) {
+    int n = 0;
+    for (int fa = f0; fa < f_end; fa += 32) {
+      const int f = fa + lane;
+      const bool s = f < f_end && (G.fstate[f] & 2);
+      const unsigned bal = __ballot_sync(0xffffffffu, s);
+      if (s) s_list[n + __popc(bal & ((1u << lane) - 1u))] = f;
+      n += __popc(bal);
+    }
+    if (lane == 0) s_n = n;
+  }
+  __syncthreads();
+  const int ns = s_n;
+  if (ns == 0) return;
+
+  // trial knots of this column: own knots p + deltaP, the frame's right boundary fixed
+  auto knots = [&](int f, float& x0, float& x1, float& y0, float& y1) {
+    const int b0 = f * W, c = b0 + cc;
+    x0 = (float)(G.p[c] + G.delta_p[c]);
+    y0 = (float)(G.p[N + c] + G.delta_p[N + c]);
+    if (cc + 1 < W) {
+      x1 = (float)(G.p[c + 1] + G.delta_p[c + 1]);
+      y1 = (float)(G.p[N + c + 1] + G.delta_p[N + c + 1]);
+    } else if (f + 1 == G.nF) {
+      x1 = y1 = (float)kPnewFill;
+    } else {
+      x1 = (float)G.p_snap[b0 + W];
+      y1 = (float)G.p_snap[N + b0 + W];
+    }
+  };
+
+  TWin win{nullptr, 0, 0, 0};
+  const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
+  if (win_cap >= 2 && !G.gquad && ns >= kMinWinFrames) {
+    float klo = INFINITY, khi = -INFINITY;
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+      float x0, x1, y0, y1;
+      knots(s_list[i], x0, x1, y0, y1);
+      klo = fminf(klo, fminf(y0, y1));
+      khi = fmaxf(khi, fmaxf(y0, y1));
+    }
+    block_minmax(klo, khi);
+    int r0, rows;
+    window_rows(G, G.col_yrange[2 * cc] + klo, G.col_yrange[2 * cc + 1] + khi, win_cap, r0, rows);
+    if (rows > 0) {
+      float* wbuf = reinterpret_cast<float*>(smem);
+      uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)win_bytes);
+      if (threadIdx.x == 0) mbar_init(bar);
+      __syncthreads();
+      unsigned phase = 0;
+      if (stage_window(G, wbuf, r0, rows, bar, phase)) win = {wbuf, r0, rows, G.tpitch};
+    }
+  }
+  if (threadIdx.x == 0) {
+    atomicAdd(G.staging + 2, 1ull);
+    if (win.p) atomicAdd(G.staging + 3, 1ull);
+    if (win.p && G.pair_ok) atomicAdd(G.staging + 4, 1ull);
+  }
+
+  const bool affine = G.geo_k > 0;
+  for (int i = warp; i < ns; i += kEvalWarps) {
+    const int f = s_list[i];
+    const int c = f * W + cc;
+    const size_t coli = (size_t)c * Hb;
+    float x0, x1, y0, y1;
+    knots(f, x0, x1, y0, y1);
+    double ssd;
+    int cnt;
+    if (win.p && G.pair_ok) {
+      trial_pairs<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(win), ssd, cnt);
+    } else {
+      ColKnots<float> k;
+      set_knots(k, x0, x1, y0, y1, x0, x1, y0, y1);
+      double out[kCsStride];
+      const ColGeo<float> geo = global_geo<float>(G, cc);
+      if (win.p) {
+        if (affine) eval_column<float, FrameT, TplT, kTrial, true, true>(G, coli, geo, k, out, cnt, nullptr, cc, win);
+        else eval_column<float, FrameT, TplT, kTrial, false, true>(G, coli, geo, k, out, cnt, nullptr, cc, win);
+      } else {
+        if (affine) eval_column<float, FrameT, TplT, kTrial, true>(G, coli, geo, k, out, cnt, nullptr, cc);
+        else eval_column<float, FrameT, TplT, kTrial>(G, coli, geo, k, out, cnt, nullptr);
+      }
+      ssd = out[kCsSsd];
+    }
+    int prev = 0;
+    if (lane == 0) {
+      G.colsum[(size_t)c * kCsStride + kCsSsd] = ssd;
+      G.colcnt[c] = cnt;
+      prev = atomic_add_acq_rel(G.ls_done + f, 1);  // releases this column's results
+    }
+    prev = __shfl_sync(0xffffffffu, prev, 0);
+    if (prev == W - 1) ls_decide(G, C, f);  // acquired every column of the frame
+  }
 }
 
 }  // namespace ss

@@ -253,6 +253,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
   if (t == 0) {
     C.n_eval += sh_nact;
     C.passes[kAssemble] += nF;
+    atomicAdd(G.searching, sh_nact);  // frames whose line search starts (trial rounds)
   }
 
   // (2) compaction: list position of every used knot (paramsUsed[N-1] is never written, so it

@@ -68,6 +68,11 @@ struct PairLoad<double> {
   __device__ static float2 cvt(W w) { return make_float2((float)w.x, (float)w.y); }
 };
 
+// Steps (64 rows) of frame samples a warp keeps in flight: trial evaluation (32-bit sample pairs;
+// fewer for wider frame types), assembly (whose 14 accumulators leave fewer registers).
+constexpr int kPrefetch = 8;
+constexpr int kPrefetchAsm = 2;
+
 // Per-warp constants of one block column for the pair loop.
 struct PairCol {
   float2 bxj, cx, byj, cy;  // x = bxj * j + cx, y = byj * j + cy (both halves)
@@ -78,9 +83,9 @@ struct PairCol {
 
 // Column constants for knots (kx0, kx1, ky0, ky1) of block column cc (lane-dependent halves).
 __device__ __forceinline__ PairCol pair_col(const GroupDesc& G, int cc, float kx0, float kx1, float ky0, float ky1) {
-  const int lane = threadIdx.x & 31, k = G.geo_k, L = G.geo_L;
+  const int lane = threadIdx.x & 31, k = G.geo_k, L = G.geo_L, ks = __ffs(k) - 1;  // k = 2^ks
   const int rA = 2 * lane, rB = 2 * lane + 1;
-  const int lA = rA % k, lB = rB % k;
+  const int lA = rA & (k - 1), lB = rB & (k - 1);
   const float fs = G.geo_fs;
   const float f0A = ((float)(lA * L) + 0.5f) * fs, f0B = ((float)(lB * L) + 0.5f) * fs;
   const float dkx = kx1 - kx0, dky = ky1 - ky0;
@@ -92,8 +97,8 @@ __device__ __forceinline__ PairCol pair_col(const GroupDesc& G, int cc, float kx
             fmaf(dky, f0B, fmaf(G.geo_ay, (float)(cc * k + lB), G.geo_by) + ky0));
   p.fsj = f2(fs);
   p.f0 = f2(f0A, f0B);
-  p.j0 = f2((float)(rA / k), (float)(rB / k));
-  p.dj = (float)(64 / k);
+  p.j0 = f2((float)(rA >> ks), (float)(rB >> ks));
+  p.dj = (float)(64 >> ks);
   return p;
 }
 
@@ -151,51 +156,60 @@ __device__ __forceinline__ void assemble_pairs(const GroupDesc& G, size_t coli, 
   int cnt = 0;
   float2 j = pc.j0;
   const float2 dj = f2(pc.dj), one = f2(1.0f);
-  typename PL::W nxt = PL::load(col, lane);
+  // kPrefetchAsm steps of frame samples in flight (a register ring)
+  typename PL::W ring[kPrefetchAsm];
+#pragma unroll
+  for (int d = 0; d < kPrefetchAsm; d++) ring[d] = d < steps ? PL::load(col, d * 32 + lane) : typename PL::W{};
 #pragma unroll 1
-  for (int t = 0; t < steps; t++) {
-    const typename PL::W cur = nxt;
-    if (t + 1 < steps) nxt = PL::load(col, (t + 1) * 32 + lane);
-    const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy), f = fma2(pc.fsj, j, pc.f0);
-    j = add2(j, dj);
-    const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
-    const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
-    cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
-    float2 xf, yf, t00, t01, t10, t11;
-    pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
-    const float2 gy0 = sub2(t10, t00), gy1 = sub2(t11, t01);
-    const float2 gx0 = sub2(t01, t00), gx1 = sub2(t11, t10);
-    const float2 a = fma2(yf, gy0, t00), b = fma2(yf, gy1, t01);
-    const float2 wI = fma2(xf, sub2(b, a), a);
-    float2 wx = fma2(yf, sub2(gx1, gx0), gx0);
-    float2 wy = fma2(xf, sub2(gy1, gy0), gy0);
-    float2 d = sub2(PL::cvt(cur), wI);
-    d = f2(mA ? d.x : 0.f, mB ? d.y : 0.f);
-    wx = f2(mA ? wx.x : 0.f, mB ? wx.y : 0.f);
-    wy = f2(mA ? wy.x : 0.f, mB ? wy.y : 0.f);
-    const float2 c = sub2(one, f);
-    const float2 csq = mul2(c, c), fsq = mul2(f, f), fc = mul2(f, c);
-    const float2 gxx = mul2(wx, wx), gyy = mul2(wy, wy), gxy = mul2(wx, wy);
-    ssd = fma2(d, d, ssd);
-    axx = fma2(gxx, csq, axx);
-    ayy = fma2(gyy, csq, ayy);
-    axy = fma2(gxy, csq, axy);
-    bxx = fma2(gxx, fsq, bxx);
-    byy = fma2(gyy, fsq, byy);
-    bxy = fma2(gxy, fsq, bxy);
-    oxx = fma2(gxx, fc, oxx);
-    oyy = fma2(gyy, fc, oyy);
-    oxy = fma2(gxy, fc, oxy);
-    const float2 d1 = mul2(d, c), d2 = mul2(d, f);
-    j1x = fma2(d1, wx, j1x);
-    j1y = fma2(d1, wy, j1y);
-    j2x = fma2(d2, wx, j2x);
-    j2y = fma2(d2, wy, j2y);
+  for (int t0 = 0; t0 < steps; t0 += kPrefetchAsm) {
+#pragma unroll
+    for (int d = 0; d < kPrefetchAsm; d++) {
+      const int t = t0 + d;
+      if (t >= steps) break;
+      const typename PL::W cur = ring[d];
+      if (t + kPrefetchAsm < steps) ring[d] = PL::load(col, (t + kPrefetchAsm) * 32 + lane);
+      const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy), f = fma2(pc.fsj, j, pc.f0);
+      j = add2(j, dj);
+      const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+      const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+      cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+      float2 xf, yf, t00, t01, t10, t11;
+      pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+      const float2 gy0 = sub2(t10, t00), gy1 = sub2(t11, t01);
+      const float2 gx0 = sub2(t01, t00), gx1 = sub2(t11, t10);
+      const float2 a = fma2(yf, gy0, t00), b = fma2(yf, gy1, t01);
+      const float2 wI = fma2(xf, sub2(b, a), a);
+      float2 wx = fma2(yf, sub2(gx1, gx0), gx0);
+      float2 wy = fma2(xf, sub2(gy1, gy0), gy0);
+      float2 d2 = sub2(PL::cvt(cur), wI);
+      d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
+      wx = f2(mA ? wx.x : 0.f, mB ? wx.y : 0.f);
+      wy = f2(mA ? wy.x : 0.f, mB ? wy.y : 0.f);
+      const float2 c = sub2(one, f);
+      const float2 csq = mul2(c, c), fsq = mul2(f, f), fc = mul2(f, c);
+      const float2 gxx = mul2(wx, wx), gyy = mul2(wy, wy), gxy = mul2(wx, wy);
+      ssd = fma2(d2, d2, ssd);
+      axx = fma2(gxx, csq, axx);
+      ayy = fma2(gyy, csq, ayy);
+      axy = fma2(gxy, csq, axy);
+      bxx = fma2(gxx, fsq, bxx);
+      byy = fma2(gyy, fsq, byy);
+      bxy = fma2(gxy, fsq, bxy);
+      oxx = fma2(gxx, fc, oxx);
+      oyy = fma2(gyy, fc, oyy);
+      oxy = fma2(gxy, fc, oxy);
+      const float2 d1 = mul2(d2, c), dd2 = mul2(d2, f);
+      j1x = fma2(d1, wx, j1x);
+      j1y = fma2(d1, wy, j1y);
+      j2x = fma2(dd2, wx, j2x);
+      j2y = fma2(dd2, wy, j2y);
+    }
   }
+  // the block's partials reduced in FP32, combined in FP64 by the solve
   cnt_out = warp_sum(cnt);
   const float2 v[kCsAssemble] = {ssd, axx, ayy, axy, bxx, byy, bxy, oxx, oyy, oxy, j1x, j1y, j2x, j2y};
 #pragma unroll
-  for (int i = 0; i < kCsAssemble; i++) out[i] = warp_sum((double)(v[i].x + v[i].y));
+  for (int i = 0; i < kCsAssemble; i++) out[i] = (double)warp_sumf(v[i].x + v[i].y);
 }
 
 // Trial SSD and valid count of one block column (task_linesearch.cu:50-74 with the SSD of
@@ -212,29 +226,120 @@ __device__ __forceinline__ void trial_pairs(const GroupDesc& G, size_t coli, con
   int cnt = 0;
   float2 j = pc.j0;
   const float2 dj = f2(pc.dj);
-  // two steps of frame samples in flight
-  typename PL::W w0 = PL::load(col, lane);
-  typename PL::W w1 = steps > 1 ? PL::load(col, 32 + lane) : w0;
+  constexpr int kPf = sizeof(typename PL::W) <= 4 ? kPrefetch : (sizeof(typename PL::W) <= 8 ? 4 : 2);
+  typename PL::W ring[kPf];
+#pragma unroll
+  for (int d = 0; d < kPf; d++) ring[d] = d < steps ? PL::load(col, d * 32 + lane) : typename PL::W{};
 #pragma unroll 1
-  for (int t = 0; t < steps; t++) {
-    const typename PL::W cur = w0;
-    w0 = w1;
-    if (t + 2 < steps) w1 = PL::load(col, (t + 2) * 32 + lane);
-    const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
-    j = add2(j, dj);
-    const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
-    const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
-    cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
-    float2 xf, yf, t00, t01, t10, t11;
-    pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
-    const float2 a = fma2(yf, sub2(t10, t00), t00), b = fma2(yf, sub2(t11, t01), t01);
-    const float2 wI = fma2(xf, sub2(b, a), a);
-    float2 d = sub2(PL::cvt(cur), wI);
-    d = f2(mA ? d.x : 0.f, mB ? d.y : 0.f);
-    ssd = fma2(d, d, ssd);
+  for (int t0 = 0; t0 < steps; t0 += kPf) {
+#pragma unroll
+    for (int d = 0; d < kPf; d++) {
+      const int t = t0 + d;
+      if (t >= steps) break;
+      const typename PL::W cur = ring[d];
+      if (t + kPf < steps) ring[d] = PL::load(col, (t + kPf) * 32 + lane);
+      const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
+      j = add2(j, dj);
+      const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+      const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+      cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+      float2 xf, yf, t00, t01, t10, t11;
+      pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+      const float2 a = fma2(yf, sub2(t10, t00), t00), b = fma2(yf, sub2(t11, t01), t01);
+      const float2 wI = fma2(xf, sub2(b, a), a);
+      float2 d2 = sub2(PL::cvt(cur), wI);
+      d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
+      ssd = fma2(d2, d2, ssd);
+    }
   }
   cnt_out = warp_sum(cnt);
-  ssd_out = warp_sum((double)(ssd.x + ssd.y));
+  ssd_out = (double)warp_sumf(ssd.x + ssd.y);
+}
+
+// Correlation sums (kCsSumD .. kCsFrDI) of one block column whose mask and difference-image knots
+// agree, in the reference's definitions (task_correlation.cu:16-60, swapped difference image D'),
+// and for the final pass also the SSD at the mask knots and the mask output. The leading run of
+// valid pixels follows the row order: within a 64-row step lane L holds rows 2L and 2L + 1.
+template <class FrameT, int MODE>
+__device__ __forceinline__ void corr_pairs(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
+                                           double (&out)[kCsStride], int& cnt_out, uint8_t* mask_out) {
+  using PL = PairLoad<FrameT>;
+  const int lane = threadIdx.x & 31;
+  const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
+  const FrameT* col = reinterpret_cast<const FrameT*>(G.image) + coli;
+  const int steps = G.Hb >> 6;
+  const unsigned lt = (1u << lane) - 1u;
+  float2 sumd = f2(0.f), sn = f2(0.f), sd = f2(0.f), sdd = f2(0.f), si = f2(0.f), sii = f2(0.f), sdi = f2(0.f),
+         fd = f2(0.f), fi = f2(0.f), fdd = f2(0.f), fii = f2(0.f), fdi = f2(0.f), fssd = f2(0.f);
+  int cnt = 0;
+  bool run = true;
+  float2 j = pc.j0;
+  const float2 dj = f2(pc.dj);
+  typename PL::W ring[kPrefetchAsm];
+#pragma unroll
+  for (int d = 0; d < kPrefetchAsm; d++) ring[d] = d < steps ? PL::load(col, d * 32 + lane) : typename PL::W{};
+#pragma unroll 1
+  for (int t0 = 0; t0 < steps; t0 += kPrefetchAsm) {
+#pragma unroll
+    for (int d = 0; d < kPrefetchAsm; d++) {
+      const int t = t0 + d;
+      if (t >= steps) break;
+      const typename PL::W cur = ring[d];
+      if (t + kPrefetchAsm < steps) ring[d] = PL::load(col, (t + kPrefetchAsm) * 32 + lane);
+      const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
+      j = add2(j, dj);
+      const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+      const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+      cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+      float2 xf, yf, t00, t01, t10, t11;
+      pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+      const float2 a = fma2(yf, sub2(t10, t00), t00), b = fma2(yf, sub2(t11, t01), t01);
+      const float2 wI = fma2(xf, sub2(b, a), a);
+      const float2 img = PL::cvt(cur);
+      const float2 diff = sub2(img, wI);          // differenceImage at valid pixels
+      float2 dp = sub2(img, diff);                // after d_swapWIDiff
+      dp = f2(mA ? dp.x : 0.f, mB ? dp.y : 0.f);
+      sumd = add2(sumd, dp);
+      const float2 im = f2(mA ? img.x : 0.f, mB ? img.y : 0.f);
+      fd = add2(fd, dp);
+      fi = add2(fi, im);
+      fdd = fma2(dp, dp, fdd);
+      fii = fma2(im, im, fii);
+      fdi = fma2(dp, im, fdi);
+      const unsigned bothv = __ballot_sync(0xffffffffu, mA && mB);
+      const bool pre = run && (bothv & lt) == lt;
+      const bool inA = pre && mA, inB = inA && mB;
+      run = run && bothv == 0xffffffffu;
+      const float2 ds = f2(inA ? dp.x : 0.f, inB ? dp.y : 0.f);
+      const float2 is = f2(inA ? img.x : 0.f, inB ? img.y : 0.f);
+      sn = add2(sn, f2(inA ? 1.f : 0.f, inB ? 1.f : 0.f));
+      sd = add2(sd, ds);
+      sdd = fma2(ds, ds, sdd);
+      si = add2(si, is);
+      sii = fma2(is, is, sii);
+      sdi = fma2(ds, is, sdi);
+      if (MODE == kFinal) {
+        const float2 dm = f2(mA ? diff.x : 0.f, mB ? diff.y : 0.f);
+        fssd = fma2(dm, dm, fssd);
+        if (mask_out)
+          reinterpret_cast<uint16_t*>(mask_out)[t * 32 + lane] = (uint16_t)((mA ? 1u : 0u) | (mB ? 0x100u : 0u));
+      }
+    }
+  }
+  cnt_out = warp_sum(cnt);
+  out[kCsSumD] = (double)warp_sumf(sumd.x + sumd.y);
+  out[kCsSetN] = (double)warp_sumf(sn.x + sn.y);
+  out[kCsSetD] = (double)warp_sumf(sd.x + sd.y);
+  out[kCsSetDD] = (double)warp_sumf(sdd.x + sdd.y);
+  out[kCsSetI] = (double)warp_sumf(si.x + si.y);
+  out[kCsSetII] = (double)warp_sumf(sii.x + sii.y);
+  out[kCsSetDI] = (double)warp_sumf(sdi.x + sdi.y);
+  out[kCsFrD] = (double)warp_sumf(fd.x + fd.y);
+  out[kCsFrI] = (double)warp_sumf(fi.x + fi.y);
+  out[kCsFrDD] = (double)warp_sumf(fdd.x + fdd.y);
+  out[kCsFrII] = (double)warp_sumf(fii.x + fii.y);
+  out[kCsFrDI] = (double)warp_sumf(fdi.x + fdi.y);
+  out[kCsFinalSsd] = MODE == kFinal ? (double)warp_sumf(fssd.x + fssd.y) : 0.0;
 }
 
 }  // namespace ss
