@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -123,6 +124,22 @@ __global__ void k_fill(double* p, size_t n, double v) {
 // ---------------------------------------------------------------------------------------------
 // kernel dispatch by (compute, frame type, template type)
 
+// Opts a kernel into `bytes` of dynamic shared memory on the current device, once per device.
+template <class F>
+static cudaError_t smem_attr(F* fn, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const std::pair<int, const void*> key(dev, reinterpret_cast<const void*>(fn));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(key)) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.insert(key);
+  return e;
+}
+
 // Dynamic shared memory for staging one block column's geometry (tfrac, basex, basey, the next
 // column's tfrac and base_mask) in k_eval.
 constexpr int kStageBytes = 96 * 1024;
@@ -144,13 +161,10 @@ static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupD
                                const GroupCtl* ctl, int max_hb, int win_bytes) {
   if (tiles <= 0) return cudaSuccess;
   constexpr int kMaxDyn = kStageBytes + kWinBytes + 64;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kAssemble>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
-    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kFinal>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
-    cudaFuncSetAttribute(k_eval<Acc, FrameT, TplT, kCorr>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDyn);
-    attr_set = true;
-  }
+  cudaError_t ae = smem_attr(k_eval<Acc, FrameT, TplT, kAssemble>, kMaxDyn);
+  if (ae == cudaSuccess) ae = smem_attr(k_eval<Acc, FrameT, TplT, kFinal>, kMaxDyn);
+  if (ae == cudaSuccess) ae = smem_attr(k_eval<Acc, FrameT, TplT, kCorr>, kMaxDyn);
+  if (ae != cudaSuccess) return ae;
   const int rows = stage_bytes<Acc>(max_hb) <= (size_t)kStageBytes ? max_hb : 0;
   if (sizeof(Acc) != 4) win_bytes = 0;
   win_bytes = std::min(win_bytes, kWinBytes) & ~15;
@@ -171,11 +185,9 @@ static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, co
   if (frames <= 0) return cudaSuccess;
   if (sizeof(Acc) != 4) win_bytes = 0;
   win_bytes = std::min(win_bytes, kLsWinBytes) & ~15;
-  static bool attr_set = false;
-  if (!attr_set && sizeof(Acc) == 4) {
-    cudaFuncSetAttribute(k_linesearch<Acc, FrameT, TplT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kLsWinBytes + 16);
-    attr_set = true;
+  if (win_bytes) {
+    cudaError_t ae = smem_attr(k_linesearch<Acc, FrameT, TplT>, kLsWinBytes + 16);
+    if (ae != cudaSuccess) return ae;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(frames * kLsCluster, 1, 1);
@@ -200,11 +212,8 @@ template <class FrameT, class TplT>
 static cudaError_t round_launch(int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, GroupCtl* ctl,
                                 int win_bytes) {
   if (tiles <= 0) return cudaSuccess;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_trial_round<FrameT, TplT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWinBytes + 16);
-    attr_set = true;
-  }
+  cudaError_t ae = smem_attr(k_trial_round<FrameT, TplT>, kWinBytes + 16);
+  if (ae != cudaSuccess) return ae;
   win_bytes = std::min(win_bytes, kWinBytes) & ~15;
   k_trial_round<FrameT, TplT><<<tiles, 32 * kEvalWarps, win_bytes ? (size_t)win_bytes + 16 : 0, s>>>(gd, tg, ctl,
                                                                                                       win_bytes);
@@ -943,8 +952,16 @@ static int reset_state(Batch::Impl* b) {
   return SS_OK;
 }
 
+// Dynamic shared memory of k_solve and k_block_tridiag: the separator system of the partitioned
+// solve and the partitions' first-interior relations.
+constexpr size_t kSolveSmem = (size_t)kSolveThreads * kPartSmemStride * sizeof(double);
+
+// Opts k_block_tridiag into kSolveSmem of dynamic shared memory.
+static cudaError_t block_tridiag_attr() { return smem_attr(k_block_tridiag, (int)kSolveSmem); }
+
 static int run_cycles(Batch::Impl* b) {
   cudaStream_t s = b->stream;
+  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
   const int nG = (int)b->gd.size();
   int max_iter = 1;
   for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
@@ -952,7 +969,7 @@ static int run_cycles(Batch::Impl* b) {
   for (int cycle = 0; cycle < max_cycles; cycle++) {
     b->cycles++;
     b->eval_timed(kAssemble);
-    k_solve<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+    k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
     b->launches++;
     SS_CK(cudaGetLastError());
     if (b->ks.round) {
@@ -1197,7 +1214,9 @@ int ss_solve_block_tridiagonal_noalloc(int32_t n, const double* diag, const doub
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // every node of the workspace that the solve reads is written first by k_block_tridiag
-  ss::k_block_tridiag<<<1, ss::kSolveThreads, 0, s>>>(n, diag, coupling, rhs, x, work);
+  cudaError_t ea = ss::block_tridiag_attr();
+  if (ea != cudaSuccess) return ss::fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
+  ss::k_block_tridiag<<<1, ss::kSolveThreads, ss::kSolveSmem, s>>>(n, diag, coupling, rhs, x, work);
   cudaError_t e = cudaGetLastError();
   cudaError_t e2 = cudaStreamSynchronize(s);
   if (e != cudaSuccess || e2 != cudaSuccess)
@@ -1215,7 +1234,9 @@ int ss_solve_block_tridiagonal(int32_t n, const double* diag, const double* coup
   double* work = nullptr;
   cudaError_t e = cudaMallocAsync(&work, (size_t)n * ss::kCrStride * sizeof(double), s);
   if (e != cudaSuccess) return ss::fail(SS_ERR_OUT_OF_MEMORY, std::string("workspace: ") + cudaGetErrorString(e));
-  ss::k_block_tridiag<<<1, ss::kSolveThreads, 0, s>>>(n, diag, coupling, rhs, x, work);
+  cudaError_t ea = ss::block_tridiag_attr();
+  if (ea != cudaSuccess) return ss::fail(SS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
+  ss::k_block_tridiag<<<1, ss::kSolveThreads, ss::kSolveSmem, s>>>(n, diag, coupling, rhs, x, work);
   e = cudaGetLastError();
   cudaError_t e2 = cudaFreeAsync(work, s);
   cudaError_t e3 = cudaStreamSynchronize(s);

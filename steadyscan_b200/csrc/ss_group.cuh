@@ -95,37 +95,228 @@ __device__ void cr_solve(double* cr, int h) {
   }
 }
 
+
+__device__ __forceinline__ M2 m2_t(const M2& x) { return {x.a, x.c, x.b, x.d}; }
+__device__ __forceinline__ M2 m2_add(const M2& x, const M2& y) { return {x.a + y.a, x.b + y.b, x.c + y.c, x.d + y.d}; }
+__device__ __forceinline__ void m2_mv(const M2& m, double v0, double v1, double& r0, double& r1) {
+  r0 = m.a * v0 + m.b * v1;
+  r1 = m.c * v0 + m.d * v1;
+}
+__device__ __forceinline__ M2 sym_inv(double d0, double d1, double d2) { return m2_inv({d0, d2, d2, d1}); }
+
+// Node layout of the partitioned block-tridiagonal solve: the h nodes are split into P =
+// min(blockDim.x, h) contiguous partitions, the first rem = h - q P of q + 1 nodes and the rest of q;
+// every field of every node has a plane of h doubles in which node k of partition t sits at
+// k P + t, so the threads of a warp, each walking its own partition, touch consecutive doubles.
+constexpr int kRelStride = 10;                      // uL (4), uR (4), u0 (2)
+constexpr int kPartSmemStride = kCrStride + kRelStride;  // shared doubles per partition
+
+enum PartPlane : int {
+  kPD0 = 0, kPD1, kPD2,         // D (xx yy xy); after the forward sweep D~^-1
+  kPR0, kPR1, kPR2, kPR3,       // R, the block coupling the node to the next: [[R0 R1] [R2 R3]]
+  kPB0, kPB1,                   // b; after the forward sweep b~
+  kPS0, kPS1, kPS2, kPS3,       // forward spike S~
+  kPlanes
+};
+
+struct PartLayout {
+  int h, P, q, rem;
+  __device__ PartLayout(int h_, int nt) : h(h_), P(min(nt, h_)), q(h_ / min(nt, h_)), rem(h_ - (h_ / min(nt, h_)) * min(nt, h_)) {}
+  __device__ int a(int t) const { return t * q + min(t, rem); }
+  __device__ int m(int t) const { return q + (t < rem ? 1 : 0); }
+  __device__ size_t pos(int t, int k) const { return (size_t)k * P + t; }
+  __device__ size_t pos_of(int i) const {  // plane position of node i
+    const int lo = rem * (q + 1);
+    if (i < lo) {
+      const int t = i / (q + 1);
+      return pos(t, i - t * (q + 1));
+    }
+    const int j = i - lo, t = rem + j / q;
+    return pos(t, j - (t - rem) * q);
+  }
+};
+
+// Solves the symmetric positive definite block-tridiagonal system of h nodes given in the planes
+// of pl (PartLayout of h and blockDim.x; L_i = R_{i-1}^T) with the whole CTA and writes x_i to
+// xo[i * xs] and yo[i * ys]. Partition method: thread t eliminates the interior of its partition
+// by block Thomas sweeps (backward for the relation of the first interior node, forward storing
+// D~^-1, S~ and b~), leaving its last node as separator; the separators' Schur complement is block
+// tridiagonal again and is solved by block cyclic reduction in shared memory (red: blockDim.x x
+// kCrStride doubles); the interior follows by back substitution. For SPD systems every block
+// elimination is a Schur complement of an SPD matrix, so this solves the same equations as the
+// reference's exact solvers (eigensolve.cpp:35-38, cusolversolver.cu:53-56) in another
+// elimination order. red holds blockDim.x x kPartSmemStride doubles: the separator system and
+// each partition's first-interior relation.
+__device__ void part_solve(double* pl, int h, double* red, double* xo, int xs, double* yo, int ys) {
+  const int t = threadIdx.x;
+  if (h <= 0) return;
+  const PartLayout L(h, blockDim.x);
+  const int P = L.P;
+  const bool own = t < P;
+  const int mt = own ? L.m(t) : 0;
+  const int a = own ? L.a(t) : 0;
+  const int e = a + mt - 1;
+  double* const D0 = pl + (size_t)kPD0 * h;
+  double* const D1 = pl + (size_t)kPD1 * h;
+  double* const D2 = pl + (size_t)kPD2 * h;
+  double* const R0 = pl + (size_t)kPR0 * h;
+  double* const R1 = pl + (size_t)kPR1 * h;
+  double* const R2 = pl + (size_t)kPR2 * h;
+  double* const R3 = pl + (size_t)kPR3 * h;
+  double* const B0 = pl + (size_t)kPB0 * h;
+  double* const B1 = pl + (size_t)kPB1 * h;
+  double* const S0 = pl + (size_t)kPS0 * h;
+  double* const S1 = pl + (size_t)kPS1 * h;
+  double* const S2 = pl + (size_t)kPS2 * h;
+  double* const S3 = pl + (size_t)kPS3 * h;
+  auto ldR = [&](size_t q) -> M2 { return {R0[q], R1[q], R2[q], R3[q]}; };
+  const M2 Z = {0, 0, 0, 0};
+  // coupling of node a to the previous separator (the last node of partition t - 1)
+  const M2 La = (own && t > 0) ? m2_t(ldR(L.pos(t - 1, L.m(t - 1) - 1))) : Z;
+
+  // backward sweep: relation x_a = u0 + uL x_(previous separator) + uR x_e of the first interior node
+  if (own && mt >= 2) {
+    size_t q = L.pos(t, mt - 2);
+    M2 Dc = {D0[q], D2[q], D2[q], D1[q]};
+    double b0 = B0[q], b1 = B1[q];
+    M2 S = ldR(q);
+    for (int k = mt - 3; k >= 0; k--) {
+      q = L.pos(t, k);
+      const M2 Ri = ldR(q);
+      const M2 Nm = m2_mul(Ri, m2_inv(Dc));
+      Dc = m2_sub({D0[q], D2[q], D2[q], D1[q]}, m2_mul(Nm, m2_t(Ri)));
+      double c0, c1;
+      m2_mv(Nm, b0, b1, c0, c1);
+      b0 = B0[q] - c0;
+      b1 = B1[q] - c1;
+      S = m2_neg(m2_mul(Nm, S));
+    }
+    const M2 Di = m2_inv(Dc);
+    const M2 uL = m2_neg(m2_mul(Di, La)), uR = m2_neg(m2_mul(Di, S));
+    double u0, u1;
+    m2_mv(Di, b0, b1, u0, u1);
+    double* r = red + (size_t)blockDim.x * kCrStride + (size_t)t * kRelStride;
+    r[0] = uL.a; r[1] = uL.b; r[2] = uL.c; r[3] = uL.d;
+    r[4] = uR.a; r[5] = uR.b; r[6] = uR.c; r[7] = uR.d;
+    r[8] = u0; r[9] = u1;
+  }
+  // forward sweep storing D~^-1, S~ and b~ of each interior node; relation of the last one
+  M2 uLe = Z, uRe = Z;
+  double u0e = 0, u1e = 0;
+  if (own && mt >= 2) {
+    size_t q = L.pos(t, 0);
+    M2 Di = m2_inv({D0[q], D2[q], D2[q], D1[q]});
+    double b0 = B0[q], b1 = B1[q];
+    M2 S = La;
+    M2 Rp = ldR(q);
+    for (int k = 0;; k++) {
+      D0[q] = Di.a; D1[q] = Di.d; D2[q] = 0.5 * (Di.b + Di.c);
+      S0[q] = S.a; S1[q] = S.b; S2[q] = S.c; S3[q] = S.d;
+      B0[q] = b0; B1[q] = b1;
+      if (k + 1 >= mt - 1) break;
+      q = L.pos(t, k + 1);
+      const M2 M = m2_mul(m2_t(Rp), Di);  // L_{i+1} D~_i^-1 with L_{i+1} = R_i^T
+      Di = m2_inv(m2_sub({D0[q], D2[q], D2[q], D1[q]}, m2_mul(M, Rp)));
+      double c0, c1;
+      m2_mv(M, b0, b1, c0, c1);
+      b0 = B0[q] - c0;
+      b1 = B1[q] - c1;
+      S = m2_neg(m2_mul(M, S));
+      Rp = ldR(q);
+    }
+    // Rp = R_{e-1}, Di = D~_{e-1}^-1
+    uRe = m2_neg(m2_mul(Di, Rp));
+    uLe = m2_neg(m2_mul(Di, S));
+    m2_mv(Di, b0, b1, u0e, u1e);
+  }
+  __syncthreads();
+  // separator rows of the reduced system
+  if (own) {
+    const size_t qe = L.pos(t, mt - 1);
+    M2 Dr = {D0[qe], D2[qe], D2[qe], D1[qe]};
+    double b0 = B0[qe], b1 = B1[qe];
+    // L_e = R_{e-1}^T: node e - 1 is an interior node, or the previous separator
+    const M2 Le = mt >= 2 ? m2_t(ldR(L.pos(t, mt - 2))) : La;
+    const M2 Re = e + 1 < h ? ldR(qe) : Z;
+    M2 Lr = Z, Rr = Z;
+    double c0, c1;
+    if (mt >= 2) {
+      Dr = m2_add(Dr, m2_mul(Le, uRe));
+      Lr = m2_mul(Le, uLe);
+      m2_mv(Le, u0e, u1e, c0, c1);
+      b0 -= c0;
+      b1 -= c1;
+    } else {
+      Lr = Le;  // coupled directly to the previous separator (zero for the first node)
+    }
+    if (t + 1 < P) {
+      if (L.m(t + 1) >= 2) {
+        const double* w = red + (size_t)blockDim.x * kCrStride + (size_t)(t + 1) * kRelStride;
+        const M2 uL1 = {w[0], w[1], w[2], w[3]}, uR1 = {w[4], w[5], w[6], w[7]};
+        Dr = m2_add(Dr, m2_mul(Re, uL1));
+        Rr = m2_mul(Re, uR1);
+        m2_mv(Re, w[8], w[9], c0, c1);
+        b0 -= c0;
+        b1 -= c1;
+      } else {
+        Rr = Re;
+      }
+    }
+    double* r = red + (size_t)t * kCrStride;
+    r[0] = Dr.a; r[1] = Dr.d; r[2] = 0.5 * (Dr.b + Dr.c);
+    r[3] = Lr.a; r[4] = Lr.b; r[5] = Lr.c; r[6] = Lr.d;
+    r[7] = Rr.a; r[8] = Rr.b; r[9] = Rr.c; r[10] = Rr.d;
+    r[11] = b0; r[12] = b1;
+  }
+  __syncthreads();
+  cr_solve(red, P);
+  // back substitution of the interior
+  if (own) {
+    const double xl0 = t > 0 ? red[(size_t)(t - 1) * kCrStride + 11] : 0.0;
+    const double xl1 = t > 0 ? red[(size_t)(t - 1) * kCrStride + 12] : 0.0;
+    double x0 = red[(size_t)t * kCrStride + 11], x1 = red[(size_t)t * kCrStride + 12];
+    xo[(size_t)e * xs] = x0;
+    yo[(size_t)e * ys] = x1;
+    for (int k = mt - 2; k >= 0; k--) {
+      const size_t q = L.pos(t, k);
+      const M2 Di = {D0[q], D2[q], D2[q], D1[q]};
+      double c0, c1, s0, s1;
+      m2_mv({S0[q], S1[q], S2[q], S3[q]}, xl0, xl1, s0, s1);
+      m2_mv(ldR(q), x0, x1, c0, c1);  // R_i x_{i+1}
+      m2_mv(Di, B0[q] - s0 - c0, B1[q] - s1 - c1, x0, x1);
+      xo[(size_t)(a + k) * xs] = x0;
+      yo[(size_t)(a + k) * ys] = x1;
+    }
+  }
+  __syncthreads();
+}
+
 // Standalone solve of a block-tridiagonal system given as diag (n x 3: xx yy xy), coupling
 // ((n-1) x 4: [[c0 c2] [c3 c1]] between block i and i+1) and rhs (n x 2) into x (n x 2), with
-// the caller's workspace cr (n x kCrStride doubles). One CTA.
+// the caller's workspace cr (n x kCrStride doubles). One CTA with blockDim.x x kPartSmemStride
+// doubles of dynamic shared memory.
 __global__ void __launch_bounds__(kSolveThreads) k_block_tridiag(int n, const double* __restrict__ diag,
                                                                  const double* __restrict__ coupling,
                                                                  const double* __restrict__ rhs,
                                                                  double* __restrict__ x, double* __restrict__ cr) {
+  const PartLayout L(n, blockDim.x);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double* q = cr + (size_t)i * kCrStride;
-    q[0] = diag[3 * i]; q[1] = diag[3 * i + 1]; q[2] = diag[3 * i + 2];
-    if (i > 0) {  // L_i = R_{i-1}^T
-      const double* c = coupling + 4 * (size_t)(i - 1);
-      q[3] = c[0]; q[4] = c[3]; q[5] = c[2]; q[6] = c[1];
-    } else {
-      q[3] = q[4] = q[5] = q[6] = 0.0;
-    }
-    if (i + 1 < n) {
-      const double* c = coupling + 4 * (size_t)i;
-      q[7] = c[0]; q[8] = c[2]; q[9] = c[3]; q[10] = c[1];
-    } else {
-      q[7] = q[8] = q[9] = q[10] = 0.0;
-    }
-    q[11] = rhs[2 * i];
-    q[12] = rhs[2 * i + 1];
+    const size_t q = L.pos_of(i);
+    cr[(size_t)kPD0 * n + q] = diag[3 * i];
+    cr[(size_t)kPD1 * n + q] = diag[3 * i + 1];
+    cr[(size_t)kPD2 * n + q] = diag[3 * i + 2];
+    const double* c = coupling + 4 * (size_t)i;
+    const bool has = i + 1 < n;
+    cr[(size_t)kPR0 * n + q] = has ? c[0] : 0.0;
+    cr[(size_t)kPR1 * n + q] = has ? c[2] : 0.0;
+    cr[(size_t)kPR2 * n + q] = has ? c[3] : 0.0;
+    cr[(size_t)kPR3 * n + q] = has ? c[1] : 0.0;
+    cr[(size_t)kPB0 * n + q] = rhs[2 * i];
+    cr[(size_t)kPB1 * n + q] = rhs[2 * i + 1];
   }
   __syncthreads();
-  cr_solve(cr, n);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    x[2 * i] = cr[(size_t)i * kCrStride + 11];
-    x[2 * i + 1] = cr[(size_t)i * kCrStride + 12];
-  }
+  extern __shared__ double sh_red[];  // blockDim.x x kPartSmemStride
+  part_solve(cr, n, sh_red, x, 2, x + 1, 2);
 }
 
 // Knot-difference regulariser of frame f (extension; lambda = 0 reproduces the reference): sum of
@@ -153,19 +344,46 @@ __device__ void smear_scan(double* v, int n, double s, double* sh_a, double* sh_
     y = __dadd_rn(__dmul_rn(y, s), __dmul_rn(v[i], om));
     a = a * s;
   }
-  sh_a[t] = a;
-  sh_b[t] = y;
-  __syncthreads();
-  if (t == 0) {
-    double carry = 0.0;
-    for (int k = 0; k < nt; k++) {
-      double nc = sh_a[k] * carry + sh_b[k];
-      sh_b[k] = carry;  // carry-in of chunk k
-      carry = nc;
+  // carry-in of each chunk: exclusive scan of the chunks' affine maps c -> a c + y (composition
+  // (a2, b2) after (a1, b1) = (a2 a1, a2 b1 + b2)), warp scans then a scan of the warp totals
+  const int lane = t & 31, warp = t >> 5, nw = (nt + 31) >> 5;
+  double A = a, B = y;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double pa = __shfl_up_sync(0xffffffffu, A, o), pb = __shfl_up_sync(0xffffffffu, B, o);
+    if (lane >= o) {
+      B = A * pb + B;
+      A = A * pa;
     }
   }
+  if (lane == 31) {
+    sh_a[warp] = A;
+    sh_b[warp] = B;
+  }
   __syncthreads();
-  y = sh_b[t];
+  if (warp == 0) {
+    double wa = lane < nw ? sh_a[lane] : 1.0, wb = lane < nw ? sh_b[lane] : 0.0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double pa = __shfl_up_sync(0xffffffffu, wa, o), pb = __shfl_up_sync(0xffffffffu, wb, o);
+      if (lane >= o) {
+        wb = wa * pb + wb;
+        wa = wa * pa;
+      }
+    }
+    // exclusive: the composition of the preceding warps applied to 0
+    const double ex = __shfl_up_sync(0xffffffffu, wb, 1);
+    __syncwarp();
+    if (lane < nw) sh_b[32 + lane] = lane == 0 ? 0.0 : ex;
+  }
+  __syncthreads();
+  {
+    // this thread's exclusive in-warp map applied to the warp's carry-in
+    const double ea = __shfl_up_sync(0xffffffffu, A, 1), eb = __shfl_up_sync(0xffffffffu, B, 1);
+    const double cw = sh_b[32 + warp];
+    y = lane == 0 ? cw : ea * cw + eb;
+  }
+  __syncthreads();
   for (int i = lo; i < hi; i++) {
     y = __dadd_rn(__dmul_rn(y, s), __dmul_rn(v[i], om));
     v[i] = y;
@@ -221,32 +439,48 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
     if (!frame_active(G, f, shift)) continue;
     G.params_used[c] = (c == 0) ? G.blocks_present[0] : (G.blocks_present[c] | G.blocks_present[c - 1]);
   }
-  for (int f = t; f < nF; f += nt) {
-    bool act = frame_active(G, f, shift);
-    const double* ks = G.p + (size_t)f * W;
-    double* km = G.kmask + (size_t)f * 2 * (W + 1);
-    double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
-    for (int k = 0; k <= W; k++) {
-      km[k] = ks[k];
-      km[W + 1 + k] = ks[N + k];
-      if (act) {
-        kd[k] = ks[k];
-        kd[W + 1 + k] = ks[N + k];
-      }
+  // knot copies: kmask of every frame, kdiff of the active ones (the state the line search starts
+  // from); line-search state
+  const int W1 = W + 1;
+  for (int idx = t; idx < nF * W1; idx += nt) {
+    const int f = idx / W1, k = idx - f * W1;
+    const double x = G.p[(size_t)f * W + k], y = G.p[(size_t)N + (size_t)f * W + k];
+    double* km = G.kmask + (size_t)f * 2 * W1;
+    km[k] = x;
+    km[W1 + k] = y;
+    if (frame_active(G, f, shift)) {
+      double* kd = G.kdiff + (size_t)f * 2 * W1;
+      kd[k] = x;
+      kd[W1 + k] = y;
     }
+  }
+  for (int f = t; f < nF; f += nt) {
+    const bool act = frame_active(G, f, shift);
     G.fstate[f] = act ? 2 : 0;  // searching once the step is known
     G.ls_trials[f] = 0;
-    if (!act) continue;
-    double e = 0;
-    long long n = 0;
-    for (int cc = 0; cc < W; cc++) {
-      e += G.colsum[(size_t)(f * W + cc) * kCsStride + kCsSsd];
-      n += G.colcnt[f * W + cc];
+    if (act) atomicAdd(&sh_nact, 1);
+  }
+  // errval of the active frames (task_calcerrval.cu:185), a warp per frame
+  {
+    const int warp = t >> 5, lane = t & 31, nwarps = nt >> 5;
+    for (int f = warp; f < nF; f += nwarps) {
+      if (!frame_active(G, f, shift)) continue;
+      const double* ks = G.p + (size_t)f * W;
+      double e = 0, rg = 0;
+      int n = 0;
+      for (int cc = lane; cc < W; cc += 32) {
+        e += G.colsum[(size_t)(f * W + cc) * kCsStride + kCsSsd];
+        n += G.colcnt[f * W + cc];
+        if (G.lambda != 0.0) {  // knot-difference regulariser (extension); the right boundary is ks[W]
+          const double dx = ks[cc + 1] - ks[cc], dy = ks[N + cc + 1] - ks[N + cc];
+          rg += dx * dx + dy * dy;
+        }
+      }
+      e = warp_sum(e);
+      n = warp_sum(n);
+      rg = warp_sum(rg);
+      if (lane == 0) G.errval[shift * nF + f] = (G.lambda != 0.0) ? (e + G.lambda * rg) / (double)n : e / (double)n;
     }
-    double val = e / (double)n;
-    if (G.lambda != 0.0) val = (e + G.lambda * frame_reg(ks, W, N, ks[W], ks[N + W])) / (double)n;
-    G.errval[shift * nF + f] = val;
-    atomicAdd(&sh_nact, 1);
   }
   for (int i = t; i < 2 * N; i += nt) G.p_snap[i] = G.p[i];
   __syncthreads();
@@ -263,19 +497,29 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
     const int lo = min(N, t * chunk), hi = min(N, lo + chunk);
     int cnt = 0;
     for (int k = lo; k < hi; k++) cnt += G.params_used[k] ? 1 : 0;
-    sh_i[t] = cnt;
+    // exclusive scan of the chunk counts: warp scans, then a scan of the warp totals
+    const int lane = t & 31, warp = t >> 5;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) sh_i[warp] = incl;
     __syncthreads();
-    if (t == 0) {
-      int run = 0;
-      for (int k = 0; k < nt; k++) {
-        int v = sh_i[k];
-        sh_i[k] = run;
-        run += v;
+    if (warp == 0) {
+      const int nw = nt >> 5;
+      int w = lane < nw ? sh_i[lane] : 0, wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += v;
       }
-      sh_h = run;
+      if (lane < nw) sh_i[32 + lane] = wi - w;
+      if (lane == nw - 1) sh_h = wi;
     }
     __syncthreads();
-    int pos = sh_i[t];
+    int pos = sh_i[32 + warp] + incl - cnt;
     for (int k = lo; k < hi; k++) {
       if (G.params_used[k]) {
         G.list[pos] = k;
@@ -296,73 +540,76 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
     for (int i = t; i < N; i += nt) G.eig_valid[i] = 0;
   __syncthreads();
 
-  // (3) blocks of the compact system; coupling to the next list position
+  // (3) blocks of the compact system, coupling to the next list position, written in the plane
+  // layout of the partitioned solve (each thread its partition's nodes)
   const double lam = G.lambda;
-  for (int i = t; i < h; i += nt) {
-    int k = G.list[i];
-    const double* a = G.colsum + (size_t)k * kCsStride;
-    double* n = G.cr + (size_t)i * kCrStride;
-    double d0 = 0, d1 = 0, d2 = 0, r0 = 0, r1 = 0;
-    if (k < fW) {
-      d0 += a[kCsAxx]; d1 += a[kCsAyy]; d2 += a[kCsAxy];
-      r0 += a[kCsJ1x]; r1 += a[kCsJ1y];
-    }
-    if (k > 0) {
-      const double* b = G.colsum + (size_t)(k - 1) * kCsStride;
-      d0 += b[kCsBxx]; d1 += b[kCsByy]; d2 += b[kCsBxy];
-      r0 += b[kCsJ2x]; r1 += b[kCsJ2y];
-    }
-    M2 R = {0, 0, 0, 0};
-    bool fresh = (i + 1 < h) && (G.list[i + 1] == k + 1);
-    if (fresh) {
-      R = {a[kCsOxx], a[kCsOxy], a[kCsOxy], a[kCsOyy]};
-      if (G.solver_id == 2) {
-        double* e = G.eig_c + (size_t)i * 4;
-        e[0] = R.a; e[1] = R.b; e[2] = R.c; e[3] = R.d;
-        G.eig_valid[i] = 1;
+  if (h > 0 && t < min(nt, h)) {
+    const PartLayout PLy(h, nt);
+    double* const pl = G.cr;
+    const int a0 = PLy.a(t), mt = PLy.m(t);
+    for (int kk = 0; kk < mt; kk++) {
+      const int i = a0 + kk;
+      const size_t q = PLy.pos(t, kk);
+      const int k = G.list[i];
+      double d0 = 0, d1 = 0, d2 = 0, r0 = 0, r1 = 0;
+      double2 o78 = make_double2(0, 0), o9 = make_double2(0, 0);
+      if (k < fW) {
+        const double2* a = reinterpret_cast<const double2*>(G.colsum + (size_t)k * kCsStride);
+        const double2 v01 = a[0], v23 = a[1], v1011 = a[5];
+        o78 = a[3];
+        o9 = a[4];
+        d0 += v01.y; d1 += v23.x; d2 += v23.y;   // kCsAxx kCsAyy kCsAxy
+        r0 += v1011.x; r1 += v1011.y;            // kCsJ1x kCsJ1y
       }
-    } else if (G.solver_id == 2 && i + 1 < h && G.eig_valid[i]) {
-      // SolverEigen keeps its matrix between solves while the used count is unchanged
-      // (eigensolve.cpp:7-31): a coupling that is not written now keeps its last value.
-      const double* e = G.eig_c + (size_t)i * 4;
-      R = {e[0], e[1], e[2], e[3]};
-    }
-    if (lam != 0.0) {
-      int deg = (k > 0) + (k < N - 1);
-      d0 += lam * deg;
-      d1 += lam * deg;
-      const double* p = G.p;
-      r0 -= lam * (deg * p[k] - (k > 0 ? p[k - 1] : 0) - (k < N - 1 ? p[k + 1] : 0));
-      r1 -= lam * (deg * p[N + k] - (k > 0 ? p[N + k - 1] : 0) - (k < N - 1 ? p[N + k + 1] : 0));
+      if (k > 0) {
+        const double2* b = reinterpret_cast<const double2*>(G.colsum + (size_t)(k - 1) * kCsStride);
+        const double2 v45 = b[2], v67 = b[3], v1213 = b[6];
+        d0 += v45.x; d1 += v45.y; d2 += v67.x;   // kCsBxx kCsByy kCsBxy
+        r0 += v1213.x; r1 += v1213.y;            // kCsJ2x kCsJ2y
+      }
+      M2 R = {0, 0, 0, 0};
+      const bool fresh = (i + 1 < h) && (G.list[i + 1] == k + 1);
       if (fresh) {
-        R.a -= lam;
-        R.d -= lam;
+        R = {o78.y, o9.y, o9.y, o9.x};  // (Oxx Oxy; Oxy Oyy)
+        if (G.solver_id == 2) {
+          double* e = G.eig_c + (size_t)i * 4;
+          e[0] = R.a; e[1] = R.b; e[2] = R.c; e[3] = R.d;
+          G.eig_valid[i] = 1;
+        }
+      } else if (G.solver_id == 2 && i + 1 < h && G.eig_valid[i]) {
+        // SolverEigen keeps its matrix between solves while the used count is unchanged
+        // (eigensolve.cpp:7-31): a coupling that is not written now keeps its last value.
+        const double* e = G.eig_c + (size_t)i * 4;
+        R = {e[0], e[1], e[2], e[3]};
       }
-    }
-    n[0] = d0; n[1] = d1; n[2] = d2;
-    n[7] = R.a; n[8] = R.b; n[9] = R.c; n[10] = R.d;
-    n[11] = r0; n[12] = r1;
-  }
-  __syncthreads();
-  for (int i = t; i < h; i += nt) {
-    double* n = G.cr + (size_t)i * kCrStride;
-    if (i > 0) {
-      const double* pr = G.cr + (size_t)(i - 1) * kCrStride;
-      n[3] = pr[7]; n[4] = pr[9]; n[5] = pr[8]; n[6] = pr[10];  // L_i = R_{i-1}^T
-    } else {
-      n[3] = n[4] = n[5] = n[6] = 0;
+      if (lam != 0.0) {
+        const int deg = (k > 0) + (k < N - 1);
+        d0 += lam * deg;
+        d1 += lam * deg;
+        const double* p = G.p;
+        r0 -= lam * (deg * p[k] - (k > 0 ? p[k - 1] : 0) - (k < N - 1 ? p[k + 1] : 0));
+        r1 -= lam * (deg * p[N + k] - (k > 0 ? p[N + k - 1] : 0) - (k < N - 1 ? p[N + k + 1] : 0));
+        if (fresh) {
+          R.a -= lam;
+          R.d -= lam;
+        }
+      }
+      pl[(size_t)kPD0 * h + q] = d0;
+      pl[(size_t)kPD1 * h + q] = d1;
+      pl[(size_t)kPD2 * h + q] = d2;
+      pl[(size_t)kPR0 * h + q] = R.a;
+      pl[(size_t)kPR1 * h + q] = R.b;
+      pl[(size_t)kPR2 * h + q] = R.c;
+      pl[(size_t)kPR3 * h + q] = R.d;
+      pl[(size_t)kPB0 * h + q] = r0;
+      pl[(size_t)kPB1 * h + q] = r1;
     }
   }
   __syncthreads();
 
-  // (4) FP64 block cyclic reduction
-  cr_solve(G.cr, h);
-  // (5) compact step [x_0..x_h-1, y_0..y_h-1]
-  for (int i = t; i < h; i += nt) {
-    G.ndp[i] = G.cr[(size_t)i * kCrStride + 11];
-    G.ndp[h + i] = G.cr[(size_t)i * kCrStride + 12];
-  }
-  __syncthreads();
+  // (4) FP64 partitioned block-tridiagonal solve into the compact step [x_0..x_h-1, y_0..y_h-1]
+  extern __shared__ double sh_red[];  // kSolveThreads x kPartSmemStride
+  part_solve(G.cr, h, sh_red, G.ndp, 1, G.ndp + h, 1);
   // (6) the solver's filter on the x half and the y half (eigensolver.cu:54-55)
   if (C.filter_active) {
     if (C.filter_kind == 1) {

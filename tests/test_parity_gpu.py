@@ -44,6 +44,8 @@ CASES = {
     "big_motion": dict(clip_px=6.0, jumps=2, jump_px=4.0, seed=11),
     "template_larger": dict(template_size=(40, 44), seed=5),
     "uint16_frames": dict(frame_dtype=np.uint16, seed=8),
+    # a knot chain longer than the solve's 1024 partitions: partitions with interior nodes
+    "long_chain": dict(n_frames=72, nknots=17, seed=61),
 }
 
 
