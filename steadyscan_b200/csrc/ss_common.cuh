@@ -55,7 +55,9 @@ struct GroupCtl {
   int phase, iteration, shift, improved, exec_result;
   int filter_active, filter_kind, filter_id, n_filter_iter;
   int stop_reason, cap_hit, eig_size, n_used;
-  int pad0;
+  int ls_state;    // 1 from the half-step solve until the line search is post-processed
+  int ls_pending;  // frames of the half-step whose line search still runs (trial rounds)
+  int pad0, pad1;
   double correlation, corr;
   long long n_eval;      // frame evaluations the reference would count: errval passes and trials
   long long passes[4];   // frames read per evaluation kind (EvalMode)
@@ -91,7 +93,8 @@ struct GroupDesc {
   int* err;                 // device error word of the batch (bit 0: a staging copy timed out)
   int pair_ok;              // precision 'S' pixel pairs: affine geometry, Hb % 64 == 0, aligned frames
   unsigned long long* staging;  // batch counters of shared-memory staging (ss_batch_stats.staging)
-  int* searching;           // batch count of frames whose line search runs (trial rounds)
+  int ls_rounds;            // 1: the line search runs in trial rounds (precision 'S')
+  int* ls_max_trials;       // batch: most trials of a frame whose search ended in the current cycle
   int* ls_done;             // nF: columns of the frame evaluated in the current trial round
   const uint8_t* base_mask;
   const int* min_points;    // W

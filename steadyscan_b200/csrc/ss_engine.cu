@@ -582,7 +582,7 @@ struct Batch::Impl {
   GroupCtl* d_ctl = nullptr;
   int* d_tile_group = nullptr;
   int* d_frame_group = nullptr;
-  int* d_counters = nullptr;  // [0] searching frames, [1] finished groups
+  int* d_counters = nullptr;  // [0] most trials of a search that ended in the cycle, [1] finished groups
   int* d_err = nullptr;       // device error word (bit 0: a shared-memory staging copy timed out)
   unsigned long long* d_staging = nullptr;  // staging counters of the run
   double* d_sum_parts = nullptr;            // partial sums of k_sum_image
@@ -701,7 +701,8 @@ static void layout(Batch::Impl* b, char* base) {
       G.col_yrange = b->compute == 1 ? cv.take<float>(2 * (size_t)g.W) : nullptr;
     }
     G.err = b->d_err;
-    G.searching = b->d_counters;
+    G.ls_rounds = b->compute == 1 ? 1 : 0;
+    G.ls_max_trials = b->d_counters;
     G.staging = b->d_staging;
     g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
     G.image = g.frames_dev ? g.frames_dev : g.d_image;
@@ -959,33 +960,33 @@ constexpr size_t kSolveSmem = (size_t)kSolveThreads * kPartSmemStride * sizeof(d
 // Opts k_block_tridiag into kSolveSmem of dynamic shared memory.
 static cudaError_t block_tridiag_attr() { return smem_attr(k_block_tridiag, (int)kSolveSmem); }
 
+// Trial rounds per cycle of the precision 'S' line search: the first cycle's, and the range of the
+// later ones (set from the longest search that ended in the cycle before).
+constexpr int kFirstRounds = 8, kMinRounds = 3, kMaxRounds = 16;
+
 static int run_cycles(Batch::Impl* b) {
   cudaStream_t s = b->stream;
   SS_CK(smem_attr(k_solve, (int)kSolveSmem));
   const int nG = (int)b->gd.size();
   int max_iter = 1;
   for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
-  const int max_cycles = 4 * (max_iter + 2) + 16;
-  for (int cycle = 0; cycle < max_cycles; cycle++) {
+  // two half-steps per iteration, a line search of up to kTrialCap trials each
+  const long long max_cycles = 4LL * (max_iter + 2) * (1 + kTrialCap / kMinRounds) + 16;
+  int rounds = kFirstRounds;
+  for (long long cycle = 0; cycle < max_cycles; cycle++) {
     b->cycles++;
     b->eval_timed(kAssemble);
     k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
     b->launches++;
     SS_CK(cudaGetLastError());
     if (b->ks.round) {
-      // trial rounds until no frame searches: a first block of rounds, then the searching count
-      int block = 6;
-      for (int guard = 0;; guard++) {
-        for (int r = 0; r < block; r++) {
-          b->rounds++;
-          b->eval_timed(kTrial);
-        }
-        SS_CK(cudaGetLastError());
-        SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, sizeof(int), cudaMemcpyDeviceToHost, s));
-        SS_CK(cudaStreamSynchronize(s));
-        if (b->h_counters[0] <= 0) break;
-        if (guard > kTrialCap) return fail(SS_ERR_CUDA, "line search did not finish within the trial bound");
-        block = 4;
+      // trial rounds without a host round trip: as many as the longest search of the previous
+      // cycle took; a search that needs more continues in the next cycle (its group skips
+      // assembly and solve until it has finished)
+      SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
+      for (int r = 0; r < rounds; r++) {
+        b->rounds++;
+        b->eval_timed(kTrial);
       }
       b->eval_timed(kCorr);  // correlation sums after the second half-step
     } else {
@@ -999,9 +1000,10 @@ static int run_cycles(Batch::Impl* b) {
     k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
     b->launches += 3;
     SS_CK(cudaGetLastError());
-    SS_CK(cudaMemcpyAsync(b->h_counters + 1, b->d_counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     SS_CK(cudaStreamSynchronize(s));
     if (b->h_counters[1] >= nG) return SS_OK;
+    if (b->h_counters[0] > 0) rounds = std::min(kMaxRounds, std::max(kMinRounds, b->h_counters[0]));
   }
   return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
 }

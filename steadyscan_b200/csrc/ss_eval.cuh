@@ -433,7 +433,9 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
   const GroupDesc& G = gds[g];
   const GroupCtl& C = ctl[g];
   if (C.phase != (MODE == kFinal ? kPhFinal : kPhHalf)) return;
-  if (MODE == kCorr && C.shift != 1) return;  // correlation sums after the second half-step
+  if (MODE == kAssemble && C.ls_state != 0) return;  // the group's line search still runs
+  // correlation sums once the line search of the second half-step has finished
+  if (MODE == kCorr && (C.shift != 1 || C.ls_state != 1 || C.ls_pending != 0)) return;
   const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
   const int nfb = (G.nF + fpc - 1) / fpc;
   const int local = blockIdx.x - G.tile_base;
@@ -574,7 +576,7 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
   const int g = frame_group[gf];
   const GroupDesc& G = gds[g];
   GroupCtl& C = ctl[g];
-  if (C.phase != kPhHalf) return;  // uniform over the cluster
+  if (C.phase != kPhHalf || C.ls_state != 1) return;  // uniform over the cluster
   const int f = gf - G.frame_base;
   const int W = G.W, N = G.N, Hb = G.Hb, b0 = f * W;
   const int shift = C.shift;
@@ -940,7 +942,8 @@ __device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f
     G.ls_done[f] = 0;
     if ((action & 15) != 1) {
       G.fstate[f] = 0;
-      atomicSub(G.searching, 1);
+      atomicSub(&C.ls_pending, 1);
+      atomicMax(G.ls_max_trials, G.ls_trials[f]);
     }
   }
 }
@@ -955,7 +958,9 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
   const int g = tile_group[blockIdx.x];
   const GroupDesc& G = gds[g];
   GroupCtl& C = ctl[g];
-  if (C.phase != kPhHalf) return;
+  // ls_pending falls while the round runs: one decision for the whole CTA (0 means every frame of
+  // the group has finished)
+  if (!__syncthreads_and(C.phase == kPhHalf && C.ls_state == 1 && *(volatile int*)&C.ls_pending > 0)) return;
   const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
   const int nfb = (G.nF + fpc - 1) / fpc;
   const int local = blockIdx.x - G.tile_base;

@@ -414,7 +414,7 @@ __device__ void range_seq(double* v, int n, double strength) {
 __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __restrict__ gds, GroupCtl* __restrict__ ctl) {
   const GroupDesc& G = gds[blockIdx.x];
   GroupCtl& C = ctl[blockIdx.x];
-  if (C.phase != kPhHalf) return;
+  if (C.phase != kPhHalf || C.ls_state != 0) return;  // a line search of the group still runs
   const int t = threadIdx.x, nt = blockDim.x;
   const int W = G.W, N = G.N, nF = G.nF, fW = G.fW, shift = C.shift;
   __shared__ double sh_a[kSolveThreads], sh_b[kSolveThreads];
@@ -487,7 +487,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
   if (t == 0) {
     C.n_eval += sh_nact;
     C.passes[kAssemble] += nF;
-    atomicAdd(G.searching, sh_nact);  // frames whose line search starts (trial rounds)
+    C.ls_state = 1;
+    C.ls_pending = G.ls_rounds ? sh_nact : 0;  // frames whose line search starts (trial rounds)
   }
 
   // (2) compaction: list position of every used knot (paramsUsed[N-1] is never written, so it
@@ -651,7 +652,8 @@ __global__ void k_after_ls(const GroupDesc* __restrict__ gds, GroupCtl* __restri
   if (g >= n_groups) return;
   const GroupDesc& G = gds[g];
   GroupCtl& C = ctl[g];
-  if (C.phase != kPhHalf) return;
+  if (C.phase != kPhHalf || C.ls_state != 1 || C.ls_pending != 0) return;
+  C.ls_state = 0;
   double e0 = 0, e1 = 0;
   for (int i = 0; i < G.nF; i++) {
     e0 += G.errval[i];

@@ -172,3 +172,22 @@ def test_batched_equals_single():
         np.testing.assert_array_equal(single["dy"], b["dy"])
         np.testing.assert_array_equal(single["mask"], b["mask"])
         np.testing.assert_array_equal(single["residrms"], b["residrms"])
+
+
+def test_persistent_grid_many_tiles_precision_s():
+    """A batch with more tiles (block column x frame chunk) than the persistent grid has CTAs, so
+    every CTA takes several tiles, and searches spread over several cycles: each group still gets
+    its single-call result."""
+    groups = []
+    for i in range(12):
+        a, _, _ = make_args(nlines=64, linewidth=64, nknots=33, n_frames=40, seed=70 + i, n_blobs=30,
+                            frame_dtype=np.uint16)
+        a["flags"] = "S"
+        groups.append(a)
+    batched = api.align_groups(groups)
+    for a, b in zip(groups, batched):
+        single = api.align_group(a)
+        assert single["iter_used"] == b["iter_used"]
+        np.testing.assert_array_equal(single["dx"], b["dx"])
+        np.testing.assert_array_equal(single["dy"], b["dy"])
+        np.testing.assert_array_equal(single["mask"], b["mask"])
