@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--cpu-sample-frames", type=int, default=16)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the unbatched per-group comparison")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the storage-precision sweep")
+    ap.add_argument("--plain-groups", type=int, default=2)
     return ap.parse_args()
 
 
@@ -153,7 +156,7 @@ def peaks():
 
 
 def traffic_summary():
-    p = os.path.join(ROOT, "profiles", "k_eval_traffic.json")
+    p = os.path.join(ROOT, "profiles", "k_trial_round_traffic.json")
     if os.path.exists(p):
         return json.load(open(p))
     return None
@@ -186,6 +189,63 @@ def cpu_sample(groups, n_frames, threads):
     o = oracle.align_group(a, n_threads=threads, want_mask=False)
     dt = time.perf_counter() - t0
     return n_frames / dt, dt, o, a
+
+
+def plain_path(groups, precision, n_groups):
+    """The unbatched per-group path: one synchronous align_group_to_template call per group from host
+    memory, one group after another, as the reference's caller drives it (frames/s)."""
+    from steadyscan_b200 import api
+    gs = []
+    for g in groups[:max(1, n_groups)]:
+        d = dict(g)
+        d["flags"] = precision
+        gs.append(d)
+    api.align_group(gs[0], want_mask=False)  # warm-up
+    t0 = time.perf_counter()
+    frames = 0
+    for d in gs:
+        api.align_group(d, want_mask=False)
+        frames += int(d["nFrames"])
+    return frames / (time.perf_counter() - t0), frames
+
+
+def precision_sweep(a, o, template_shape):
+    """Storage choices of precision S on the oracle's sample: frames uint16 / FP16 x template and
+    gradients FP32 / FP16, each against the FP64 oracle: RMS and max knot error (px) and the relative
+    L2 of the corrected frames."""
+    from steadyscan_b200 import api, correct
+    n = int(a["nFrames"])
+    geo = (a["tfrac"], a["basex"], a["basey"], a["base_mask"])
+    ref_c, ref_w = correct.correct_frames(a["bmData"], o["dx"], o["dy"], *geo, n, template_shape)
+    counts = np.rint(np.asarray(a["bmData"])).astype(np.uint16)
+    out = []
+    for fname, fr in (("uint16", counts), ("float16", counts.astype(np.float16))):
+        for tname in ("f32", "f16"):
+            b = dict(a)
+            b["bmData"] = np.asfortranarray(fr)
+            b["flags"] = "S"
+            g = api.align_group(b, want_mask=False, template_storage=tname)
+            d = np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]])
+            c, w = correct.correct_frames(a["bmData"], g["dx"], g["dy"], *geo, n, template_shape)
+            out.append({"frames": fname, "template": tname, "rms_px": float(np.sqrt(np.mean(d * d))),
+                        "max_px": float(np.max(np.abs(d))),
+                        "corrected_rel_l2": correct.relative_l2(c, w, ref_c, ref_w)})
+    # control: the FP64 path on the template rounded to FP16 separates the storage path's error
+    # from the quantisation of the template itself
+    from steadyscan_b200 import prep
+    t16 = np.asarray(a["template_image"]).astype(np.float16).astype(np.float64)
+    b = dict(a)
+    b["bmData"] = np.asfortranarray(counts)
+    b["flags"] = "D"
+    b["template_image"] = t16
+    b["xgrad"], b["ygrad"] = prep.template_gradients(t16)
+    g = api.align_group(b, want_mask=False)
+    d = np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]])
+    c, w = correct.correct_frames(a["bmData"], g["dx"], g["dy"], *geo, n, template_shape)
+    out.append({"frames": "uint16", "template": "f16-rounded, FP64 path (control)",
+                "rms_px": float(np.sqrt(np.mean(d * d))), "max_px": float(np.max(np.abs(d))),
+                "corrected_rel_l2": correct.relative_l2(c, w, ref_c, ref_w)})
+    return {"sample": f"{n} frames of one 512x512 group vs the FP64 oracle", "variants": out}
 
 
 def main():
@@ -271,19 +331,27 @@ def main():
     results = batch.collect()
     frame_bytes = lay.frame_h * lay.frame_w * 2
     passes = rs["frame_passes"]
-    eval_ms = sum(rs["eval_ms"])
-    launches_eval = None
-    algo_bytes = sum(passes) * frame_bytes
-    achieved = algo_bytes / (eval_ms / 1000.0) / 1e9 if eval_ms > 0 else None
+    ems = rs["eval_ms"]
     peak, peak_kind = peaks()
     tr = traffic_summary()
-    roofline = {"kernel": "k_eval (assembly, trial, correlation, final passes)", "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s",
+    # the dominant kernel: the line-search trial rounds; one frame-trial reads one frame
+    n_launch = max(1, rs["linesearch_rounds"])
+    units = passes[1] / n_launch
+    launch_ms = ems[1] / n_launch
+    achieved = units * frame_bytes / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+    by_pass = {}
+    for i, name in enumerate(("assembly", "trial", "correlation", "final")):
+        gbs = passes[i] * frame_bytes / (ems[i] / 1e3) / 1e9 if ems[i] > 0 else None
+        by_pass[name] = {"frame_passes": passes[i], "ms": ems[i], "achieved_gbs": gbs,
+                         "frac": gbs / peak if gbs else None}
+    roofline = {"kernel": "k_trial_round (line-search trial rounds, the largest share of device time)",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": tr.get("bytes_per_frame_pass") if tr else None,
-                "algorithmic_bytes_per_frame_pass": frame_bytes,
-                "frame_passes": passes, "eval_ms_by_pass": rs["eval_ms"], "eval_share_of_step":
-                    eval_ms / rs["run_ms"] if rs["run_ms"] else None, "staging": rs["staging"]}
+                "traffic": tr["bytes_per_frame_pass"] * units if tr else None,
+                "algorithmic_bytes_per_launch": units * frame_bytes, "launch_ms": launch_ms,
+                "launches": n_launch, "by_pass": by_pass,
+                "eval_share_of_step": sum(ems) / rs["run_ms"] if rs["run_ms"] else None,
+                "staging": rs["staging"]}
 
     # end to end through the public C ABI from pinned host memory
     e2e = None
@@ -332,6 +400,20 @@ def main():
         rms = float(np.sqrt(np.mean(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]) ** 2)))
         mx = float(np.max(np.abs(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]))))
         acc = {"rms_px_vs_fp64": rms, "max_px_vs_fp64": mx, "sample": f"{args.cpu_sample_frames} frames"}
+        if not args.no_sweep:
+            acc["precision_sweep"] = precision_sweep(a, o, np.asarray(a["template_image"]).shape)
+
+    plain = None
+    if rank == 0 and not args.no_plain:
+        plain = {}
+        for prec in ("D", "S"):
+            v, nfr = plain_path(groups, prec, args.plain_groups)
+            plain[prec] = {"value": v, "unit": "frames/s", "frames": nfr}
+        plain["path"] = ("unbatched: one synchronous ss_align_group_to_template call per group of "
+                         f"{args.group} frames from host memory, serially")
+        plain["batched_vs_plain_D"] = value / plain["D"]["value"]
+        if e2e:
+            plain["e2e_vs_plain_D"] = e2e["value"] / plain["D"]["value"]
 
     if rank == 0:
         iters = [r["iter_used"] for r in results]
@@ -339,7 +421,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32" if args.precision == "S" else "f64", "data": "synthetic",
                 "config": workload_config(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc,
+                "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc, "plain_gpu": plain,
                 "run": {"cycles": st["cycles"], "linesearch_rounds": st["linesearch_rounds"],
                         "iterations_min": int(min(iters)), "iterations_max": int(max(iters)),
                         "arena_bytes": st["arena_bytes"]}}

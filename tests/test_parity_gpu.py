@@ -191,3 +191,20 @@ def test_persistent_grid_many_tiles_precision_s():
         np.testing.assert_array_equal(single["dx"], b["dx"])
         np.testing.assert_array_equal(single["dy"], b["dy"])
         np.testing.assert_array_equal(single["mask"], b["mask"])
+
+
+def test_fp16_template_storage_matches_fp64_on_the_rounded_template():
+    """Template and gradients stored in FP16 (precision S): the error against FP64 comes from rounding
+    the template itself, so the storage path agrees with the FP64 path run on the FP16-rounded
+    template within the precision-S bound."""
+    from steadyscan_b200 import prep
+    args, _, _ = make_args(frame_dtype=np.uint16, seed=14)
+    t16 = np.asarray(args["template_image"]).astype(np.float16).astype(np.float64)
+    d = dict(args)
+    d["template_image"] = t16
+    d["xgrad"], d["ygrad"] = prep.template_gradients(t16)
+    ref = api.align_group(d)
+    s = dict(args)
+    s["flags"] = "S"
+    g = api.align_group(s, template_storage="f16")
+    assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([ref["dx"], ref["dy"]])) <= KNOT_RMS_S
