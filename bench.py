@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the unbatched per-group comparison")
     ap.add_argument("--no-sweep", action="store_true", help="skip the storage-precision sweep")
     ap.add_argument("--plain-groups", type=int, default=2)
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="seconds of generated serving load (8 sessions, 0 to skip)")
     return ap.parse_args()
 
 
@@ -248,6 +250,58 @@ def precision_sweep(a, o, template_shape):
     return {"sample": f"{n} frames of one 512x512 group vs the FP64 oracle", "variants": out}
 
 
+def serve(args, device, seconds, plain_d):
+    """Serving load: 8 sessions, each with its own 512x512 template; groups of 1-64 frames arrive
+    per session as a Poisson process at 30 Hz, doubled for 2 s of every 10 s. Frames come from a
+    per-session pool rendered on the GPU; each session's later groups start from its last knots."""
+    import torch
+    from steadyscan_b200 import api, serving
+    from steadyscan_b200._lib import SS_U16
+    n_ses, pool_frames = 8, 512
+    server = serving.Server(memory_budget=24 << 30, device=device.index or 0, max_active=96)
+    pools = []
+    for s in range(n_ses):
+        groups, dev, _, lay = make_workload(pool_frames, 512, pool_frames, "S", 1005 + 31 * s, device)
+        server.add_session(groups[0])
+        pools.append((dev[0], lay))
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(1005)
+    sched = serving.arrival_schedule(n_ses, seconds, 30.0, 10.0, 2.0, 2.0, (1, 64), rng)
+    cursor = [0] * n_ses
+    t0 = time.perf_counter()
+    k = 0
+    while k < len(sched) or server.by_slot or server.pending:
+        now = time.perf_counter() - t0
+        while k < len(sched) and sched[k][0] <= now:
+            t, s, n = sched[k]
+            flat, lay = pools[s]
+            if cursor[s] + n > pool_frames:
+                cursor[s] = 0
+            f0 = cursor[s]
+            cursor[s] += n
+            px = lay.frame_h * lay.frame_w
+            view = flat[f0 * px:(f0 + n) * px]
+            m = api.DeviceMatrix(view.data_ptr(), lay.frame_h, lay.frame_w * n, SS_U16, owner=view)
+            server.submit(s, m, n, t_arrival=t0 + t)
+            k += 1
+        server.tick()
+    elapsed = time.perf_counter() - t0
+    st = serving.latency_stats(server.done)
+    offered = sum(n for _, _, n in sched) / seconds
+    iters = [r.result["iter_used"] for r in server.done]
+    out = {"sessions": n_ses, "seconds": seconds, "offered_frames_per_s": offered,
+           "frames_per_s": st["frames"] / elapsed, "groups": st["groups"], "p50_ms": st["p50_ms"],
+           "p99_ms": st["p99_ms"], "max_ms": st["max_ms"], "peak_in_flight": server.peak_active,
+           "peak_device_bytes": server.peak_bytes, "server_cycles": server.cycles,
+           "ms_per_cycle": 1000.0 * elapsed / max(1, server.cycles),
+           "iterations_mean": float(np.mean(iters)) if iters else None,
+           "plain_serial_frames_per_s": plain_d,
+           "load": "Poisson 30 Hz per session, 2x for 2 s of every 10 s, groups U[1,64] frames of 512x512 uint16, "
+                   "precision S, warm starts"}
+    server.close()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -415,6 +469,11 @@ def main():
         if e2e:
             plain["e2e_vs_plain_D"] = e2e["value"] / plain["D"]["value"]
 
+    serving_line = None
+    if rank == 0 and args.serve_seconds > 0:
+        batch.close()
+        serving_line = serve(args, device, args.serve_seconds, plain["D"]["value"] if plain else None)
+
     if rank == 0:
         iters = [r["iter_used"] for r in results]
         line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -422,6 +481,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32" if args.precision == "S" else "f64", "data": "synthetic",
                 "config": workload_config(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc, "plain_gpu": plain,
+                "serving": serving_line,
                 "run": {"cycles": st["cycles"], "linesearch_rounds": st["linesearch_rounds"],
                         "iterations_min": int(min(iters)), "iterations_max": int(max(iters)),
                         "arena_bytes": st["arena_bytes"]}}

@@ -158,6 +158,52 @@ SS_API int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats);
 SS_API void* ss_batch_stream(const ss_batch* batch);
 SS_API void ss_batch_destroy(ss_batch* batch);
 
+/* Serving support (no counterpart in the reference, which aligns one group per MEX call).
+ *
+ * A session keeps one imaging session's template, gradients and scan geometry (the ss_inputs
+ * fields 1-7 and 13 of `proto`, with its precision and template_storage) resident on the device,
+ * converted once. Groups of a batch made with ss_batch_create_ex, or admitted to a server, may name
+ * a session; they then use its buffers and their own fields 1-7 and 13 only give the shapes, which
+ * must match. A session must outlive every batch or server group that uses it. */
+typedef struct ss_session ss_session;
+SS_API int ss_session_create(const ss_inputs* proto, ss_session** session);
+SS_API void ss_session_destroy(ss_session* session);
+
+/* Device bytes the batch of these groups needs (no device work, nothing allocated). */
+SS_API int ss_batch_measure(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_session* const* sessions,
+                            int64_t* arena_bytes);
+/* ss_batch_create with per-group sessions (array of n_groups entries, NULL entries or a NULL array
+ * for none) and, when arena is not NULL, the caller's device memory of arena_bytes (at least what
+ * ss_batch_measure returned) instead of an allocation of its own. */
+SS_API int ss_batch_create_ex(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_session* const* sessions,
+                              void* arena, int64_t arena_bytes, ss_batch** batch);
+/* ss_batch_run one cycle at a time without blocking: ss_batch_start resets every group to its
+ * initial knots (asynchronous); ss_batch_step launches one cycle of every group (assembly, solve,
+ * line search, iteration control); ss_batch_poll returns 0 while that cycle runs, 1 when it has
+ * finished and the next ss_batch_step is due, 2 when every group has stopped (then
+ * ss_batch_collect), or an error. */
+SS_API int ss_batch_start(ss_batch* batch);
+SS_API int ss_batch_step(ss_batch* batch);
+SS_API int ss_batch_poll(ss_batch* batch);
+
+/* Continuous batching: a server holds `capacity` group slots on one stream and serves every
+ * active group with one launch sequence per cycle. ss_server_admit prepares a group in a free slot
+ * (its buffers in the caller's arena of arena_bytes from ss_batch_measure, or an allocation of its
+ * own when arena is NULL; its template and geometry from `session` when not NULL; outputs to `out`
+ * when it stops) and returns the slot; it joins at the next ss_server_step, which launches one
+ * cycle of every active group. ss_server_poll returns 0 while that cycle runs; else it collects the
+ * outputs of the groups that stopped, lists their slots in done_slots (up to max_done; call again
+ * for more) and returns 1: those slots and their arenas are free. Groups may be admitted while a
+ * cycle runs. Every group's results are those it gets alone. */
+typedef struct ss_server ss_server;
+SS_API int ss_server_create(int32_t capacity, int32_t device, ss_server** server);
+SS_API int ss_server_admit(ss_server* server, const ss_inputs* in, ss_outputs* out, ss_session* session, void* arena,
+                           int64_t arena_bytes, int32_t* slot);
+SS_API int ss_server_step(ss_server* server);
+SS_API int ss_server_poll(ss_server* server, int32_t* done_slots, int32_t max_done, int32_t* n_done);
+SS_API int32_t ss_server_active(const ss_server* server);
+SS_API void ss_server_destroy(ss_server* server);
+
 /* The FP64 knot-chain solve of one half-step on its own: the symmetric positive definite
  * block-tridiagonal normal equations (2x2 blocks, one per used knot) that the reference assembles
  * in task_filldiagonals.cu:47-159 and task_filljtr.cu:3-58 and hands to its sparse solvers

@@ -86,6 +86,32 @@ def load(build_if_missing: bool = True):
     lib.ss_batch_stream.restype = C.c_void_p
     lib.ss_batch_destroy.argtypes = [C.c_void_p]
     lib.ss_batch_destroy.restype = None
+    lib.ss_session_create.argtypes = [C.POINTER(SSInputs), C.POINTER(C.c_void_p)]
+    lib.ss_session_create.restype = C.c_int
+    lib.ss_session_destroy.argtypes = [C.c_void_p]
+    lib.ss_session_destroy.restype = None
+    lib.ss_batch_measure.argtypes = [C.c_int32, C.POINTER(SSInputs), C.POINTER(SSOutputs), C.c_void_p,
+                                     C.POINTER(C.c_int64)]
+    lib.ss_batch_measure.restype = C.c_int
+    lib.ss_batch_create_ex.argtypes = [C.c_int32, C.POINTER(SSInputs), C.POINTER(SSOutputs), C.c_void_p,
+                                       C.c_void_p, C.c_int64, C.POINTER(C.c_void_p)]
+    lib.ss_batch_create_ex.restype = C.c_int
+    for name in ("ss_batch_start", "ss_batch_step", "ss_batch_poll"):
+        getattr(lib, name).argtypes = [C.c_void_p]
+        getattr(lib, name).restype = C.c_int
+    lib.ss_server_create.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    lib.ss_server_create.restype = C.c_int
+    lib.ss_server_admit.argtypes = [C.c_void_p, C.POINTER(SSInputs), C.POINTER(SSOutputs), C.c_void_p, C.c_void_p,
+                                    C.c_int64, C.POINTER(C.c_int32)]
+    lib.ss_server_admit.restype = C.c_int
+    lib.ss_server_step.argtypes = [C.c_void_p]
+    lib.ss_server_step.restype = C.c_int
+    lib.ss_server_poll.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32)]
+    lib.ss_server_poll.restype = C.c_int
+    lib.ss_server_active.argtypes = [C.c_void_p]
+    lib.ss_server_active.restype = C.c_int32
+    lib.ss_server_destroy.argtypes = [C.c_void_p]
+    lib.ss_server_destroy.restype = None
     lib.ss_solve_block_tridiagonal.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                C.c_void_p]
     lib.ss_solve_block_tridiagonal.restype = C.c_int

@@ -143,6 +143,23 @@ def _result(o: SSOutputs, a: dict, dims) -> dict:
     return r
 
 
+def _batch_args(groups, want_mask, want_history, template_storage, memo: dict | None = None):
+    n = len(groups)
+    ins = (SSInputs * n)()
+    outs = (SSOutputs * n)()
+    keep, arrays, dims = [], [], []
+    memo = {} if memo is None else memo
+    for k, g in enumerate(groups):
+        i, kk = _inputs(g, template_storage, memo)
+        ins[k] = i
+        keep.append(kk)
+        o, a, d = _outputs(g, want_mask, want_history)
+        outs[k] = o
+        arrays.append(a)
+        dims.append(d)
+    return ins, outs, keep, arrays, dims
+
+
 def align_groups(groups: list, want_mask: bool = True, want_history: bool = False, template_storage=None) -> list:
     """Runs many groups (argument dicts) in one batched run on one GPU; returns a list of dicts."""
     lib = load()
@@ -222,31 +239,92 @@ def solve_block_tridiagonal_noalloc(diag, coupling, rhs, stream: int = 0):
     return x
 
 
-class Batch:
-    """A prepared batch of groups (ss_batch_*): inputs resident on the device, runnable repeatedly."""
+class Session:
+    """One imaging session's template, gradients and scan geometry resident on the device
+    (ss_session_*): ``proto`` is an argument dict whose fields 1-7 and 13, precision and device are
+    used (frames and knots are ignored)."""
 
-    def __init__(self, groups: list, want_mask: bool = False, want_history: bool = False, template_storage=None):
+    def __init__(self, proto: dict, template_storage=None):
+        self._lib = load()
+        i, keep = _inputs(proto, template_storage)
+        self._keep = keep
+        self.template_storage = template_storage
+        h = C.c_void_p()
+        check(self._lib.ss_session_create(C.byref(i), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ss_session_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _session_array(sessions, n):
+    if not sessions:
+        return None
+    arr = (C.c_void_p * n)()
+    for k, s in enumerate(sessions):
+        arr[k] = s.handle if s is not None else None
+    return arr
+
+
+class Batch:
+    """A prepared batch of groups (ss_batch_*): inputs resident on the device, runnable repeatedly.
+    ``sessions`` (one entry per group, or None) use resident session buffers; ``arena`` (device
+    pointer, bytes) places the batch in the caller's device memory."""
+
+    def __init__(self, groups: list, want_mask: bool = False, want_history: bool = False, template_storage=None,
+                 sessions=None, arena=None):
         from ._lib import SSBatchStats  # noqa: F401
         self._lib = load()
         n = len(groups)
-        self._ins = (SSInputs * n)()
-        self._outs = (SSOutputs * n)()
-        self._keep, self._arrays, self._dims = [], [], []
-        memo: dict = {}
-        for k, g in enumerate(groups):
-            i, kk = _inputs(g, template_storage, memo)
-            self._ins[k] = i
-            self._keep.append(kk)
-            o, a, d = _outputs(g, want_mask, want_history)
-            self._outs[k] = o
-            self._arrays.append(a)
-            self._dims.append(d)
+        self._ins, self._outs, self._keep, self._arrays, self._dims = _batch_args(groups, want_mask, want_history,
+                                                                                 template_storage)
+        self._ses = _session_array(sessions, n)
         h = C.c_void_p()
-        check(self._lib.ss_batch_create(n, self._ins, self._outs, C.byref(h)))
+        if sessions is None and arena is None:
+            check(self._lib.ss_batch_create(n, self._ins, self._outs, C.byref(h)))
+        else:
+            ptr, nbytes = arena if arena is not None else (None, 0)
+            check(self._lib.ss_batch_create_ex(n, self._ins, self._outs, self._ses, ptr, nbytes, C.byref(h)))
         self._h = h
+
+    @staticmethod
+    def measure(groups: list, want_mask: bool = False, want_history: bool = False, template_storage=None,
+                sessions=None, memo: dict | None = None) -> int:
+        """Device bytes a Batch of these groups needs (nothing allocated). ``memo`` reuses matrices
+        converted by earlier calls for the same argument objects (kept alive by the caller)."""
+        lib = load()
+        ins, outs, keep, arrays, dims = _batch_args(groups, want_mask, want_history, template_storage, memo)
+        nb = C.c_int64()
+        check(lib.ss_batch_measure(len(groups), ins, outs, _session_array(sessions, len(groups)), C.byref(nb)))
+        return int(nb.value)
 
     def run(self):
         check(self._lib.ss_batch_run(self._h))
+
+    def start(self):
+        check(self._lib.ss_batch_start(self._h))
+
+    def step(self):
+        check(self._lib.ss_batch_step(self._h))
+
+    def poll(self) -> int:
+        """0 while the launched cycle runs, 1 when the next step is due, 2 when every group stopped."""
+        rc = self._lib.ss_batch_poll(self._h)
+        if rc < 0:
+            check(rc)
+        return rc
 
     def collect(self) -> list:
         check(self._lib.ss_batch_collect(self._h))

@@ -344,6 +344,9 @@ static int parse_flags(const char* flags, int& compute, int& bits) {
 // ---------------------------------------------------------------------------------------------
 // Batch
 
+// Source index of template and geometry buffers that a resident session holds.
+constexpr int kFromSession = -2;
+
 struct HostGroup {
   const ss_inputs* in = nullptr;
   int compute = 0, flags = 0;
@@ -354,7 +357,10 @@ struct HostGroup {
   std::vector<float> frac_f, bx_f, by_f;  // precision 'S' geometry
   std::vector<float> yrange;              // per block column [min, max] of basey over valid rows
   int frames_per_cta = 32;
-  int tpl_src = -1, geo_src = -1;         // earlier group whose template / geometry buffers are shared
+  int tpl_src = -1, geo_src = -1;         // earlier group whose template / geometry buffers are shared,
+                                          // or kFromSession
+  const GroupDesc* ses_gd = nullptr;      // resident session buffers (kFromSession)
+  const HostGroup* ses_hg = nullptr;
   int geo_k = 0, geo_L = 0;               // affine geometry (0: tables)
   double geo_ax = 0, geo_bx = 0, geo_ay = 0, geo_by = 0, geo_fs = 0;
   std::vector<uint8_t> bmask;
@@ -393,6 +399,10 @@ static int validate_group(const ss_inputs* in, HostGroup& g) {
   g.nF = in->n_frames;
   if (g.nF < 1) return fail(SS_ERR_INVALID_ARGUMENT, "n_frames must be positive");
   g.fW = g.W * g.nF;
+  {  // frame chunks of the evaluation tiles: at most 32 frames, as even as the group allows
+    const int chunks = (g.nF + 31) / 32;
+    g.frames_per_cta = (g.nF + chunks - 1) / chunks;
+  }
   g.N = g.fW + 1;
   if ((long long)g.Hb * g.fW > (1LL << 31) - 1) return fail(SS_ERR_INVALID_ARGUMENT, "too many pixels in one group");
   if (in->bm_data.rows != g.Hb || in->bm_data.cols != g.fW)
@@ -434,10 +444,10 @@ static void find_shared_inputs(std::vector<HostGroup>& hg) {
     const ss_inputs* a = hg[i].in;
     for (size_t j = 0; j < i; j++) {
       const ss_inputs* b = hg[j].in;
-      if (hg[i].tpl_src < 0 && hg[j].tpl_src < 0 && same_matrix(a->template_image, b->template_image) &&
+      if (hg[i].tpl_src == -1 && hg[j].tpl_src == -1 && same_matrix(a->template_image, b->template_image) &&
           same_matrix(a->xgrad, b->xgrad) && same_matrix(a->ygrad, b->ygrad))
         hg[i].tpl_src = (int)j;
-      if (hg[i].geo_src < 0 && hg[j].geo_src < 0 && same_matrix(a->tfrac, b->tfrac) &&
+      if (hg[i].geo_src == -1 && hg[j].geo_src == -1 && same_matrix(a->tfrac, b->tfrac) &&
           same_matrix(a->basex, b->basex) && same_matrix(a->basey, b->basey) &&
           same_matrix(a->base_mask, b->base_mask) && same_matrix(a->min_points_per_block, b->min_points_per_block))
         hg[i].geo_src = (int)j;
@@ -449,13 +459,13 @@ static int load_host_inputs(std::vector<HostGroup>& all, size_t gi) {
   HostGroup& g = all[gi];
   const ss_inputs* in = g.in;
   int rc;
-  if (g.tpl_src < 0) {
+  if (g.tpl_src == -1) {
     if ((rc = host_doubles(in->template_image, "template_image", g.templ))) return rc;
     if ((rc = host_doubles(in->xgrad, "xgrad", g.xg))) return rc;
     if ((rc = host_doubles(in->ygrad, "ygrad", g.yg))) return rc;
   }
   std::vector<double> tmp;
-  if (g.geo_src < 0) {
+  if (g.geo_src == -1) {
     if ((rc = host_doubles(in->tfrac, "tfrac", g.frac))) return rc;
     if ((rc = host_doubles(in->basex, "basex", g.bx))) return rc;
     if ((rc = host_doubles(in->basey, "basey", g.by))) return rc;
@@ -485,7 +495,7 @@ static int load_host_inputs(std::vector<HostGroup>& all, size_t gi) {
       g.p0[j + g.N] = ey[(size_t)f * (g.W + 1) + g.W];
     }
   }
-  if (g.tpl_src < 0) {
+  if (g.tpl_src == -1) {
     // gradients that are exactly the template's forward differences are re-derived on the device
     g.grad_derived = true;
     for (int c = 0; c + 1 < g.Wt && g.grad_derived; c++)
@@ -499,16 +509,16 @@ static int load_host_inputs(std::vector<HostGroup>& all, size_t gi) {
         if (!(g.yg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
       }
   } else {
-    g.grad_derived = all[g.tpl_src].grad_derived;
+    g.grad_derived = g.tpl_src == kFromSession ? g.ses_hg->grad_derived : all[g.tpl_src].grad_derived;
   }
-  if (g.geo_src < 0) {
+  if (g.geo_src == -1) {
     g.frac_uniform = true;
     for (int c = 1; c < g.W && g.frac_uniform; c++)
       for (int r = 0; r < g.Hb; r++)
         if (std::memcmp(&g.frac[(size_t)c * g.Hb + r], &g.frac[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
     if (g.compute == 1 && g.frac_uniform) detect_affine_geometry(g);
   } else {
-    const HostGroup& s = all[g.geo_src];
+    const HostGroup& s = g.geo_src == kFromSession ? *g.ses_hg : all[g.geo_src];
     g.frac_uniform = s.frac_uniform;
     g.geo_k = s.geo_k; g.geo_L = s.geo_L;
     g.geo_ax = s.geo_ax; g.geo_bx = s.geo_bx; g.geo_ay = s.geo_ay; g.geo_by = s.geo_by; g.geo_fs = s.geo_fs;
@@ -571,6 +581,7 @@ struct Carve {
 struct Batch::Impl {
   int device = 0;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
   int compute = 0, frame_dt = SS_F64, tpl_dt = SS_F64;
   std::vector<HostGroup> hg;
   std::vector<GroupDesc> gd;
@@ -603,6 +614,12 @@ struct Batch::Impl {
   std::vector<int> event_mode;
   size_t event_used = 0;
   double eval_ms[4] = {0, 0, 0, 0};
+  // non-blocking cycle state: 0 prepared, 1 ready to launch a cycle, 2 cycle in flight, 3 finished
+  int state = 0;
+  int cur_rounds = 0;
+  long long cycle_no = 0, max_cycles = 0;
+  cudaEvent_t ev_cycle = nullptr;
+  std::chrono::steady_clock::time_point t_start;
 
   void eval_timed(int mode) {
     if (timing) {
@@ -630,11 +647,12 @@ struct Batch::Impl {
 
 Batch::Batch() : d(new Impl) {}
 Batch::~Batch() {
-  if (d->stream) cudaStreamSynchronize(d->stream);
+  if (d->stream && d->own_stream) cudaStreamSynchronize(d->stream);
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
+  if (d->ev_cycle) cudaEventDestroy(d->ev_cycle);
   if (d->arena && !d->external_arena) cudaFree(d->arena);
   if (d->h_counters) cudaFreeHost(d->h_counters);
-  if (d->stream) cudaStreamDestroy(d->stream);
+  if (d->stream && d->own_stream) cudaStreamDestroy(d->stream);
   delete d;
 }
 
@@ -679,8 +697,8 @@ static void layout(Batch::Impl* b, char* base) {
     G.ls_mult = in->linesearch_reduction_multiplier;
     const size_t hbw = (size_t)g.Hb * g.W, npx = (size_t)g.Hb * g.fW, N = g.N, nF = g.nF;
     const size_t nq = (size_t)(g.Ht - 1) * (g.Wt - 1);
-    if (g.geo_src >= 0) {  // shared with an earlier group
-      const GroupDesc& S = gd[g.geo_src];
+    if (g.geo_src != -1) {  // shared with an earlier group or held by a session
+      const GroupDesc& S = g.geo_src == kFromSession ? *g.ses_gd : gd[g.geo_src];
       G.frac = S.frac; G.basex = S.basex; G.basey = S.basey;
       G.frac_f = S.frac_f; G.basex_f = S.basex_f; G.basey_f = S.basey_f;
       G.base_mask = S.base_mask; G.min_points = S.min_points;
@@ -711,11 +729,12 @@ static void layout(Batch::Impl* b, char* base) {
       G.pair_ok = (b->compute == 1 && g.geo_k > 0 && g.Hb % 64 == 0 &&
                    reinterpret_cast<uintptr_t>(G.image) % (2 * fsz) == 0) ? 1 : 0;
     }
-    if (g.tpl_src >= 0) {
-      G.tquad = gd[g.tpl_src].tquad;
-      G.gquad = gd[g.tpl_src].gquad;
-      G.tplain = gd[g.tpl_src].tplain;
-      G.tpitch = gd[g.tpl_src].tpitch;
+    if (g.tpl_src != -1) {
+      const GroupDesc& S = g.tpl_src == kFromSession ? *g.ses_gd : gd[g.tpl_src];
+      G.tquad = S.tquad;
+      G.gquad = S.gquad;
+      G.tplain = S.tplain;
+      G.tpitch = S.tpitch;
     } else {
       G.tquad = cv.take<char>(nq * 4 * tsz);
       G.gquad = g.grad_derived ? nullptr : cv.take<char>(nq * 4 * tsz);
@@ -776,7 +795,8 @@ static void layout(Batch::Impl* b, char* base) {
   b->arena_bytes = cv.off + 256;
 }
 
-int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes) {
+int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
+                   const Batch* const* sessions, bool measure_only, void* borrow_stream) {
   Impl* b = d;
   if (n < 1) return fail(SS_ERR_INVALID_ARGUMENT, "no groups");
   b->hg.assign(n, HostGroup{});
@@ -785,6 +805,19 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     int rc = validate_group(&in[i], b->hg[i]);
     if (rc) return rc;
     b->outs[i] = out ? &out[i] : nullptr;
+    if (sessions && sessions[i]) {  // template and geometry resident in a session
+      const Impl* S = sessions[i]->d;
+      if (S->hg.empty()) return fail(SS_ERR_INVALID_ARGUMENT, "session is not prepared");
+      const HostGroup& sh = S->hg[0];
+      HostGroup& g = b->hg[i];
+      if (sh.Ht != g.Ht || sh.Wt != g.Wt || sh.Hb != g.Hb || sh.W != g.W)
+        return fail(SS_ERR_INVALID_ARGUMENT, "group and session differ in template or frame geometry");
+      if (sh.compute != g.compute || sh.tpl_dt != g.tpl_dt || S->device != in[i].gpu_device_id)
+        return fail(SS_ERR_INVALID_ARGUMENT, "group and session differ in precision, template storage or device");
+      g.tpl_src = g.geo_src = kFromSession;
+      g.ses_gd = &S->gd[0];
+      g.ses_hg = &sh;
+    }
     if (i > 0) {
       const HostGroup& a = b->hg[0];
       const HostGroup& c = b->hg[i];
@@ -804,6 +837,10 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
   b->ks = pick_kernels(b->compute, b->frame_dt, b->tpl_dt);
   b->sum = pick_sum(b->frame_dt);
   if (!b->ks.eval || !b->sum) return fail(SS_ERR_INVALID_ARGUMENT, "unsupported dtype combination");
+  if (measure_only) {
+    layout(b, nullptr);
+    return SS_OK;
+  }
 
   auto t0 = std::chrono::steady_clock::now();
   int ndev = 0;
@@ -811,8 +848,13 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
   b->device = in[0].gpu_device_id;
   if (b->device < 0 || b->device >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
   SS_CK(cudaSetDevice(b->device));
-  SS_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
-  SS_CK(cudaHostAlloc(&b->h_counters, 4 * sizeof(int), cudaHostAllocDefault));
+  if (borrow_stream) {  // a server slot: the server's stream, no blocking
+    b->stream = static_cast<cudaStream_t>(borrow_stream);
+    b->own_stream = false;
+  } else {
+    SS_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->own_stream = true;
+  }
   layout(b, nullptr);
   if (external) {
     if (external_bytes < b->arena_bytes) return fail(SS_ERR_OUT_OF_MEMORY, "external arena too small");
@@ -832,7 +874,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     HostGroup& g = b->hg[i];
     GroupDesc& G = b->gd[i];
     const size_t hbw = (size_t)g.Hb * g.W;
-    if (g.geo_src < 0) {
+    if (g.geo_src == -1) {
       SS_CK(cudaMemcpyAsync((void*)G.frac, g.frac.data(), hbw * 8, cudaMemcpyHostToDevice, s));
       SS_CK(cudaMemcpyAsync((void*)G.basex, g.bx.data(), hbw * 8, cudaMemcpyHostToDevice, s));
       SS_CK(cudaMemcpyAsync((void*)G.basey, g.by.data(), hbw * 8, cudaMemcpyHostToDevice, s));
@@ -865,7 +907,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     if (!g.frames_dev)
       SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
     SS_CK(cudaMemcpyAsync(g.d_p0, g.p0.data(), g.p0.size() * 8, cudaMemcpyHostToDevice, s));
-    if (g.tpl_src < 0) {
+    if (g.tpl_src == -1) {
       SS_CK(cudaMemcpyAsync(g.d_templ_stage, g.templ.data(), g.templ.size() * 8, cudaMemcpyHostToDevice, s));
       if (!g.grad_derived) {
         SS_CK(cudaMemcpyAsync(g.d_xg_stage, g.xg.data(), g.xg.size() * 8, cudaMemcpyHostToDevice, s));
@@ -873,8 +915,8 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
       }
     }
     const int nb = 148 * 4;
-    if (g.tpl_src >= 0) {
-      // template quads shared with an earlier group
+    if (g.tpl_src != -1) {
+      // template quads shared with an earlier group or held by a session
     } else if (b->tpl_dt == SS_F64) {
       k_build_tquad<double><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (double*)G.tquad);
       if (!g.grad_derived)
@@ -899,7 +941,8 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
   SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_tile_group, tile_group.data(), tile_group.size() * 4, cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_frame_group, frame_group.data(), frame_group.size() * 4, cudaMemcpyHostToDevice, s));
-  SS_CK(cudaStreamSynchronize(s));
+  // pageable sources are staged before the copies return; an own stream is also drained
+  if (b->own_stream) SS_CK(cudaStreamSynchronize(s));
   return SS_OK;
 }
 
@@ -964,62 +1007,78 @@ static cudaError_t block_tridiag_attr() { return smem_attr(k_block_tridiag, (int
 // later ones (set from the longest search that ended in the cycle before).
 constexpr int kFirstRounds = 8, kMinRounds = 3, kMaxRounds = 16;
 
-static int run_cycles(Batch::Impl* b) {
+// Launches one cycle of every group's state machine on the batch stream (assembly, solve, trial
+// rounds or the cluster line search, correlation, iteration end, final pass) and the copy of the
+// cycle's counters to pinned memory, then records the cycle event. No host synchronisation.
+static int launch_cycle(Batch::Impl* b) {
   cudaStream_t s = b->stream;
-  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
   const int nG = (int)b->gd.size();
-  int max_iter = 1;
-  for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
-  // two half-steps per iteration, a line search of up to kTrialCap trials each
-  const long long max_cycles = 4LL * (max_iter + 2) * (1 + kTrialCap / kMinRounds) + 16;
-  int rounds = kFirstRounds;
-  for (long long cycle = 0; cycle < max_cycles; cycle++) {
-    b->cycles++;
-    b->eval_timed(kAssemble);
-    k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
-    b->launches++;
-    SS_CK(cudaGetLastError());
-    if (b->ks.round) {
-      // trial rounds without a host round trip: as many as the longest search of the previous
-      // cycle took; a search that needs more continues in the next cycle (its group skips
-      // assembly and solve until it has finished)
-      SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
-      for (int r = 0; r < rounds; r++) {
-        b->rounds++;
-        b->eval_timed(kTrial);
-      }
-      b->eval_timed(kCorr);  // correlation sums after the second half-step
-    } else {
+  b->cycles++;
+  b->eval_timed(kAssemble);
+  k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
+  b->launches++;
+  SS_CK(cudaGetLastError());
+  if (b->ks.round) {
+    // trial rounds without a host round trip: as many as the longest search of the previous
+    // cycle took; a search that needs more continues in the next cycle (its group skips
+    // assembly and solve until it has finished)
+    SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
+    for (int r = 0; r < b->cur_rounds; r++) {
       b->rounds++;
-      b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
+      b->eval_timed(kTrial);
     }
-    SS_CK(cudaGetLastError());
-    k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
-    k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
-    b->eval_timed(kFinal);
-    k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
-    b->launches += 3;
-    SS_CK(cudaGetLastError());
-    SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    SS_CK(cudaStreamSynchronize(s));
-    if (b->h_counters[1] >= nG) return SS_OK;
-    if (b->h_counters[0] > 0) rounds = std::min(kMaxRounds, std::max(kMinRounds, b->h_counters[0]));
+    b->eval_timed(kCorr);  // correlation sums after the second half-step
+  } else {
+    b->rounds++;
+    b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
   }
-  return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
+  SS_CK(cudaGetLastError());
+  k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+  k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+  b->eval_timed(kFinal);
+  k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
+  b->launches += 3;
+  SS_CK(cudaGetLastError());
+  SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (!b->ev_cycle) SS_CK(cudaEventCreateWithFlags(&b->ev_cycle, cudaEventDisableTiming));
+  SS_CK(cudaEventRecord(b->ev_cycle, s));
+  return SS_OK;
 }
 
-int Batch::run() {
+int Batch::start() {
   Impl* b = d;
-  auto t0 = std::chrono::steady_clock::now();
+  b->t_start = std::chrono::steady_clock::now();
   SS_CK(cudaSetDevice(b->device));
+  if (!b->h_counters) SS_CK(cudaHostAlloc(&b->h_counters, 4 * sizeof(int), cudaHostAllocDefault));
+  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
   int rc = reset_state(b);
   if (rc) return rc;
   b->cycles = 0;
   b->rounds = 0;
   b->launches = 0;
   b->event_used = 0;
-  rc = run_cycles(b);
+  b->cur_rounds = kFirstRounds;
+  b->cycle_no = 0;
+  b->state = 1;
+  int max_iter = 1;
+  for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
+  // two half-steps per iteration, a line search of up to kTrialCap trials each
+  b->max_cycles = 4LL * (max_iter + 2) * (1 + kTrialCap / kMinRounds) + 16;
+  return SS_OK;
+}
+
+int Batch::step() {
+  Impl* b = d;
+  if (b->state != 1) return fail(SS_ERR_INVALID_ARGUMENT, "batch: step() needs start() and a finished cycle");
+  SS_CK(cudaSetDevice(b->device));
+  int rc = launch_cycle(b);
   if (rc) return rc;
+  b->state = 2;
+  return SS_OK;
+}
+
+// Completion of the batch: final state, error word and staging counters on the host.
+static int finish_run(Batch::Impl* b) {
   SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost,
                         b->stream));
   SS_CK(cudaMemcpyAsync(b->h_counters + 2, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
@@ -1032,7 +1091,48 @@ int Batch::run() {
     SS_CK(cudaEventElapsedTime(&ms, b->events[k], b->events[k + 1]));
     b->eval_ms[b->event_mode[k]] += ms;
   }
-  b->run_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  b->run_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - b->t_start).count();
+  return SS_OK;
+}
+
+int Batch::poll() {
+  Impl* b = d;
+  if (b->state == 3) return 2;
+  if (b->state != 2) return fail(SS_ERR_INVALID_ARGUMENT, "batch: poll() without a cycle in flight");
+  cudaError_t q = cudaEventQuery(b->ev_cycle);
+  if (q == cudaErrorNotReady) return 0;
+  if (q != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cycle: ") + cudaGetErrorString(q));
+  if (b->h_counters[1] >= (int)b->gd.size()) {
+    b->state = 3;
+    int rc = finish_run(b);
+    return rc ? rc : 2;
+  }
+  if (b->h_counters[0] > 0) b->cur_rounds = std::min(kMaxRounds, std::max(kMinRounds, b->h_counters[0]));
+  if (++b->cycle_no >= b->max_cycles) return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
+  b->state = 1;
+  return 1;
+}
+
+int Batch::run() {
+  int rc = start();
+  if (rc) return rc;
+  for (;;) {
+    if ((rc = step())) return rc;
+    SS_CK(cudaStreamSynchronize(d->stream));
+    rc = poll();
+    if (rc < 0) return rc;
+    if (rc == 2) return SS_OK;
+  }
+}
+
+// Resets the batch's groups to their initial state (the start of a server slot; waits on an own
+// stream).
+int Batch::reset() {
+  Impl* b = d;
+  SS_CK(cudaSetDevice(b->device));
+  int rc = reset_state(b);
+  if (rc) return rc;
+  if (b->own_stream) SS_CK(cudaStreamSynchronize(b->stream));
   return SS_OK;
 }
 
@@ -1094,6 +1194,274 @@ int Batch::collect() {
   return SS_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Continuous batching: a table of group slots served by one launch sequence per cycle
+
+struct Server::Impl {
+  struct Slot {
+    Batch* batch = nullptr;  // the group's buffers (its arena) and host metadata
+    bool active = false;
+    bool joining = false;    // admitted since the last cycle was launched
+    int tiles = 0, frames = 0;
+    GroupCtl init;           // initial control state, uploaded when the slot joins
+  };
+  int device = 0, capacity = 0;
+  cudaStream_t stream = nullptr;         // the cycles
+  cudaStream_t upload_stream = nullptr;  // admissions: uploads and resets that need not wait for a cycle
+  cudaEvent_t ev_upload = nullptr;
+  bool configured = false;
+  int compute = 0, frame_dt = 0, tpl_dt = 0;
+  KernelSet ks = {nullptr, nullptr, nullptr};
+  int max_hb = 0, win_bytes = 0, ls_win_bytes = 0;
+  std::vector<Slot> slots;
+  std::vector<GroupDesc> h_gd;
+  GroupCtl* h_ctl = nullptr;  // pinned: the slots' control state after each cycle
+  GroupDesc* d_gd = nullptr;
+  GroupCtl* d_ctl = nullptr;
+  int* d_tile_group = nullptr;
+  int* d_frame_group = nullptr;
+  int tile_cap = 0, frame_cap = 0, n_tiles = 0, n_frames = 0;
+  std::vector<int> tg, fg;
+  int* d_counters = nullptr;  // [0] most trials of a search that ended in the cycle, [1] finished groups
+  int* h_counters = nullptr;  // pinned
+  int* d_err = nullptr;
+  unsigned long long* d_staging = nullptr;
+  cudaEvent_t ev = nullptr;
+  bool dirty = false, in_flight = false;
+  int cur_rounds = kFirstRounds;
+  long long cycles = 0;
+};
+
+Server::Server() : d(new Impl) {}
+Server::~Server() {
+  Impl* v = d;
+  if (v->stream) cudaStreamSynchronize(v->stream);
+  if (v->upload_stream) cudaStreamSynchronize(v->upload_stream);
+  for (auto& sl : v->slots) {
+    delete sl.batch;
+    sl.batch = nullptr;
+  }
+  if (v->ev) cudaEventDestroy(v->ev);
+  if (v->ev_upload) cudaEventDestroy(v->ev_upload);
+  if (v->upload_stream) cudaStreamDestroy(v->upload_stream);
+  cudaFree(v->d_gd);
+  cudaFree(v->d_ctl);
+  cudaFree(v->d_tile_group);
+  cudaFree(v->d_frame_group);
+  cudaFree(v->d_counters);
+  cudaFree(v->d_err);
+  cudaFree(v->d_staging);
+  if (v->h_ctl) cudaFreeHost(v->h_ctl);
+  if (v->h_counters) cudaFreeHost(v->h_counters);
+  if (v->stream) cudaStreamDestroy(v->stream);
+  delete v;
+}
+
+int Server::create(int capacity, int device) {
+  Impl* v = d;
+  if (capacity < 1) return fail(SS_ERR_INVALID_ARGUMENT, "server capacity must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "device out of range");
+  v->device = device;
+  v->capacity = capacity;
+  SS_CK(cudaSetDevice(device));
+  SS_CK(cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking));
+  SS_CK(cudaStreamCreateWithFlags(&v->upload_stream, cudaStreamNonBlocking));
+  SS_CK(cudaEventCreateWithFlags(&v->ev, cudaEventDisableTiming));
+  SS_CK(cudaEventCreateWithFlags(&v->ev_upload, cudaEventDisableTiming));
+  v->slots.assign(capacity, Impl::Slot{});
+  v->h_gd.assign(capacity, GroupDesc{});
+  SS_CK(cudaHostAlloc(&v->h_ctl, capacity * sizeof(GroupCtl), cudaHostAllocDefault));
+  SS_CK(cudaHostAlloc(&v->h_counters, 4 * sizeof(int), cudaHostAllocDefault));
+  SS_CK(cudaMalloc(&v->d_gd, capacity * sizeof(GroupDesc)));
+  SS_CK(cudaMalloc(&v->d_ctl, capacity * sizeof(GroupCtl)));
+  SS_CK(cudaMalloc(&v->d_counters, 4 * sizeof(int)));
+  SS_CK(cudaMalloc(&v->d_err, sizeof(int)));
+  SS_CK(cudaMalloc(&v->d_staging, 6 * sizeof(unsigned long long)));
+  SS_CK(cudaMemset(v->d_counters, 0, 4 * sizeof(int)));
+  SS_CK(cudaMemset(v->d_err, 0, sizeof(int)));
+  SS_CK(cudaMemset(v->d_staging, 0, 6 * sizeof(unsigned long long)));
+  // empty slots are in the done phase: every kernel passes them by
+  for (int k = 0; k < capacity; k++) {
+    std::memset(&v->h_ctl[k], 0, sizeof(GroupCtl));
+    v->h_ctl[k].phase = kPhDone;
+  }
+  SS_CK(cudaMemcpy(v->d_ctl, v->h_ctl, capacity * sizeof(GroupCtl), cudaMemcpyHostToDevice));
+  SS_CK(cudaMemset(v->d_gd, 0, capacity * sizeof(GroupDesc)));
+  return SS_OK;
+}
+
+int Server::admit(const ss_inputs* in, ss_outputs* out, const Batch* session, void* arena, size_t arena_bytes,
+                  int* slot_out) {
+  Impl* v = d;
+  if (!in || !slot_out) return fail(SS_ERR_INVALID_ARGUMENT, "bad admit arguments");
+  int slot = -1;
+  for (int k = 0; k < v->capacity; k++)
+    if (!v->slots[k].batch) {
+      slot = k;
+      break;
+    }
+  if (slot < 0) return fail(SS_ERR_BUSY, "every server slot is taken");
+  if (in->gpu_device_id != v->device) return fail(SS_ERR_INVALID_ARGUMENT, "group and server differ in device");
+  Batch* b = new Batch;
+  const Batch* ses[1] = {session};
+  int rc = b->prepare(1, in, out, arena, arena_bytes, ses, false, v->upload_stream);
+  if (!rc) rc = b->reset();
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  Batch::Impl* bi = b->d;
+  if (!v->configured) {
+    v->compute = bi->compute;
+    v->frame_dt = bi->frame_dt;
+    v->tpl_dt = bi->tpl_dt;
+    v->ks = bi->ks;
+    v->configured = true;
+  } else if (bi->compute != v->compute || bi->frame_dt != v->frame_dt || bi->tpl_dt != v->tpl_dt) {
+    delete b;
+    return fail(SS_ERR_INVALID_ARGUMENT, "all groups of a server need the same precision, frame and template types");
+  }
+  v->max_hb = std::max(v->max_hb, bi->max_hb);
+  v->win_bytes = std::max(v->win_bytes, bi->win_bytes);
+  v->ls_win_bytes = std::max(v->ls_win_bytes, bi->ls_win_bytes);
+  Impl::Slot& sl = v->slots[slot];
+  sl.batch = b;
+  sl.joining = true;
+  sl.active = true;
+  const HostGroup& g = bi->hg[0];
+  sl.tiles = g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
+  sl.frames = g.nF;
+  GroupDesc G = bi->gd[0];
+  G.err = v->d_err;
+  G.staging = v->d_staging;
+  G.ls_max_trials = v->d_counters;
+  v->h_gd[slot] = G;
+  sl.init = bi->h_ctl[0];  // not into h_ctl: a cycle in flight still copies into it
+  v->dirty = true;
+  *slot_out = slot;
+  return SS_OK;
+}
+
+// Tile and frame tables over the active slots, descriptors and the joining slots' control state.
+static int server_tables(Server::Impl* v) {
+  cudaStream_t s = v->stream;
+  v->n_tiles = 0;
+  v->n_frames = 0;
+  for (int k = 0; k < v->capacity; k++) {
+    auto& sl = v->slots[k];
+    if (!sl.active) continue;
+    v->h_gd[k].tile_base = v->n_tiles;
+    v->h_gd[k].frame_base = v->n_frames;
+    v->n_tiles += sl.tiles;
+    v->n_frames += sl.frames;
+  }
+  if (v->n_tiles > v->tile_cap || v->n_frames > v->frame_cap) {  // between cycles: nothing in flight
+    SS_CK(cudaStreamSynchronize(s));
+    cudaFree(v->d_tile_group);
+    cudaFree(v->d_frame_group);
+    v->tile_cap = std::max(2 * v->tile_cap, v->n_tiles);
+    v->frame_cap = std::max(2 * v->frame_cap, v->n_frames);
+    SS_CK(cudaMalloc(&v->d_tile_group, (size_t)v->tile_cap * sizeof(int)));
+    SS_CK(cudaMalloc(&v->d_frame_group, (size_t)v->frame_cap * sizeof(int)));
+  }
+  v->tg.assign(std::max(1, v->n_tiles), 0);
+  v->fg.assign(std::max(1, v->n_frames), 0);
+  for (int k = 0; k < v->capacity; k++) {
+    auto& sl = v->slots[k];
+    if (!sl.active) continue;
+    for (int t = 0; t < sl.tiles; t++) v->tg[v->h_gd[k].tile_base + t] = k;
+    for (int f = 0; f < sl.frames; f++) v->fg[v->h_gd[k].frame_base + f] = k;
+  }
+  // pageable sources are staged before the copies return
+  SS_CK(cudaMemcpyAsync(v->d_gd, v->h_gd.data(), v->capacity * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
+  if (v->n_tiles)
+    SS_CK(cudaMemcpyAsync(v->d_tile_group, v->tg.data(), v->n_tiles * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (v->n_frames)
+    SS_CK(cudaMemcpyAsync(v->d_frame_group, v->fg.data(), v->n_frames * sizeof(int), cudaMemcpyHostToDevice, s));
+  for (int k = 0; k < v->capacity; k++) {
+    auto& sl = v->slots[k];
+    if (!sl.joining) continue;
+    SS_CK(cudaMemcpyAsync(v->d_ctl + k, &sl.init, sizeof(GroupCtl), cudaMemcpyHostToDevice, s));
+    sl.joining = false;
+  }
+  v->dirty = false;
+  return SS_OK;
+}
+
+int Server::step() {
+  Impl* v = d;
+  if (v->in_flight) return fail(SS_ERR_INVALID_ARGUMENT, "server: a cycle is in flight");
+  SS_CK(cudaSetDevice(v->device));
+  if (v->dirty) {
+    // joining groups' uploads and resets come first
+    SS_CK(cudaEventRecord(v->ev_upload, v->upload_stream));
+    SS_CK(cudaStreamWaitEvent(v->stream, v->ev_upload, 0));
+    int rc = server_tables(v);
+    if (rc) return rc;
+  }
+  if (v->n_tiles == 0) return SS_OK;  // nothing to run
+  cudaStream_t s = v->stream;
+  const int nG = v->capacity;
+  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
+  v->cycles++;
+  v->ks.eval(kAssemble, v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->max_hb, v->win_bytes);
+  k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(v->d_gd, v->d_ctl);
+  if (v->ks.round) {
+    SS_CK(cudaMemsetAsync(v->d_counters, 0, sizeof(int), s));
+    for (int r = 0; r < v->cur_rounds; r++) v->ks.round(v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->win_bytes);
+    v->ks.eval(kCorr, v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->max_hb, v->win_bytes);
+  } else {
+    v->ks.ls(v->n_frames, s, v->d_gd, v->d_frame_group, v->d_ctl, v->ls_win_bytes);
+  }
+  k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(v->d_gd, v->d_ctl, nG);
+  k_iter_end<<<nG, kSolveThreads, 0, s>>>(v->d_gd, v->d_ctl);
+  v->ks.eval(kFinal, v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->max_hb, v->win_bytes);
+  k_final<<<nG, 256, 0, s>>>(v->d_gd, v->d_ctl, v->d_counters + 1);
+  SS_CK(cudaGetLastError());
+  SS_CK(cudaMemcpyAsync(v->h_counters, v->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  SS_CK(cudaMemcpyAsync(v->h_ctl, v->d_ctl, nG * sizeof(GroupCtl), cudaMemcpyDeviceToHost, s));
+  SS_CK(cudaEventRecord(v->ev, s));
+  v->in_flight = true;
+  return SS_OK;
+}
+
+int Server::poll(int* done, int max_done, int* n_done) {
+  Impl* v = d;
+  *n_done = 0;
+  if (v->in_flight) {
+    cudaError_t q = cudaEventQuery(v->ev);
+    if (q == cudaErrorNotReady) return 0;
+    if (q != cudaSuccess) return fail(SS_ERR_CUDA, std::string("server cycle: ") + cudaGetErrorString(q));
+    v->in_flight = false;
+    int err = 0;
+    SS_CK(cudaMemcpy(&err, v->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err & 1) return fail(SS_ERR_CUDA, "a shared-memory staging copy did not complete in time");
+    if (v->h_counters[0] > 0) v->cur_rounds = std::min(kMaxRounds, std::max(kMinRounds, v->h_counters[0]));
+  }
+  for (int k = 0; k < v->capacity && *n_done < max_done; k++) {
+    auto& sl = v->slots[k];
+    if (!sl.active || sl.joining || v->h_ctl[k].phase != kPhDone) continue;
+    // the group has stopped: its control state to its own batch, then its outputs to the host
+    Batch::Impl* bi = sl.batch->d;
+    SS_CK(cudaMemcpy(bi->d_ctl, v->d_ctl + k, sizeof(GroupCtl), cudaMemcpyDeviceToDevice));
+    int rc = sl.batch->collect();
+    if (rc) return rc;
+    delete sl.batch;
+    sl = Impl::Slot{};
+    v->dirty = true;
+    done[(*n_done)++] = k;
+  }
+  return 1;
+}
+
+int Server::active() const {
+  int n = 0;
+  for (auto& sl : d->slots) n += sl.active ? 1 : 0;
+  return n;
+}
+
 int Batch::cycles() const { return d->cycles; }
 int Batch::rounds() const { return d->rounds; }
 int Batch::n_groups() const { return (int)d->gd.size(); }
@@ -1130,6 +1498,15 @@ struct ss_batch {
   ss::Batch b;
 };
 
+struct ss_server {
+  ss::Server v;
+};
+
+struct ss_session {
+  ss::Batch b;
+  std::vector<double> zeros, kx, ky;
+};
+
 int ss_batch_create(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_batch** batch) {
   if (!batch || !in || n_groups < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad batch arguments");
   *batch = nullptr;
@@ -1142,6 +1519,120 @@ int ss_batch_create(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_b
   *batch = h;
   return SS_OK;
 }
+
+int ss_session_create(const ss_inputs* proto, ss_session** session) {
+  if (!proto || !session) return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad session arguments");
+  *session = nullptr;
+  const int64_t hb = proto->basex.rows, w = proto->basex.cols;
+  if (hb < 1 || w < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "basex is empty");
+  ss_session* h = new ss_session;
+  // a one-frame group of zeros carries the session's template and geometry into device memory
+  ss_inputs in = *proto;
+  h->zeros.assign((size_t)hb * w, 0.0);
+  h->kx.assign((size_t)w + 1, 0.0);
+  h->ky.assign((size_t)w + 1, 0.0);
+  in.n_frames = 1;
+  in.bm_data = {h->zeros.data(), hb, w, SS_F64, SS_HOST};
+  in.est_dx_knots = {h->kx.data(), w + 1, 1, SS_F64, SS_HOST};
+  in.est_dy_knots = {h->ky.data(), w + 1, 1, SS_F64, SS_HOST};
+  int rc = h->b.prepare(1, &in, nullptr, nullptr, 0);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *session = h;
+  return SS_OK;
+}
+
+void ss_session_destroy(ss_session* session) { delete session; }
+
+static std::vector<const ss::Batch*> session_list(int32_t n, ss_session* const* sessions) {
+  std::vector<const ss::Batch*> v((size_t)n, nullptr);
+  if (sessions)
+    for (int32_t i = 0; i < n; i++) v[i] = sessions[i] ? &sessions[i]->b : nullptr;
+  return v;
+}
+
+int ss_batch_measure(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_session* const* sessions,
+                     int64_t* arena_bytes) {
+  if (!in || n_groups < 1 || !arena_bytes) return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad batch arguments");
+  ss::Batch b;
+  const auto ses = session_list(n_groups, sessions);
+  int rc = b.prepare(n_groups, in, out, nullptr, 0, ses.data(), true);
+  if (rc) return rc;
+  *arena_bytes = (int64_t)b.arena_bytes();
+  return SS_OK;
+}
+
+int ss_batch_create_ex(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_session* const* sessions,
+                       void* arena, int64_t arena_bytes, ss_batch** batch) {
+  if (!batch || !in || n_groups < 1 || (arena && arena_bytes <= 0))
+    return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad batch arguments");
+  *batch = nullptr;
+  ss_batch* h = new ss_batch;
+  const auto ses = session_list(n_groups, sessions);
+  int rc = h->b.prepare(n_groups, in, out, arena, arena ? (size_t)arena_bytes : 0, ses.data());
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *batch = h;
+  return SS_OK;
+}
+
+int ss_batch_start(ss_batch* batch) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  return batch->b.start();
+}
+
+int ss_batch_step(ss_batch* batch) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  return batch->b.step();
+}
+
+int ss_batch_poll(ss_batch* batch) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  return batch->b.poll();
+}
+
+int ss_server_create(int32_t capacity, int32_t device, ss_server** server) {
+  if (!server) return ss::fail(SS_ERR_INVALID_ARGUMENT, "server is NULL");
+  *server = nullptr;
+  ss_server* h = new ss_server;
+  int rc = h->v.create(capacity, device);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *server = h;
+  return SS_OK;
+}
+
+int ss_server_admit(ss_server* server, const ss_inputs* in, ss_outputs* out, ss_session* session, void* arena,
+                    int64_t arena_bytes, int32_t* slot) {
+  if (!server || !slot || (arena && arena_bytes <= 0)) return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad admit arguments");
+  int k = -1;
+  int rc = server->v.admit(in, out, session ? &session->b : nullptr, arena, arena ? (size_t)arena_bytes : 0, &k);
+  *slot = k;
+  return rc;
+}
+
+int ss_server_step(ss_server* server) {
+  if (!server) return ss::fail(SS_ERR_INVALID_ARGUMENT, "server is NULL");
+  return server->v.step();
+}
+
+int ss_server_poll(ss_server* server, int32_t* done_slots, int32_t max_done, int32_t* n_done) {
+  if (!server || !n_done || (max_done > 0 && !done_slots)) return ss::fail(SS_ERR_INVALID_ARGUMENT, "bad poll arguments");
+  int n = 0;
+  int rc = server->v.poll(done_slots, max_done, &n);
+  *n_done = n;
+  return rc;
+}
+
+int32_t ss_server_active(const ss_server* server) { return server ? server->v.active() : 0; }
+
+void ss_server_destroy(ss_server* server) { delete server; }
 
 int ss_batch_run(ss_batch* batch) {
   if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");

@@ -24,9 +24,22 @@ class Batch {
 
   // Validates the groups, lays out and fills device memory (one arena; or the caller's
   // `external` buffer of `external_bytes` when given). Outputs are remembered for collect().
-  int prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes);
+  // sessions[i], when given and not null, is a prepared batch whose first group's template and
+  // geometry buffers group i uses instead of its own (they must outlive this batch). With
+  // measure_only the call stops after computing arena_bytes(): no device work. borrow_stream (a
+  // cudaStream_t) runs the batch on the caller's stream without blocking on it.
+  int prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
+              const Batch* const* sessions = nullptr, bool measure_only = false, void* borrow_stream = nullptr);
   // Runs every group from its initial knots to its stop criterion.
   int run();
+  // The same run one cycle at a time without blocking: start() resets every group to its initial
+  // knots, step() launches one cycle on the batch stream, poll() returns 0 while that cycle runs,
+  // 1 when it has finished and another is needed, 2 when every group has stopped.
+  int start();
+  int step();
+  int poll();
+  // Resets every group to its initial state (the start of a server slot; waits on an own stream).
+  int reset();
   // Copies the results into the ss_outputs given to prepare().
   int collect();
 
@@ -38,6 +51,30 @@ class Batch {
   int n_groups() const;
   const GroupCtl* host_ctl() const;
   void* stream() const;
+
+ private:
+  friend class Server;
+  Impl* d;
+};
+
+// Continuous batching: a table of `capacity` group slots on one stream. admit() prepares a group
+// (in the caller's arena, with a session's resident buffers) into a free slot; step() applies the
+// admissions and retirements since the last cycle and launches one cycle of every active group;
+// poll() returns 0 while the cycle runs, else 1 after collecting the outputs of the groups that
+// stopped (their slots listed in `done`, their arenas free again).
+class Server {
+ public:
+  struct Impl;
+  Server();
+  ~Server();
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+  int create(int capacity, int device);
+  int admit(const ss_inputs* in, ss_outputs* out, const Batch* session, void* arena, size_t arena_bytes,
+            int* slot);
+  int step();
+  int poll(int* done, int max_done, int* n_done);
+  int active() const;
 
  private:
   Impl* d;

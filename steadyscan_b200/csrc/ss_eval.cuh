@@ -32,6 +32,7 @@ constexpr int kEvalWarps = 8;       // warps per assembly/final CTA
 constexpr int kLsCluster = 8;       // CTAs per frame in the line-search cluster
 constexpr int kLsMaxKnots = 256;    // knots per cluster CTA: frame_w <= kLsCluster * kLsMaxKnots
 constexpr int kMaxFrameW = kLsCluster * kLsMaxKnots;
+constexpr int kMinWinFrames = 4;    // frames of a tile worth staging a template window for
 
 // Resident 256-thread CTAs per SM requested from the register allocator: the FP32 path is
 // latency-bound on frame loads and template gathers and needs the warps; the FP64 path keeps its
@@ -464,12 +465,12 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
   const int f_end = min(G.nF, (fb + 1) * fpc);
 
   // Precision 'S': stage the template rows every pixel of this CTA can sample (the column's basey
-  // range widened by its frames' y knots) into shared memory; windows that would not fit fall back
-  // to the global template.
+  // range widened by its frames' y knots) into shared memory; windows that would not fit, and
+  // tiles of too few frames to repay the copy, use the global template.
   TWin win{nullptr, 0, 0, 0};
   if constexpr (sizeof(Acc) == 4) {
     const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
-    if (win_cap >= 2 && !G.gquad) {
+    if (win_cap >= 2 && !G.gquad && f_end - fb * fpc >= kMinWinFrames) {
       const size_t geo_bytes = (!affine && Hb <= stage_rows) ? stage_bytes<Acc>(Hb) : 0;
       float* wbuf = reinterpret_cast<float*>(smem + geo_bytes);
       uint64_t* bar = reinterpret_cast<uint64_t*>(smem + geo_bytes + (size_t)win_bytes);
@@ -867,7 +868,6 @@ __device__ __forceinline__ int atomic_add_acq_rel(int* p, int v) {
   asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
 }
-constexpr int kMinWinFrames = 4;    // searching frames of a tile worth staging a window for
 
 // Decision for frame f after all its columns of the round were evaluated (one warp).
 __device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f) {
