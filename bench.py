@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--plain-groups", type=int, default=2)
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="seconds of generated serving load (8 sessions, 0 to skip)")
+    ap.add_argument("--serve-warm", action="store_true",
+                    help="start each session's groups from its last displacement instead of zero")
     return ap.parse_args()
 
 
@@ -258,7 +260,8 @@ def serve(args, device, seconds, plain_d):
     from steadyscan_b200 import api, serving
     from steadyscan_b200._lib import SS_U16
     n_ses, pool_frames = 8, 512
-    server = serving.Server(memory_budget=24 << 30, device=device.index or 0, max_active=96)
+    server = serving.Server(memory_budget=24 << 30, device=device.index or 0, max_active=96,
+                            warm_start=args.serve_warm)
     pools = []
     for s in range(n_ses):
         groups, dev, _, lay = make_workload(pool_frames, 512, pool_frames, "S", 1005 + 31 * s, device)
@@ -296,8 +299,9 @@ def serve(args, device, seconds, plain_d):
            "ms_per_cycle": 1000.0 * elapsed / max(1, server.cycles),
            "iterations_mean": float(np.mean(iters)) if iters else None,
            "plain_serial_frames_per_s": plain_d,
+           "warm_start": args.serve_warm,
            "load": "Poisson 30 Hz per session, 2x for 2 s of every 10 s, groups U[1,64] frames of 512x512 uint16, "
-                   "precision S, warm starts"}
+                   "precision S"}
     server.close()
     return out
 

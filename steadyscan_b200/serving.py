@@ -73,7 +73,7 @@ class SessionState:
     sid: int
     proto: dict
     session: api.Session
-    last_knots: tuple | None = None  # (dx, dy) at the end of the latest finished group
+    last_knots: tuple | None = None  # (dx, dy) of the latest group that aligned well, its last frame
     memo: dict = field(default_factory=dict)  # converted template / geometry matrices, reused per request
     keep: list = field(default_factory=list)
 
@@ -163,8 +163,8 @@ class Server:
         ex, ey = r.est_dx, r.est_dy
         if ex is None:
             if self.warm_start and st.last_knots is not None:
-                # the displacement where the session's last group ended, for every knot: the best
-                # guess of a drifting displacement a moment later
+                # the displacement where the session's last group ended, for every knot: the guess
+                # of a drifting displacement a moment later
                 ex = np.full((w1, r.n_frames), st.last_knots[0])
                 ey = np.full((w1, r.n_frames), st.last_knots[1])
             else:
@@ -214,26 +214,32 @@ class Server:
         r._c = None
         self.pool.release(r.block)
         st = self.sessions[r.sid]
-        st.last_knots = (float(np.asarray(r.result["dx"])[-1]), float(np.asarray(r.result["dy"])[-1]))
+        # warm start: the median of the last frame's knots without its last two (the chain's last
+        # knot is never solved, and the last block column is bounded by a fixed knot); a group that
+        # did not align (low correlation) leaves the warm start as it was
+        w1 = r.args["tfrac"].shape[1] + 1
+        dx = np.asarray(r.result["dx"])[-w1:-2]
+        dy = np.asarray(r.result["dy"])[-w1:-2]
+        corr = np.asarray(r.result["frame_corr"], dtype=np.float64)
+        if dx.size and np.all(np.isfinite(corr)) and float(np.mean(corr)) >= 0.5:
+            st.last_knots = (float(np.median(dx)), float(np.median(dy)))
         self.done.append(r)
 
     def tick(self) -> int:
-        """One pass of the loop: if the cycle in flight has finished, retire the groups that stopped,
-        admit queued ones and launch the next cycle; else admit queued ones (they join at the next
-        cycle). Returns the number of groups in the server."""
+        """One pass of the loop: once the cycle in flight has finished, retire the groups that
+        stopped and launch the next cycle; then admit queued requests while the GPU works (they join
+        at the following cycle). Returns the number of groups in the server."""
         n = C.c_int32(0)
         rc = self._lib.ss_server_poll(self._h, self._done_buf, self.max_active, C.byref(n))
         if rc < 0:
             check(rc)
-        if rc == 0:
-            self._admit()
-            return len(self.by_slot)
-        for k in range(n.value):
-            self._retire(self._done_buf[k])
+        if rc == 1:
+            for k in range(n.value):
+                self._retire(self._done_buf[k])
+            if self.by_slot:
+                check(self._lib.ss_server_step(self._h))
+                self.cycles += 1
         self._admit()
-        if self.by_slot:
-            check(self._lib.ss_server_step(self._h))
-            self.cycles += 1
         return len(self.by_slot)
 
     def drain(self, timeout_s: float = 600.0):
