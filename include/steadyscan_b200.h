@@ -95,6 +95,9 @@ typedef struct ss_inputs {
   /* Extension: storage type of template samples on the device for precision 'S'
    * (SS_F32 default, or SS_F16). Precision 'D' always keeps FP64. */
   int32_t template_storage;
+  /* Extension (a tuning choice, no effect on precision D results): frames per evaluation tile,
+   * 1..64; 0 splits the group's frames into even chunks of at most 32. */
+  int32_t frames_per_cta;
 } ss_inputs;
 
 /* Outputs; every pointer may be NULL (that output is then not produced). Host memory. Index
@@ -153,6 +156,11 @@ SS_API int ss_batch_run(ss_batch* batch);
 SS_API int ss_batch_collect(ss_batch* batch);
 /* 1 turns on CUDA-event timing of the evaluation kernels for later runs (adds events to the stream). */
 SS_API int ss_batch_set_timing(ss_batch* batch, int32_t on);
+/* 1 (the default) runs a batch as one CUDA graph: device-side loops over cycles and line-search trial
+ * rounds, launched once per ss_batch_run / ss_batch_step, with no host round trip until every group
+ * has stopped (ss_batch_poll then returns 2). 0 launches one cycle per ss_batch_step from the host.
+ * Timing (ss_batch_set_timing) always runs host-launched cycles. Results are the same either way. */
+SS_API int ss_batch_set_graph(ss_batch* batch, int32_t on);
 SS_API int ss_batch_stats_get(const ss_batch* batch, ss_batch_stats* stats);
 /* The cudaStream_t the batch launches on, as an opaque pointer (for the caller's own events). */
 SS_API void* ss_batch_stream(const ss_batch* batch);

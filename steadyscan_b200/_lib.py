@@ -31,6 +31,7 @@ class SSInputs(C.Structure):
         ("max_filter_iterations", C.c_int32), ("filter_deactivation_threshold", C.c_double),
         ("lam", C.c_double), ("linesearch_reduction_multiplier", C.c_double), ("solver_id", C.c_int32),
         ("filter_id", C.c_int32), ("gpu_device_id", C.c_int32), ("template_storage", C.c_int32),
+        ("frames_per_cta", C.c_int32),
     ]
 
 
@@ -80,6 +81,8 @@ def load(build_if_missing: bool = True):
         getattr(lib, name).restype = C.c_int
     lib.ss_batch_set_timing.argtypes = [C.c_void_p, C.c_int32]
     lib.ss_batch_set_timing.restype = C.c_int
+    lib.ss_batch_set_graph.argtypes = [C.c_void_p, C.c_int32]
+    lib.ss_batch_set_graph.restype = C.c_int
     lib.ss_batch_stats_get.argtypes = [C.c_void_p, C.POINTER(SSBatchStats)]
     lib.ss_batch_stats_get.restype = C.c_int
     lib.ss_batch_stream.argtypes = [C.c_void_p]

@@ -99,7 +99,7 @@ def _inputs(args: dict, template_storage=None, memo: dict | None = None):
         float(args["filter_strength"]), int(args["max_filter_iterations"]),
         float(args["filter_deactivation_threshold"]), float(args.get("lambda", 0.0)),
         float(args["linesearch_reduction_multiplier"]), int(args["solver_id"]), int(args["filter_id"]),
-        int(args["gpu_device_id"]), int(ts or 0))
+        int(args["gpu_device_id"]), int(ts or 0), int(args.get("frames_per_cta", 0) or 0))
     return i, keep
 
 
@@ -332,6 +332,10 @@ class Batch:
 
     def set_timing(self, on: bool):
         check(self._lib.ss_batch_set_timing(self._h, 1 if on else 0))
+
+    def set_graph(self, on: bool):
+        """True (default): the whole run as one CUDA graph; False: one host-launched cycle per step."""
+        check(self._lib.ss_batch_set_graph(self._h, 1 if on else 0))
 
     def stats(self) -> dict:
         from ._lib import SSBatchStats

@@ -159,12 +159,11 @@ using SumFn = void (*)(const void* img, size_t n, double* parts, double* out, cu
 template <class Acc, class FrameT, class TplT>
 static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
                                const GroupCtl* ctl, int max_hb, int win_bytes) {
-  if (tiles <= 0) return cudaSuccess;
   constexpr int kMaxDyn = kStageBytes + kWinBytes + 64;
   cudaError_t ae = smem_attr(k_eval<Acc, FrameT, TplT, kAssemble>, kMaxDyn);
   if (ae == cudaSuccess) ae = smem_attr(k_eval<Acc, FrameT, TplT, kFinal>, kMaxDyn);
   if (ae == cudaSuccess) ae = smem_attr(k_eval<Acc, FrameT, TplT, kCorr>, kMaxDyn);
-  if (ae != cudaSuccess) return ae;
+  if (ae != cudaSuccess || tiles <= 0) return ae;
   const int rows = stage_bytes<Acc>(max_hb) <= (size_t)kStageBytes ? max_hb : 0;
   if (sizeof(Acc) != 4) win_bytes = 0;
   win_bytes = std::min(win_bytes, kWinBytes) & ~15;
@@ -182,13 +181,13 @@ static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupD
 template <class Acc, class FrameT, class TplT>
 static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl,
                              int win_bytes) {
-  if (frames <= 0) return cudaSuccess;
   if (sizeof(Acc) != 4) win_bytes = 0;
   win_bytes = std::min(win_bytes, kLsWinBytes) & ~15;
   if (win_bytes) {
     cudaError_t ae = smem_attr(k_linesearch<Acc, FrameT, TplT>, kLsWinBytes + 16);
     if (ae != cudaSuccess) return ae;
   }
+  if (frames <= 0) return cudaSuccess;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(frames * kLsCluster, 1, 1);
   cfg.blockDim = dim3(LsShape<Acc>::threads, 1, 1);
@@ -211,9 +210,8 @@ using RoundFn = cudaError_t (*)(int tiles, cudaStream_t s, const GroupDesc* gd, 
 template <class FrameT, class TplT>
 static cudaError_t round_launch(int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, GroupCtl* ctl,
                                 int win_bytes) {
-  if (tiles <= 0) return cudaSuccess;
   cudaError_t ae = smem_attr(k_trial_round<FrameT, TplT>, kWinBytes + 16);
-  if (ae != cudaSuccess) return ae;
+  if (ae != cudaSuccess || tiles <= 0) return ae;
   win_bytes = std::min(win_bytes, kWinBytes) & ~15;
   k_trial_round<FrameT, TplT><<<tiles, 32 * kEvalWarps, win_bytes ? (size_t)win_bytes + 16 : 0, s>>>(gd, tg, ctl,
                                                                                                       win_bytes);
@@ -347,6 +345,17 @@ static int parse_flags(const char* flags, int& compute, int& bits) {
 // Source index of template and geometry buffers that a resident session holds.
 constexpr int kFromSession = -2;
 
+// Run counters of a batch on the device (and their pinned host copy).
+enum RunCounter {
+  kCtrMaxTrials = 0,  // most trials of a line search that ended in the cycle (host-driven cycles)
+  kCtrDone = 1,       // groups that have finished
+  kCtrCycles = 2,     // cycles run by the graph
+  kCtrRound = 3,      // trial rounds of the graph's current cycle
+  kCtrRounds = 4,     // trial rounds run by the graph
+  kCtrBound = 5,      // bit 0: the graph stopped at the cycle bound; bit 1: a cycle hit its round bound
+  kCounters = 8
+};
+
 struct HostGroup {
   const ss_inputs* in = nullptr;
   int compute = 0, flags = 0;
@@ -399,7 +408,11 @@ static int validate_group(const ss_inputs* in, HostGroup& g) {
   g.nF = in->n_frames;
   if (g.nF < 1) return fail(SS_ERR_INVALID_ARGUMENT, "n_frames must be positive");
   g.fW = g.W * g.nF;
-  {  // frame chunks of the evaluation tiles: at most 32 frames, as even as the group allows
+  if (in->frames_per_cta < 0 || in->frames_per_cta > kMaxChunk)
+    return fail(SS_ERR_INVALID_ARGUMENT, "frames_per_cta must be 0 or 1..64");
+  if (in->frames_per_cta > 0) {
+    g.frames_per_cta = in->frames_per_cta;
+  } else {  // frame chunks of the evaluation tiles: at most 32 frames, as even as the group allows
     const int chunks = (g.nF + 31) / 32;
     g.frames_per_cta = (g.nF + chunks - 1) / chunks;
   }
@@ -593,7 +606,7 @@ struct Batch::Impl {
   GroupCtl* d_ctl = nullptr;
   int* d_tile_group = nullptr;
   int* d_frame_group = nullptr;
-  int* d_counters = nullptr;  // [0] most trials of a search that ended in the cycle, [1] finished groups
+  int* d_counters = nullptr;  // kCounters run counters (kCtr*)
   int* d_err = nullptr;       // device error word (bit 0: a shared-memory staging copy timed out)
   unsigned long long* d_staging = nullptr;  // staging counters of the run
   double* d_sum_parts = nullptr;            // partial sums of k_sum_image
@@ -620,6 +633,11 @@ struct Batch::Impl {
   long long cycle_no = 0, max_cycles = 0;
   cudaEvent_t ev_cycle = nullptr;
   std::chrono::steady_clock::time_point t_start;
+  // the whole run as one CUDA graph (device-side loops over cycles and trial rounds)
+  bool use_graph = true;
+  bool graph_run = false;  // the run in flight was launched as the graph
+  cudaGraphExec_t run_exec = nullptr;
+  cudaStream_t cap_stream = nullptr;
 
   void eval_timed(int mode) {
     if (timing) {
@@ -636,7 +654,6 @@ struct Batch::Impl {
     if (mode == kTrial && ks.round) ks.round(n_tiles, stream, d_gd, d_tile_group, d_ctl, win_bytes);
     else if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl, ls_win_bytes);
     else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb, win_bytes);
-    launches++;
     if (timing) {
       cudaEventRecord(events[event_used + 1], stream);
       event_mode[event_used] = mode;
@@ -650,6 +667,8 @@ Batch::~Batch() {
   if (d->stream && d->own_stream) cudaStreamSynchronize(d->stream);
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
   if (d->ev_cycle) cudaEventDestroy(d->ev_cycle);
+  if (d->run_exec) cudaGraphExecDestroy(d->run_exec);
+  if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
   if (d->arena && !d->external_arena) cudaFree(d->arena);
   if (d->h_counters) cudaFreeHost(d->h_counters);
   if (d->stream && d->own_stream) cudaStreamDestroy(d->stream);
@@ -668,7 +687,7 @@ static void layout(Batch::Impl* b, char* base) {
   std::vector<GroupDesc>& gd = b->gd;
   gd.assign(b->hg.size(), GroupDesc{});
   b->d_err = cv.take<int>(1);
-  b->d_counters = cv.take<int>(4);
+  b->d_counters = cv.take<int>(kCounters);
   b->d_staging = cv.take<unsigned long long>(6);
   b->d_sum_parts = cv.take<double>(kSumBlocks);
   b->win_bytes = 0;
@@ -990,7 +1009,7 @@ static int reset_state(Batch::Impl* b) {
     }
   }
   SS_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl.data(), b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyHostToDevice, s));
-  SS_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(int), s));
+  SS_CK(cudaMemsetAsync(b->d_counters, 0, kCounters * sizeof(int), s));
   SS_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), s));
   SS_CK(cudaMemsetAsync(b->d_staging, 0, 6 * sizeof(unsigned long long), s));
   return SS_OK;
@@ -1007,29 +1026,23 @@ static cudaError_t block_tridiag_attr() { return smem_attr(k_block_tridiag, (int
 // later ones (set from the longest search that ended in the cycle before).
 constexpr int kFirstRounds = 8, kMinRounds = 3, kMaxRounds = 16;
 
-// Launches one cycle of every group's state machine on the batch stream (assembly, solve, trial
+// Enqueues one cycle of every group's state machine on the batch stream (assembly, solve, trial
 // rounds or the cluster line search, correlation, iteration end, final pass) and the copy of the
-// cycle's counters to pinned memory, then records the cycle event. No host synchronisation.
-static int launch_cycle(Batch::Impl* b) {
+// cycle's counters to pinned memory.
+static int enqueue_cycle(Batch::Impl* b) {
   cudaStream_t s = b->stream;
   const int nG = (int)b->gd.size();
-  b->cycles++;
   b->eval_timed(kAssemble);
   k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
-  b->launches++;
   SS_CK(cudaGetLastError());
   if (b->ks.round) {
     // trial rounds without a host round trip: as many as the longest search of the previous
     // cycle took; a search that needs more continues in the next cycle (its group skips
     // assembly and solve until it has finished)
     SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
-    for (int r = 0; r < b->cur_rounds; r++) {
-      b->rounds++;
-      b->eval_timed(kTrial);
-    }
+    for (int r = 0; r < b->cur_rounds; r++) b->eval_timed(kTrial);
     b->eval_timed(kCorr);  // correlation sums after the second half-step
   } else {
-    b->rounds++;
     b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
   }
   SS_CK(cudaGetLastError());
@@ -1037,11 +1050,164 @@ static int launch_cycle(Batch::Impl* b) {
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
   b->eval_timed(kFinal);
   k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
-  b->launches += 3;
   SS_CK(cudaGetLastError());
   SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  return SS_OK;
+}
+
+// Launches one cycle and records the cycle event. No host synchronisation.
+static int launch_cycle(Batch::Impl* b) {
+  b->cycles++;
+  b->rounds += b->ks.round ? b->cur_rounds : 1;
+  b->launches += b->ks.round ? b->cur_rounds + 7 : 7;
+  int rc = enqueue_cycle(b);
+  if (rc) return rc;
   if (!b->ev_cycle) SS_CK(cudaEventCreateWithFlags(&b->ev_cycle, cudaEventDisableTiming));
-  SS_CK(cudaEventRecord(b->ev_cycle, s));
+  SS_CK(cudaEventRecord(b->ev_cycle, b->stream));
+  return SS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The whole run as one CUDA graph: a WHILE node over cycles whose body is the cycle, and inside it
+// (precision 'S') a WHILE node over trial rounds. One-thread control kernels set both conditions
+// from the groups' state on the device, so the run needs no host round trip until every group has
+// stopped. Both loops are bounded by counters (cycles by the batch's cycle bound, rounds per cycle
+// by kGraphRounds, after which a search continues in the next cycle).
+
+constexpr int kGraphRounds = 64;
+
+// Condition of the trial-round loop: another round while a line search is open and the cycle is
+// under its round bound. `first` starts the cycle's round count.
+__global__ void __launch_bounds__(256) k_rounds_ctl(const GroupCtl* __restrict__ ctl, int n_groups,
+                                                    int* __restrict__ ctr, int first,
+                                                    cudaGraphConditionalHandle h) {
+  int open = 0;
+  for (int g = threadIdx.x; g < n_groups; g += blockDim.x)
+    open |= (ctl[g].ls_state == 1 && ctl[g].ls_pending > 0) ? 1 : 0;
+  open = __syncthreads_or(open);
+  if (threadIdx.x == 0) {
+    if (first) ctr[kCtrRound] = 0;
+    const bool more = open && ctr[kCtrRound] < kGraphRounds;
+    if (more) {
+      ctr[kCtrRound]++;
+      ctr[kCtrRounds]++;
+    } else if (open) {
+      ctr[kCtrBound] |= 2;
+    }
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+  }
+}
+
+// Condition of the cycle loop: another cycle while a group is running, up to `max_cycles`.
+__global__ void k_cycle_ctl(int* __restrict__ ctr, int n_groups, int max_cycles, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  const int c = ++ctr[kCtrCycles];
+  const bool running = ctr[kCtrDone] < n_groups;
+  if (running && c >= max_cycles) ctr[kCtrBound] |= 1;
+  cudaGraphSetConditional(h, running && c < max_cycles ? 1u : 0u);
+}
+
+// Adds a WHILE node after the work captured so far on `s` and makes it the capture's dependency;
+// returns its body graph.
+static int capture_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t n_deps = 0;
+  SS_CK(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &n_deps));
+  if (st != cudaStreamCaptureStatusActive) return fail(SS_ERR_CUDA, "run graph: stream is not capturing");
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  SS_CK(cudaGraphAddNode(&node, g, deps, n_deps, &p));
+  *body = p.conditional.phGraph_out[0];
+  SS_CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return SS_OK;
+}
+
+// Opts every kernel of the run into its shared memory before capture (no attribute calls inside).
+static int prime_attributes(Batch::Impl* b) {
+  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
+  SS_CK(b->ks.eval(kAssemble, 0, b->stream, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes));
+  if (b->ks.round) SS_CK(b->ks.round(0, b->stream, b->d_gd, b->d_tile_group, b->d_ctl, b->win_bytes));
+  else SS_CK(b->ks.ls(0, b->stream, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes));
+  return SS_OK;
+}
+
+static int build_run_graph(Batch::Impl* b) {
+  int rc = prime_attributes(b);
+  if (rc) return rc;
+  if (!b->cap_stream) SS_CK(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+  cudaStream_t s = b->cap_stream;
+  const int nG = (int)b->gd.size();
+  // two half-steps per iteration, a line search of up to kTrialCap trials each
+  int max_iter = 1;
+  for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
+  const int max_cycles = 4 * (max_iter + 2) * (1 + kTrialCap / kGraphRounds) + 16;
+  cudaGraph_t top = nullptr, body = nullptr, rounds_body = nullptr;
+  SS_CK(cudaGraphCreate(&top, 0));
+  struct GraphGuard {
+    cudaGraph_t g;
+    ~GraphGuard() { cudaGraphDestroy(g); }
+  } guard{top};
+  cudaGraphConditionalHandle h_cycle = 0, h_round = 0;
+  SS_CK(cudaGraphConditionalHandleCreate(&h_cycle, top, 1, cudaGraphCondAssignDefault));
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  // top: counters, the cycle loop, the counters to the host
+  SS_CK(cudaStreamBeginCaptureToGraph(s, top, nullptr, nullptr, 0, mode));
+  cudaMemsetAsync(b->d_counters + kCtrCycles, 0, (kCtrBound - kCtrCycles + 1) * sizeof(int), s);
+  rc = capture_while(s, h_cycle, &body);
+  cudaMemcpyAsync(b->h_counters, b->d_counters, kCounters * sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaGraph_t out = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("run graph: ") + cudaGetErrorString(e));
+  // one cycle
+  if (b->ks.round) SS_CK(cudaGraphConditionalHandleCreate(&h_round, body, 0, 0));
+  SS_CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, mode));
+  b->ks.eval(kAssemble, b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes);
+  k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
+  if (b->ks.round) {
+    k_rounds_ctl<<<1, 256, 0, s>>>(b->d_ctl, nG, b->d_counters, 1, h_round);
+    rc = capture_while(s, h_round, &rounds_body);
+    if (!rc) b->ks.eval(kCorr, b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes);
+  } else {
+    b->ks.ls(b->n_frames_total, s, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes);
+  }
+  k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+  k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+  b->ks.eval(kFinal, b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes);
+  k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + kCtrDone);
+  k_cycle_ctl<<<1, 32, 0, s>>>(b->d_counters, nG, max_cycles, h_cycle);
+  e = cudaStreamEndCapture(s, &out);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("run graph cycle: ") + cudaGetErrorString(e));
+  // one trial round
+  if (b->ks.round) {
+    SS_CK(cudaStreamBeginCaptureToGraph(s, rounds_body, nullptr, nullptr, 0, mode));
+    b->ks.round(b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->win_bytes);
+    k_rounds_ctl<<<1, 256, 0, s>>>(b->d_ctl, nG, b->d_counters, 0, h_round);
+    e = cudaStreamEndCapture(s, &out);
+    if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("run graph rounds: ") + cudaGetErrorString(e));
+  }
+  SS_CK(cudaGetLastError());
+  SS_CK(cudaGraphInstantiate(&b->run_exec, top, 0));
+  return SS_OK;
+}
+
+// Launches the whole run as the graph and records the cycle event.
+static int launch_run_graph(Batch::Impl* b) {
+  if (!b->run_exec) {
+    int rc = build_run_graph(b);
+    if (rc) return rc;
+  }
+  SS_CK(cudaGraphLaunch(b->run_exec, b->stream));
+  if (!b->ev_cycle) SS_CK(cudaEventCreateWithFlags(&b->ev_cycle, cudaEventDisableTiming));
+  SS_CK(cudaEventRecord(b->ev_cycle, b->stream));
+  b->graph_run = true;
   return SS_OK;
 }
 
@@ -1049,7 +1215,7 @@ int Batch::start() {
   Impl* b = d;
   b->t_start = std::chrono::steady_clock::now();
   SS_CK(cudaSetDevice(b->device));
-  if (!b->h_counters) SS_CK(cudaHostAlloc(&b->h_counters, 4 * sizeof(int), cudaHostAllocDefault));
+  if (!b->h_counters) SS_CK(cudaHostAlloc(&b->h_counters, (kCounters + 1) * sizeof(int), cudaHostAllocDefault));
   SS_CK(smem_attr(k_solve, (int)kSolveSmem));
   int rc = reset_state(b);
   if (rc) return rc;
@@ -1059,6 +1225,7 @@ int Batch::start() {
   b->event_used = 0;
   b->cur_rounds = kFirstRounds;
   b->cycle_no = 0;
+  b->graph_run = false;
   b->state = 1;
   int max_iter = 1;
   for (auto& g : b->hg) max_iter = std::max(max_iter, g.in->max_iter);
@@ -1071,7 +1238,7 @@ int Batch::step() {
   Impl* b = d;
   if (b->state != 1) return fail(SS_ERR_INVALID_ARGUMENT, "batch: step() needs start() and a finished cycle");
   SS_CK(cudaSetDevice(b->device));
-  int rc = launch_cycle(b);
+  int rc = b->use_graph && !b->timing ? launch_run_graph(b) : launch_cycle(b);
   if (rc) return rc;
   b->state = 2;
   return SS_OK;
@@ -1081,10 +1248,10 @@ int Batch::step() {
 static int finish_run(Batch::Impl* b) {
   SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost,
                         b->stream));
-  SS_CK(cudaMemcpyAsync(b->h_counters + 2, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  SS_CK(cudaMemcpyAsync(b->h_counters + kCounters, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   SS_CK(cudaMemcpyAsync(b->h_staging, b->d_staging, sizeof(b->h_staging), cudaMemcpyDeviceToHost, b->stream));
   SS_CK(cudaStreamSynchronize(b->stream));
-  if (b->h_counters[2] & 1) return fail(SS_ERR_CUDA, "a shared-memory staging copy did not complete in time");
+  if (b->h_counters[kCounters] & 1) return fail(SS_ERR_CUDA, "a shared-memory staging copy did not complete in time");
   for (int m = 0; m < 4; m++) b->eval_ms[m] = 0;
   for (size_t k = 0; k < b->event_used; k += 2) {
     float ms = 0;
@@ -1102,6 +1269,20 @@ int Batch::poll() {
   cudaError_t q = cudaEventQuery(b->ev_cycle);
   if (q == cudaErrorNotReady) return 0;
   if (q != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cycle: ") + cudaGetErrorString(q));
+  if (b->graph_run) {
+    const int* c = b->h_counters;
+    b->graph_run = false;
+    b->cycles = c[kCtrCycles];
+    b->rounds = b->ks.round ? c[kCtrRounds] : c[kCtrCycles];
+    // per cycle: assembly, solve, after-ls, iteration end, final pass, final, cycle control, and
+    // the line search (precision 'D') or the round control and correlation (precision 'S'); two
+    // launches per trial round
+    b->launches = b->ks.round ? 9 * c[kCtrCycles] + 2 * c[kCtrRounds] : 8 * c[kCtrCycles];
+    if (c[kCtrBound] & 1) return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
+    b->state = 3;
+    int rc = finish_run(b);
+    return rc ? rc : 2;
+  }
   if (b->h_counters[1] >= (int)b->gd.size()) {
     b->state = 3;
     int rc = finish_run(b);
@@ -1137,6 +1318,7 @@ int Batch::reset() {
 }
 
 void Batch::set_timing(bool on) { d->timing = on; }
+void Batch::set_graph(bool on) { d->use_graph = on; }
 
 void Batch::stats(ss_batch_stats* st) const {
   std::memset(st, 0, sizeof(*st));
@@ -1647,6 +1829,12 @@ int ss_batch_collect(ss_batch* batch) {
 int ss_batch_set_timing(ss_batch* batch, int32_t on) {
   if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
   batch->b.set_timing(on != 0);
+  return SS_OK;
+}
+
+int ss_batch_set_graph(ss_batch* batch, int32_t on) {
+  if (!batch) return ss::fail(SS_ERR_INVALID_ARGUMENT, "batch is NULL");
+  batch->b.set_graph(on != 0);
   return SS_OK;
 }
 

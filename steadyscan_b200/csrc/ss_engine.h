@@ -44,6 +44,7 @@ class Batch {
   int collect();
 
   void set_timing(bool on);
+  void set_graph(bool on);
   void stats(ss_batch_stats* st) const;
   size_t arena_bytes() const;
   int cycles() const;

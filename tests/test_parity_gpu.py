@@ -208,3 +208,32 @@ def test_fp16_template_storage_matches_fp64_on_the_rounded_template():
     s["flags"] = "S"
     g = api.align_group(s, template_storage="f16")
     assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([ref["dx"], ref["dy"]])) <= KNOT_RMS_S
+
+
+@pytest.mark.parametrize("flags", ["D", "S"])
+def test_graph_run_equals_host_launched_cycles(flags):
+    """The run as one CUDA graph (device-side loops over cycles and trial rounds) gives every group
+    of a ragged batch the result of host-launched cycles, bit for bit."""
+    specs = [dict(seed=81, frame_dtype=np.uint16), dict(n_frames=3, seed=82, frame_dtype=np.uint16),
+             dict(nlines=24, linewidth=20, nknots=7, seed=83, frame_dtype=np.uint16),
+             dict(nlines=64, linewidth=64, nknots=33, n_frames=9, seed=84, n_blobs=30, frame_dtype=np.uint16)]
+    groups = []
+    for s in specs:
+        a = make_args(**s)[0]
+        a["flags"] = flags
+        groups.append(a)
+    res = []
+    for graph in (True, False):
+        b = api.Batch(groups, want_mask=True)
+        b.set_graph(graph)
+        b.run()
+        res.append((b.collect(), b.stats()))
+    (rg, sg), (rh, sh) = res
+    for a, b in zip(rg, rh):
+        assert a["iter_used"] == b["iter_used"]
+        np.testing.assert_array_equal(a["dx"], b["dx"])
+        np.testing.assert_array_equal(a["dy"], b["dy"])
+        np.testing.assert_array_equal(a["mask"], b["mask"])
+        np.testing.assert_array_equal(a["residrms"], b["residrms"])
+    assert sg["cycles"] > 0 and sg["kernel_launches"] > 0
+    assert sg["cycles"] <= sh["cycles"]
