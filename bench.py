@@ -49,6 +49,13 @@ def parse():
     ap.add_argument("--plain-groups", type=int, default=2)
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="seconds of generated serving load (8 sessions, 0 to skip)")
+    ap.add_argument("--ragged-groups", type=int, default=0, help="groups of the ragged batch (0: 96)")
+    ap.add_argument("--ragged-single", type=int, default=16,
+                    help="groups of the ragged batch also run one batch per group")
+    ap.add_argument("--no-ragged", action="store_true", help="skip the ragged batch with the autotuner")
+    ap.add_argument("--only-ragged", action="store_true", help="run and print only the ragged batch")
+    ap.add_argument("--ragged-lean", action="store_true",
+                    help="ragged batch at the default schedule only (no tuner, no comparison runs)")
     ap.add_argument("--serve-warm", action="store_true",
                     help="start each session's groups from its last displacement instead of zero")
     return ap.parse_args()
@@ -56,6 +63,42 @@ def parse():
 
 # ------------------------------------------------------------------------------------------------
 # workload
+
+def to_block_columns(img, k):
+    """A frame (lines x pixels tensor) as a flat block matrix of the default scan geometry: block
+    column cc holds lines cc*k .. cc*k+k-1, MATLAB column-major inside the block."""
+    nlines, linewidth = img.shape
+    return img.view(nlines // k, k, linewidth).permute(0, 2, 1).contiguous().view(-1)
+
+
+def render_block_frames(tmpl, walk, n_frames, nlines, linewidth, k, gen, device):
+    """uint16 frames (Poisson counts of the template sampled along ``walk``, one row per scan line),
+    each as a flat block matrix: block column cc holds lines cc*k .. cc*k+k-1, MATLAB column-major
+    inside the block."""
+    import torch
+    T = tmpl if isinstance(tmpl, torch.Tensor) else torch.tensor(tmpl, device=device)
+    th, tw = T.shape
+    jj = torch.arange(linewidth, device=device, dtype=torch.float64)[None, :]
+    ll = torch.arange(nlines, device=device, dtype=torch.float64)[:, None]
+    wl_all = walk if isinstance(walk, torch.Tensor) else torch.tensor(walk, device=device)
+    bg = float(T.min())
+    out = []
+    for f in range(n_frames):
+        wl = wl_all[f * nlines:(f + 1) * nlines]
+        x = jj + wl[:, 0:1]
+        y = ll + wl[:, 1:2]
+        x0 = torch.floor(x)
+        y0 = torch.floor(y)
+        fx, fy = x - x0, y - y0
+        x0l, y0l = x0.long(), y0.long()
+        inside = (x0l >= 0) & (y0l >= 0) & (x0l < tw - 1) & (y0l < th - 1)
+        xc, yc = x0l.clamp(0, tw - 2), y0l.clamp(0, th - 2)
+        v = (1 - fx) * ((1 - fy) * T[yc, xc] + fy * T[yc + 1, xc]) + fx * ((1 - fy) * T[yc, xc + 1] + fy * T[yc + 1, xc + 1])
+        lam = torch.where(inside, v, torch.full_like(v, bg))
+        cnt = torch.poisson(lam, generator=gen).clamp(0, 65535).to(torch.int32).to(torch.uint16)
+        out.append(to_block_columns(cnt, k))
+    return out
+
 
 def make_workload(n_frames, size, group, precision, seed, device):
     """Returns (groups: list of host argument dicts, device frame tensors per group, settings)."""
@@ -69,29 +112,9 @@ def make_workload(n_frames, size, group, precision, seed, device):
     s = prep.init_settings({"nknots": nk, "gpu_forced_precision": precision, "lambda": 5e-3}, tmpl, size, size)
     lay = prep.block_layout(s)
     k = size // (nk - 1)
-    T = torch.tensor(tmpl, device=device)
     gen = torch.Generator(device=device)
     gen.manual_seed(seed)
-    jj = torch.arange(size, device=device, dtype=torch.float64)[None, :]
-    ll = torch.arange(size, device=device, dtype=torch.float64)[:, None]
-    wl_all = torch.tensor(walk, device=device)
-    bg = float(tmpl.min())
-    frames_bm = []
-    for f in range(n_frames):
-        wl = wl_all[f * size:(f + 1) * size]
-        x = jj + wl[:, 0:1]
-        y = ll + wl[:, 1:2]
-        x0 = torch.floor(x)
-        y0 = torch.floor(y)
-        fx, fy = x - x0, y - y0
-        x0l, y0l = x0.long(), y0.long()
-        inside = (x0l >= 0) & (y0l >= 0) & (x0l < size - 1) & (y0l < size - 1)
-        xc, yc = x0l.clamp(0, size - 2), y0l.clamp(0, size - 2)
-        v = (1 - fx) * ((1 - fy) * T[yc, xc] + fy * T[yc + 1, xc]) + fx * ((1 - fy) * T[yc, xc + 1] + fy * T[yc + 1, xc + 1])
-        lam = torch.where(inside, v, torch.full_like(v, bg))
-        cnt = torch.poisson(lam, generator=gen).clamp(0, 65535).to(torch.int32).to(torch.uint16)
-        # block-matrix column cc holds lines cc*k .. cc*k+k-1, MATLAB column-major inside the block
-        frames_bm.append(cnt.view(nk - 1, k, size).permute(0, 2, 1).contiguous().view(-1))
+    frames_bm = render_block_frames(tmpl, walk, n_frames, size, size, k, gen, device)
     groups, dev = [], []
     grads = prep.template_gradients(tmpl)
     for g0 in range(0, n_frames, group):
@@ -102,6 +125,184 @@ def make_workload(n_frames, size, group, precision, seed, device):
         args = prep.boundary_arguments(s, tmpl, host, nF, layout=lay, gradients=grads)
         groups.append(args)
     return groups, dev, s, lay
+
+
+RAGGED_SETTINGS = {"lambda": 1e-2, "move_thresh": 1e-3, "max_iter": 30}
+
+
+def make_ragged_workload(precision, seed, device, n_groups=None, walks=None):
+    """Ragged batch: groups of U[1,128] frames, each of a frame size drawn from 128x128, 256x512,
+    512x512 and 796x512 (lines x pixels) and a knot spacing from {1, 2, 4} lines; one template per
+    frame size (80 blobs per 256x256 of area, sigma 2-5 px, 200-photon peak); per-line random walk
+    N(0, 0.15 px) clipped to +-6 px with one jump of up to 4 px per frame; Poisson noise; lambda
+    1e-2, move threshold 1e-3 px, at most 30 iterations. Returns (host argument dicts, device frame
+    tensors, per-group (lines, pixels, lines per knot, frames)); a list ``walks`` receives each
+    group's per-line displacement (the ground truth)."""
+    import torch
+
+    from steadyscan_b200 import prep, synth
+    sp = synth.WORKLOADS[3]
+    rng = np.random.default_rng(seed)
+    n_groups = n_groups or sp["n_groups"]
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    tmpls, setts = {}, {}
+    groups, dev, meta = [], [], []
+    for _ in range(n_groups):
+        h, w = sp["sizes"][int(rng.integers(len(sp["sizes"])))]
+        k = sp["lines_per_knot"][int(rng.integers(len(sp["lines_per_knot"])))]
+        nf = int(rng.integers(sp["group_len"][0], sp["group_len"][1] + 1))
+        if (h, w) not in tmpls:
+            t = synth.make_template(h, w, max(1, round(80 * h * w / (256 * 256))), (2.0, 5.0), rng)
+            tmpls[(h, w)] = (t, prep.template_gradients(t), torch.tensor(t, device=device))
+        tmpl, grads, tdev = tmpls[(h, w)]
+        if (h, w, k) not in setts:
+            s = prep.init_settings(dict(RAGGED_SETTINGS, nknots=h // k + 1, gpu_forced_precision=precision), tmpl, h, w)
+            setts[(h, w, k)] = (s, prep.block_layout(s))
+        s, lay = setts[(h, w, k)]
+        walk = synth.make_walk(h * (nf + 1), sp["walk_sigma"], sp["clip_px"], sp["jumps_per_frame"], h,
+                               sp["jump_px"], rng)
+        if walks is not None:
+            walks.append(walk)
+        flat = torch.cat(render_block_frames(tdev, walk, nf, h, w, k, gen, device))
+        host = flat.cpu().numpy().reshape(lay.frame_h, lay.frame_w * nf, order="F")
+        groups.append(prep.boundary_arguments(s, tmpl, host, nf, layout=lay, gradients=grads))
+        dev.append((flat, lay))
+        meta.append((h, w, k, nf))
+    return groups, dev, meta
+
+
+def device_groups(groups, dev):
+    """Argument dicts whose frames are the device tensors (uint16 block matrices)."""
+    from steadyscan_b200 import api
+    from steadyscan_b200._lib import SS_U16
+    out = []
+    for g, (t, lay) in zip(groups, dev):
+        d = dict(g)
+        d["bmData"] = api.DeviceMatrix(t.data_ptr(), lay.frame_h, lay.frame_w * int(g["nFrames"]), SS_U16, owner=t)
+        out.append(d)
+    return out
+
+
+def timed_batch(groups, device, steps, warmup=1, graph=True, template_storage=None):
+    """Device ms per run of one batch (CUDA events on the engine's stream), its stats and results."""
+    import torch
+
+    from steadyscan_b200 import api
+    b = api.Batch(groups, template_storage=template_storage)
+    b.set_graph(graph)
+    stream = torch.cuda.ExternalStream(b.stream_ptr, device=device)
+    for _ in range(warmup):
+        b.run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    for _ in range(steps):
+        b.run()
+        launches += b.stats()["kernel_launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = b.stats()
+    res = b.collect()
+    b.close()
+    return ms, st, res, launches
+
+
+def ragged(args, device):
+    """The ragged batch with the autotuned tile schedule, as one graph launch per run, next to the
+    default schedule, host-launched cycles, one batch per group, and the FP64 path."""
+    from steadyscan_b200 import synth
+    from steadyscan_b200.autotune import Autotuner
+    walks = []
+    groups, dev, meta = make_ragged_workload("S", 1003, device, args.ragged_groups or None, walks=walks)
+    dg = device_groups(groups, dev)
+    frames = sum(m[3] for m in meta)
+    steps = max(1, args.steps)
+    if args.ragged_lean:
+        ms, st, res, launches = timed_batch(dg, device, steps, warmup=args.warmup)
+        iters = np.array([r["iter_used"] for r in res])
+        return {"frames": frames, "groups": len(meta), "value": frames / (ms / 1e3), "unit": "frames/s",
+                "ms_per_run": ms, "kernel_launches_per_run": launches // steps, "cycles": st["cycles"],
+                "linesearch_rounds": st["linesearch_rounds"],
+                "iterations": {"min": int(iters.min()), "max": int(iters.max()), "mean": float(iters.mean())}}
+    tuner = Autotuner(candidates=(8, 16, 32, 64), reps=2)
+    t0 = time.perf_counter()
+    tuned = tuner.apply(dg)
+    tune_s = time.perf_counter() - t0
+    ms_t, st_t, res_t, launches = timed_batch(tuned, device, steps)
+    ms_d, st_d, res_d, _ = timed_batch(dg, device, steps)
+    ms_h, st_h, res_h, _ = timed_batch(tuned, device, steps, graph=False)
+    # graph and host-launched cycles agree bit for bit; tile schedules at FP32 rounding level
+    same = all(np.array_equal(a["dx"], b["dx"]) and np.array_equal(a["dy"], b["dy"]) for a, b in zip(res_t, res_h))
+    sched_diff = max(float(np.max(np.abs(np.concatenate([a["dx"] - b["dx"], a["dy"] - b["dy"]]))))
+                     for a, b in zip(res_t, res_d))
+    # one batch per group, serially (a sample of the groups)
+    n1 = min(len(tuned), args.ragged_single)
+    ms1, fr1 = 0.0, 0
+    for g in tuned[:n1]:
+        ms, _, _, _ = timed_batch([g], device, 1)
+        ms1 += ms
+        fr1 += int(g["nFrames"])
+    # FP64 reference: precision D on the same frames (the D path agrees with the FP64 oracle to 1e-6 px)
+    dgd = [dict(g, flags="D") for g in dg]
+    ms_64, _, res_64, _ = timed_batch(dgd, device, 1, warmup=0)
+    # error of precision S against FP64 per frame size: over all knots, and over the knots where the
+    # FP64 solution is within 0.5 px of the true displacement (elsewhere the problem is ill-posed,
+    # e.g. knots every line on lines without template structure, and FP64 itself runs away from the
+    # truth, so tiny rounding differences grow); knots within 0.5 px of the truth for both precisions
+    acc = {}
+    for (h, w, k, nf), wk, a, o in zip(meta, walks, res_t, res_64):
+        nk = h // k + 1
+        tx, ty = synth.truth_knots(wk, h, nk, nf)
+        sx, sy = np.asarray(a["dx"]).reshape(nf, nk).T, np.asarray(a["dy"]).reshape(nf, nk).T
+        ox, oy = np.asarray(o["dx"]).reshape(nf, nk).T, np.asarray(o["dy"]).reshape(nf, nk).T
+        e = np.concatenate([(sx - ox).ravel(), (sy - oy).ravel()])
+        e = e[np.isfinite(e)]
+        # the last knot of a frame repeats the one before it (an output convention), not a time point
+        inner = np.zeros_like(tx, dtype=bool)
+        inner[:-1] = True
+        ok64 = inner & (np.abs(ox - tx) <= 0.5) & (np.abs(oy - ty) <= 0.5)
+        okS = inner & (np.abs(sx - tx) <= 0.5) & (np.abs(sy - ty) <= 0.5)
+        ec = np.concatenate([(sx - ox)[ok64], (sy - oy)[ok64]])
+        cur = acc.setdefault(f"{h}x{w}", {"se": 0.0, "n": 0, "max": 0.0, "se_c": 0.0, "n_c": 0, "max_c": 0.0,
+                                          "knots": 0, "ok64": 0, "okS": 0})
+        cur["se"] += float(np.sum(e * e))
+        cur["n"] += e.size
+        cur["max"] = max(cur["max"], float(np.max(np.abs(e))))
+        cur["se_c"] += float(np.sum(ec * ec))
+        cur["n_c"] += ec.size
+        cur["max_c"] = max(cur["max_c"], float(np.max(np.abs(ec))) if ec.size else 0.0)
+        cur["knots"] += int(inner.sum())
+        cur["ok64"] += int(ok64.sum())
+        cur["okS"] += int(okS.sum())
+    err = {k: {"rms_px": float(np.sqrt(v["se"] / v["n"])), "max_px": v["max"],
+               "rms_px_where_fp64_within_0.5px_of_truth": float(np.sqrt(v["se_c"] / max(1, v["n_c"]))),
+               "max_px_where_fp64_within_0.5px_of_truth": v["max_c"],
+               "knots_within_0.5px_of_truth": {"fp64": v["ok64"] / v["knots"], "S": v["okS"] / v["knots"]}}
+           for k, v in acc.items()}
+    iters = np.array([r["iter_used"] for r in res_t])
+    choices = {k: v for k, v in tuner.choices.items()}
+    timings = {k: {str(c): round(1e3 * t, 3) for c, t in v.items()} for k, v in tuner.timings.items()}
+    return {"workload": f"{len(meta)} groups, U[1,128] frames of 128x128 / 256x512 / 512x512 / 796x512 "
+                        "uint16, knots every 1, 2 or 4 lines, precision S, lambda 1e-2, move threshold 1e-3 px, "
+                        "at most 30 iterations",
+            "frames": frames, "groups": len(meta),
+            "frames_by_size": {k: int(sum(m[3] for m in meta if f"{m[0]}x{m[1]}" == k))
+                               for k in sorted({f"{m[0]}x{m[1]}" for m in meta})},
+            "value": frames / (ms_t / 1e3), "unit": "frames/s", "ms_per_run": ms_t,
+            "graph_launches_per_run": 1, "kernel_launches_per_run": launches // steps,
+            "cycles": st_t["cycles"], "linesearch_rounds": st_t["linesearch_rounds"],
+            "iterations": {"min": int(iters.min()), "max": int(iters.max()), "mean": float(iters.mean())},
+            "default_schedule": {"value": frames / (ms_d / 1e3), "ms_per_run": ms_d},
+            "host_launched_cycles": {"value": frames / (ms_h / 1e3), "ms_per_run": ms_h, "cycles": st_h["cycles"]},
+            "one_batch_per_group": {"value": fr1 / (ms1 / 1e3), "groups": n1, "frames": fr1},
+            "graph_equals_host_cycles": bool(same), "max_px_diff_tuned_vs_default_schedule": sched_diff,
+            "autotune": {"seconds": tune_s, "choices": choices, "median_ms": timings},
+            "fp64_path": {"value": frames / (ms_64 / 1e3), "ms_per_run": ms_64},
+            "error_vs_fp64": err}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -345,6 +546,11 @@ def main():
     from steadyscan_b200 import api
     from steadyscan_b200._lib import SS_U16
 
+    if args.only_ragged:
+        if rank == 0:
+            print(json.dumps({"ragged": ragged(args, device)}))
+        return
+
     groups, dev_frames, settings, lay = make_workload(args.frames, args.size, args.group, args.precision,
                                                       1002 + 17 * rank, device)
     torch.cuda.synchronize()
@@ -473,6 +679,10 @@ def main():
         if e2e:
             plain["e2e_vs_plain_D"] = e2e["value"] / plain["D"]["value"]
 
+    ragged_line = None
+    if rank == 0 and not args.no_ragged:
+        ragged_line = ragged(args, device)
+
     serving_line = None
     if rank == 0 and args.serve_seconds > 0:
         batch.close()
@@ -485,7 +695,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32" if args.precision == "S" else "f64", "data": "synthetic",
                 "config": workload_config(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc, "plain_gpu": plain,
-                "serving": serving_line,
+                "ragged": ragged_line, "serving": serving_line,
                 "run": {"cycles": st["cycles"], "linesearch_rounds": st["linesearch_rounds"],
                         "iterations_min": int(min(iters)), "iterations_max": int(max(iters)),
                         "arena_bytes": st["arena_bytes"]}}

@@ -67,11 +67,11 @@ struct GroupDesc {
   // geometry (mexgateway.cpp:176-198)
   int Hb, W, nF, fW, N, Ht, Wt;
   int group_size, n_rg;
-  int tile_base;    // first k_eval tile of this group
+  int chunk_base;   // first frame chunk of this group in the batch's chunk table
   int frame_base;   // first global frame index of this group
   // settings
   int max_iter, solver_id, max_filter_iter, filter_id, flags, frac_uniform;
-  int frames_per_cta;       // assembly/final CTA frames (a tuning choice): eval tiles = W * ceil(nF / it)
+  int frames_per_cta;       // frames of an evaluation tile (a tuning choice): W * ceil(nF / it) tiles
   double move_thresh, halt_corr, corr_inc_thr, filter_strength, filter_corr_thr, lambda, ls_mult;
   // inputs on the device
   const double* frac;       // Hb x W column-major

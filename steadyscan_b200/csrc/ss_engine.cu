@@ -10,6 +10,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <mutex>
 #include <set>
 #include <string>
@@ -150,31 +152,56 @@ constexpr int kWinBytes = 72 * 1024;
 // with the kernel's static shared memory one 1024-thread CTA per SM).
 constexpr int kLsWinBytes = 196 * 1024;
 
-using EvalFn = cudaError_t (*)(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
+// Grid of an evaluation launch: the CTAs of `fn` resident on the device at once with `smem` bytes,
+// at most the batch's tiles (the CTAs take tiles from the launch's schedule until it is exhausted).
+template <class F>
+static int resident_grid(F* fn, int threads, size_t smem, int max_tiles) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, size_t>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return std::max(1, std::min(max_tiles, 148));
+  const auto key = std::make_tuple(dev, reinterpret_cast<const void*>(fn), smem);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it == cache.end()) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) per_sm = 1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+    it = cache.emplace(key, std::max(1, per_sm) * std::max(1, sms)).first;
+  }
+  return std::max(1, std::min(max_tiles, it->second));
+}
+
+using EvalFn = cudaError_t (*)(int mode, int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
                                const GroupCtl* ctl, int max_hb, int win_bytes);
 using LsFn = cudaError_t (*)(int frames, cudaStream_t s, const GroupDesc* gd, const int* fg, GroupCtl* ctl,
                              int win_bytes);
 using SumFn = void (*)(const void* img, size_t n, double* parts, double* out, cudaStream_t s);
 
 template <class Acc, class FrameT, class TplT>
-static cudaError_t eval_launch(int mode, int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg,
+static cudaError_t eval_launch(int mode, int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
                                const GroupCtl* ctl, int max_hb, int win_bytes) {
   constexpr int kMaxDyn = kStageBytes + kWinBytes + 64;
   cudaError_t ae = smem_attr(k_eval<Acc, FrameT, TplT, kAssemble>, kMaxDyn);
   if (ae == cudaSuccess) ae = smem_attr(k_eval<Acc, FrameT, TplT, kFinal>, kMaxDyn);
   if (ae == cudaSuccess) ae = smem_attr(k_eval<Acc, FrameT, TplT, kCorr>, kMaxDyn);
-  if (ae != cudaSuccess || tiles <= 0) return ae;
+  if (ae != cudaSuccess) return ae;
   const int rows = stage_bytes<Acc>(max_hb) <= (size_t)kStageBytes ? max_hb : 0;
   if (sizeof(Acc) != 4) win_bytes = 0;
   win_bytes = std::min(win_bytes, kWinBytes) & ~15;
-  // geometry staging (16-byte multiple), then the template window and its mbarrier
-  const size_t smem = (rows ? stage_bytes<Acc>(rows) : 0) + (win_bytes ? (size_t)win_bytes + 16 : 0) + 64;
-  if (mode == kAssemble)
-    k_eval<Acc, FrameT, TplT, kAssemble><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
-  else if (mode == kCorr)
-    k_eval<Acc, FrameT, TplT, kCorr><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
-  else
-    k_eval<Acc, FrameT, TplT, kFinal><<<tiles, 32 * kEvalWarps, smem, s>>>(gd, tg, ctl, rows, win_bytes);
+  // the window's mbarrier, geometry staging (16-byte multiple), then the template window
+  const size_t smem = 16 + (rows ? stage_bytes<Acc>(rows) : 0) + (size_t)win_bytes;
+  const int th = 32 * kEvalWarps;
+  auto* fa = k_eval<Acc, FrameT, TplT, kAssemble>;
+  auto* fc = k_eval<Acc, FrameT, TplT, kCorr>;
+  auto* ff = k_eval<Acc, FrameT, TplT, kFinal>;
+  // grids first (the occupancy queries are cached: none runs while a graph is captured)
+  const int ga = resident_grid(fa, th, smem, max_tiles), gc = resident_grid(fc, th, smem, max_tiles),
+            gf = resident_grid(ff, th, smem, max_tiles);
+  if (max_tiles <= 0) return cudaSuccess;
+  if (mode == kAssemble) fa<<<ga, th, smem, s>>>(gd, sched, cap, ctl, rows, win_bytes);
+  else if (mode == kCorr) fc<<<gc, th, smem, s>>>(gd, sched, cap, ctl, rows, win_bytes);
+  else ff<<<gf, th, smem, s>>>(gd, sched, cap, ctl, rows, win_bytes);
   return cudaGetLastError();
 }
 
@@ -203,18 +230,32 @@ static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, co
   return cudaLaunchKernelEx(&cfg, k_linesearch<Acc, FrameT, TplT>, gd, fg, ctl, win_bytes);
 }
 
-using RoundFn = cudaError_t (*)(int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, GroupCtl* ctl,
-                                int win_bytes);
+using RoundFn = cudaError_t (*)(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
+                                GroupCtl* ctl, int win_bytes);
 
-// One line-search trial round of precision 'S' over the assembly tiles.
+// One line-search trial round of precision 'S' over the tiles of the round's schedule.
 template <class FrameT, class TplT>
-static cudaError_t round_launch(int tiles, cudaStream_t s, const GroupDesc* gd, const int* tg, GroupCtl* ctl,
-                                int win_bytes) {
-  cudaError_t ae = smem_attr(k_trial_round<FrameT, TplT>, kWinBytes + 16);
-  if (ae != cudaSuccess || tiles <= 0) return ae;
+static cudaError_t round_launch(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
+                                GroupCtl* ctl, int win_bytes) {
+  auto* fn = k_trial_round<FrameT, TplT>;
+  cudaError_t ae = smem_attr(fn, kWinBytes + 16);
+  if (ae != cudaSuccess) return ae;
   win_bytes = std::min(win_bytes, kWinBytes) & ~15;
-  k_trial_round<FrameT, TplT><<<tiles, 32 * kEvalWarps, win_bytes ? (size_t)win_bytes + 16 : 0, s>>>(gd, tg, ctl,
-                                                                                                      win_bytes);
+  const size_t smem = 16 + (size_t)win_bytes;
+  const int th = 32 * kEvalWarps;
+  const int grid = resident_grid(fn, th, smem, max_tiles);  // cached before any capture
+  if (max_tiles <= 0) return cudaSuccess;
+  fn<<<grid, th, smem, s>>>(gd, sched, cap, ctl, win_bytes);
+  return cudaGetLastError();
+}
+
+// The schedule of an evaluation launch of `mode` (one CTA).
+static cudaError_t sched_launch(int mode, cudaStream_t s, const GroupDesc* gd, const GroupCtl* ctl,
+                                const int* chunk_group, int n_chunks, int* sched) {
+  if (mode == kAssemble) k_schedule<kAssemble><<<1, kSchedThreads, 0, s>>>(gd, ctl, chunk_group, n_chunks, sched, n_chunks);
+  else if (mode == kTrial) k_schedule<kTrial><<<1, kSchedThreads, 0, s>>>(gd, ctl, chunk_group, n_chunks, sched, n_chunks);
+  else if (mode == kCorr) k_schedule<kCorr><<<1, kSchedThreads, 0, s>>>(gd, ctl, chunk_group, n_chunks, sched, n_chunks);
+  else k_schedule<kFinal><<<1, kSchedThreads, 0, s>>>(gd, ctl, chunk_group, n_chunks, sched, n_chunks);
   return cudaGetLastError();
 }
 
@@ -604,7 +645,8 @@ struct Batch::Impl {
   bool external_arena = false;
   GroupDesc* d_gd = nullptr;
   GroupCtl* d_ctl = nullptr;
-  int* d_tile_group = nullptr;
+  int* d_chunk_group = nullptr;  // group of each frame chunk (the schedules' source)
+  int* d_sched = nullptr;        // the schedule of the next evaluation launch (ss_sched.cuh)
   int* d_frame_group = nullptr;
   int* d_counters = nullptr;  // kCounters run counters (kCtr*)
   int* d_err = nullptr;       // device error word (bit 0: a shared-memory staging copy timed out)
@@ -614,7 +656,7 @@ struct Batch::Impl {
   int win_bytes = 0;          // template window bytes per assembly/final CTA (0: no windows)
   int ls_win_bytes = 0;       // template window bytes per line-search CTA (0: no windows)
   int* h_counters = nullptr;  // pinned
-  int n_tiles = 0, n_frames_total = 0;
+  int n_tiles = 0, n_chunks = 0, n_frames_total = 0;
   int max_hb = 0;  // largest block height among groups whose geometry k_eval stages in shared memory
   KernelSet ks = {nullptr, nullptr, nullptr};
   SumFn sum = nullptr;
@@ -640,6 +682,7 @@ struct Batch::Impl {
   cudaStream_t cap_stream = nullptr;
 
   void eval_timed(int mode) {
+    if (mode != kTrial || ks.round) sched_launch(mode, stream, d_gd, d_ctl, d_chunk_group, n_chunks, d_sched);
     if (timing) {
       if (event_used + 2 > events.size()) {
         for (int k = 0; k < 64; k++) {
@@ -651,9 +694,9 @@ struct Batch::Impl {
       }
       cudaEventRecord(events[event_used], stream);
     }
-    if (mode == kTrial && ks.round) ks.round(n_tiles, stream, d_gd, d_tile_group, d_ctl, win_bytes);
+    if (mode == kTrial && ks.round) ks.round(n_tiles, stream, d_gd, d_sched, n_chunks, d_ctl, win_bytes);
     else if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl, ls_win_bytes);
-    else ks.eval(mode, n_tiles, stream, d_gd, d_tile_group, d_ctl, max_hb, win_bytes);
+    else ks.eval(mode, n_tiles, stream, d_gd, d_sched, n_chunks, d_ctl, max_hb, win_bytes);
     if (timing) {
       cudaEventRecord(events[event_used + 1], stream);
       event_mode[event_used] = mode;
@@ -683,6 +726,7 @@ static void layout(Batch::Impl* b, char* base) {
   cv.base = base;
   const size_t tsz = dtype_size(b->tpl_dt);
   b->n_tiles = 0;
+  b->n_chunks = 0;
   b->n_frames_total = 0;
   std::vector<GroupDesc>& gd = b->gd;
   gd.assign(b->hg.size(), GroupDesc{});
@@ -697,13 +741,14 @@ static void layout(Batch::Impl* b, char* base) {
     GroupDesc& G = gd[i];
     G.Hb = g.Hb; G.W = g.W; G.nF = g.nF; G.fW = g.fW; G.N = g.N; G.Ht = g.Ht; G.Wt = g.Wt;
     G.group_size = g.group_size; G.n_rg = g.n_rg;
-    G.tile_base = b->n_tiles;
+    G.chunk_base = b->n_chunks;
     G.frames_per_cta = g.frames_per_cta;
     G.geo_k = g.geo_k;
     G.geo_L = g.geo_L;
     G.geo_ax = (float)g.geo_ax; G.geo_bx = (float)g.geo_bx; G.geo_ay = (float)g.geo_ay; G.geo_by = (float)g.geo_by;
     G.geo_fs = (float)g.geo_fs;
     b->n_tiles += g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
+    b->n_chunks += (g.nF + g.frames_per_cta - 1) / g.frames_per_cta;
     if (!(b->compute == 1 && g.geo_k > 0)) b->max_hb = std::max(b->max_hb, g.Hb);  // affine: no tables
     G.frame_base = b->n_frames_total;
     b->n_frames_total += g.nF;
@@ -809,7 +854,8 @@ static void layout(Batch::Impl* b, char* base) {
   }
   b->d_gd = cv.take<GroupDesc>(gd.size());
   b->d_ctl = cv.take<GroupCtl>(gd.size());
-  b->d_tile_group = cv.take<int>(std::max(1, b->n_tiles));
+  b->d_chunk_group = cv.take<int>(std::max(1, b->n_chunks));
+  b->d_sched = cv.take<int>(sched_ints(b->n_chunks));
   b->d_frame_group = cv.take<int>(std::max(1, b->n_frames_total));
   b->arena_bytes = cv.off + 256;
 }
@@ -888,7 +934,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
 
   // uploads
   cudaStream_t s = b->stream;
-  std::vector<int> tile_group(std::max(1, b->n_tiles)), frame_group(std::max(1, b->n_frames_total));
+  std::vector<int> chunk_group(std::max(1, b->n_chunks)), frame_group(std::max(1, b->n_frames_total));
   for (size_t i = 0; i < b->hg.size(); i++) {
     HostGroup& g = b->hg[i];
     GroupDesc& G = b->gd[i];
@@ -953,12 +999,12 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     SS_CK(cudaGetLastError());
     b->sum(G.image, (size_t)g.Hb * g.fW, b->d_sum_parts, g.d_sum, s);
     SS_CK(cudaGetLastError());
-    const int ntiles = g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
-    for (int t = 0; t < ntiles; t++) tile_group[G.tile_base + t] = (int)i;
+    const int nchunks = (g.nF + g.frames_per_cta - 1) / g.frames_per_cta;
+    for (int t = 0; t < nchunks; t++) chunk_group[G.chunk_base + t] = (int)i;
     for (int f = 0; f < g.nF; f++) frame_group[G.frame_base + f] = (int)i;
   }
   SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
-  SS_CK(cudaMemcpyAsync(b->d_tile_group, tile_group.data(), tile_group.size() * 4, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(b->d_chunk_group, chunk_group.data(), chunk_group.size() * 4, cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_frame_group, frame_group.data(), frame_group.size() * 4, cudaMemcpyHostToDevice, s));
   // pageable sources are staged before the copies return; an own stream is also drained
   if (b->own_stream) SS_CK(cudaStreamSynchronize(s));
@@ -1059,7 +1105,9 @@ static int enqueue_cycle(Batch::Impl* b) {
 static int launch_cycle(Batch::Impl* b) {
   b->cycles++;
   b->rounds += b->ks.round ? b->cur_rounds : 1;
-  b->launches += b->ks.round ? b->cur_rounds + 7 : 7;
+  // schedules and evaluation passes (2 each), solve, after-ls, iteration end, final; the line
+  // search (precision 'D') or the correlation pass and two launches per trial round (precision 'S')
+  b->launches += b->ks.round ? 2 * b->cur_rounds + 10 : 9;
   int rc = enqueue_cycle(b);
   if (rc) return rc;
   if (!b->ev_cycle) SS_CK(cudaEventCreateWithFlags(&b->ev_cycle, cudaEventDisableTiming));
@@ -1076,22 +1124,21 @@ static int launch_cycle(Batch::Impl* b) {
 
 constexpr int kGraphRounds = 64;
 
-// Condition of the trial-round loop: another round while a line search is open and the cycle is
-// under its round bound. `first` starts the cycle's round count.
-__global__ void __launch_bounds__(256) k_rounds_ctl(const GroupCtl* __restrict__ ctl, int n_groups,
-                                                    int* __restrict__ ctr, int first,
-                                                    cudaGraphConditionalHandle h) {
-  int open = 0;
-  for (int g = threadIdx.x; g < n_groups; g += blockDim.x)
-    open |= (ctl[g].ls_state == 1 && ctl[g].ls_pending > 0) ? 1 : 0;
-  open = __syncthreads_or(open);
+// Schedule of the next trial round and the condition of the trial-round loop: another round while
+// a frame is searching and the cycle is under its round bound. `first` starts the cycle's count.
+__global__ void __launch_bounds__(kSchedThreads) k_sched_rounds(const GroupDesc* __restrict__ gds,
+                                                                const GroupCtl* __restrict__ ctl,
+                                                                const int* __restrict__ chunk_group, int n_chunks,
+                                                                int* __restrict__ sched, int* __restrict__ ctr,
+                                                                int first, cudaGraphConditionalHandle h) {
+  const int tiles = build_schedule<kTrial>(gds, ctl, chunk_group, n_chunks, sched, n_chunks);
   if (threadIdx.x == 0) {
     if (first) ctr[kCtrRound] = 0;
-    const bool more = open && ctr[kCtrRound] < kGraphRounds;
+    const bool more = tiles > 0 && ctr[kCtrRound] < kGraphRounds;
     if (more) {
       ctr[kCtrRound]++;
       ctr[kCtrRounds]++;
-    } else if (open) {
+    } else if (tiles > 0) {
       ctr[kCtrBound] |= 2;
     }
     cudaGraphSetConditional(h, more ? 1u : 0u);
@@ -1131,8 +1178,8 @@ static int capture_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph
 // Opts every kernel of the run into its shared memory before capture (no attribute calls inside).
 static int prime_attributes(Batch::Impl* b) {
   SS_CK(smem_attr(k_solve, (int)kSolveSmem));
-  SS_CK(b->ks.eval(kAssemble, 0, b->stream, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes));
-  if (b->ks.round) SS_CK(b->ks.round(0, b->stream, b->d_gd, b->d_tile_group, b->d_ctl, b->win_bytes));
+  SS_CK(b->ks.eval(kAssemble, 0, b->stream, b->d_gd, b->d_sched, b->n_chunks, b->d_ctl, b->max_hb, b->win_bytes));
+  if (b->ks.round) SS_CK(b->ks.round(0, b->stream, b->d_gd, b->d_sched, b->n_chunks, b->d_ctl, b->win_bytes));
   else SS_CK(b->ks.ls(0, b->stream, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes));
   return SS_OK;
 }
@@ -1168,18 +1215,25 @@ static int build_run_graph(Batch::Impl* b) {
   // one cycle
   if (b->ks.round) SS_CK(cudaGraphConditionalHandleCreate(&h_round, body, 0, 0));
   SS_CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, mode));
-  b->ks.eval(kAssemble, b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes);
+  int* sc = b->d_sched;
+  const int nc = b->n_chunks;
+  sched_launch(kAssemble, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
+  b->ks.eval(kAssemble, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
   k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
   if (b->ks.round) {
-    k_rounds_ctl<<<1, 256, 0, s>>>(b->d_ctl, nG, b->d_counters, 1, h_round);
+    k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc, b->d_counters, 1, h_round);
     rc = capture_while(s, h_round, &rounds_body);
-    if (!rc) b->ks.eval(kCorr, b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes);
+    if (!rc) {
+      sched_launch(kCorr, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
+      b->ks.eval(kCorr, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
+    }
   } else {
     b->ks.ls(b->n_frames_total, s, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes);
   }
   k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
-  b->ks.eval(kFinal, b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->max_hb, b->win_bytes);
+  sched_launch(kFinal, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
+  b->ks.eval(kFinal, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
   k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + kCtrDone);
   k_cycle_ctl<<<1, 32, 0, s>>>(b->d_counters, nG, max_cycles, h_cycle);
   e = cudaStreamEndCapture(s, &out);
@@ -1188,8 +1242,8 @@ static int build_run_graph(Batch::Impl* b) {
   // one trial round
   if (b->ks.round) {
     SS_CK(cudaStreamBeginCaptureToGraph(s, rounds_body, nullptr, nullptr, 0, mode));
-    b->ks.round(b->n_tiles, s, b->d_gd, b->d_tile_group, b->d_ctl, b->win_bytes);
-    k_rounds_ctl<<<1, 256, 0, s>>>(b->d_ctl, nG, b->d_counters, 0, h_round);
+    b->ks.round(b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->win_bytes);
+    k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc, b->d_counters, 0, h_round);
     e = cudaStreamEndCapture(s, &out);
     if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("run graph rounds: ") + cudaGetErrorString(e));
   }
@@ -1274,10 +1328,10 @@ int Batch::poll() {
     b->graph_run = false;
     b->cycles = c[kCtrCycles];
     b->rounds = b->ks.round ? c[kCtrRounds] : c[kCtrCycles];
-    // per cycle: assembly, solve, after-ls, iteration end, final pass, final, cycle control, and
-    // the line search (precision 'D') or the round control and correlation (precision 'S'); two
-    // launches per trial round
-    b->launches = b->ks.round ? 9 * c[kCtrCycles] + 2 * c[kCtrRounds] : 8 * c[kCtrCycles];
+    // per cycle: schedules and evaluation passes, solve, after-ls, iteration end, final, cycle
+    // control, and the line search (precision 'D') or the first round schedule and the correlation
+    // pass (precision 'S'); two launches per trial round
+    b->launches = b->ks.round ? 12 * c[kCtrCycles] + 2 * c[kCtrRounds] : 10 * c[kCtrCycles];
     if (c[kCtrBound] & 1) return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
     b->state = 3;
     int rc = finish_run(b);
@@ -1384,7 +1438,7 @@ struct Server::Impl {
     Batch* batch = nullptr;  // the group's buffers (its arena) and host metadata
     bool active = false;
     bool joining = false;    // admitted since the last cycle was launched
-    int tiles = 0, frames = 0;
+    int tiles = 0, chunks = 0, frames = 0;
     GroupCtl init;           // initial control state, uploaded when the slot joins
   };
   int device = 0, capacity = 0;
@@ -1400,10 +1454,11 @@ struct Server::Impl {
   GroupCtl* h_ctl = nullptr;  // pinned: the slots' control state after each cycle
   GroupDesc* d_gd = nullptr;
   GroupCtl* d_ctl = nullptr;
-  int* d_tile_group = nullptr;
+  int* d_chunk_group = nullptr;
+  int* d_sched = nullptr;
   int* d_frame_group = nullptr;
-  int tile_cap = 0, frame_cap = 0, n_tiles = 0, n_frames = 0;
-  std::vector<int> tg, fg;
+  int chunk_cap = 0, frame_cap = 0, n_tiles = 0, n_chunks = 0, n_frames = 0;
+  std::vector<int> cg, fg;
   int* d_counters = nullptr;  // [0] most trials of a search that ended in the cycle, [1] finished groups
   int* h_counters = nullptr;  // pinned
   int* d_err = nullptr;
@@ -1428,7 +1483,8 @@ Server::~Server() {
   if (v->upload_stream) cudaStreamDestroy(v->upload_stream);
   cudaFree(v->d_gd);
   cudaFree(v->d_ctl);
-  cudaFree(v->d_tile_group);
+  cudaFree(v->d_chunk_group);
+  cudaFree(v->d_sched);
   cudaFree(v->d_frame_group);
   cudaFree(v->d_counters);
   cudaFree(v->d_err);
@@ -1513,7 +1569,8 @@ int Server::admit(const ss_inputs* in, ss_outputs* out, const Batch* session, vo
   sl.joining = true;
   sl.active = true;
   const HostGroup& g = bi->hg[0];
-  sl.tiles = g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
+  sl.chunks = (g.nF + g.frames_per_cta - 1) / g.frames_per_cta;
+  sl.tiles = g.W * sl.chunks;
   sl.frames = g.nF;
   GroupDesc G = bi->gd[0];
   G.err = v->d_err;
@@ -1530,36 +1587,40 @@ int Server::admit(const ss_inputs* in, ss_outputs* out, const Batch* session, vo
 static int server_tables(Server::Impl* v) {
   cudaStream_t s = v->stream;
   v->n_tiles = 0;
+  v->n_chunks = 0;
   v->n_frames = 0;
   for (int k = 0; k < v->capacity; k++) {
     auto& sl = v->slots[k];
     if (!sl.active) continue;
-    v->h_gd[k].tile_base = v->n_tiles;
+    v->h_gd[k].chunk_base = v->n_chunks;
     v->h_gd[k].frame_base = v->n_frames;
     v->n_tiles += sl.tiles;
+    v->n_chunks += sl.chunks;
     v->n_frames += sl.frames;
   }
-  if (v->n_tiles > v->tile_cap || v->n_frames > v->frame_cap) {  // between cycles: nothing in flight
+  if (v->n_chunks > v->chunk_cap || v->n_frames > v->frame_cap) {  // between cycles: nothing in flight
     SS_CK(cudaStreamSynchronize(s));
-    cudaFree(v->d_tile_group);
+    cudaFree(v->d_chunk_group);
+    cudaFree(v->d_sched);
     cudaFree(v->d_frame_group);
-    v->tile_cap = std::max(2 * v->tile_cap, v->n_tiles);
+    v->chunk_cap = std::max(2 * v->chunk_cap, v->n_chunks);
     v->frame_cap = std::max(2 * v->frame_cap, v->n_frames);
-    SS_CK(cudaMalloc(&v->d_tile_group, (size_t)v->tile_cap * sizeof(int)));
+    SS_CK(cudaMalloc(&v->d_chunk_group, (size_t)v->chunk_cap * sizeof(int)));
+    SS_CK(cudaMalloc(&v->d_sched, sched_ints(v->chunk_cap) * sizeof(int)));
     SS_CK(cudaMalloc(&v->d_frame_group, (size_t)v->frame_cap * sizeof(int)));
   }
-  v->tg.assign(std::max(1, v->n_tiles), 0);
+  v->cg.assign(std::max(1, v->n_chunks), 0);
   v->fg.assign(std::max(1, v->n_frames), 0);
   for (int k = 0; k < v->capacity; k++) {
     auto& sl = v->slots[k];
     if (!sl.active) continue;
-    for (int t = 0; t < sl.tiles; t++) v->tg[v->h_gd[k].tile_base + t] = k;
+    for (int t = 0; t < sl.chunks; t++) v->cg[v->h_gd[k].chunk_base + t] = k;
     for (int f = 0; f < sl.frames; f++) v->fg[v->h_gd[k].frame_base + f] = k;
   }
   // pageable sources are staged before the copies return
   SS_CK(cudaMemcpyAsync(v->d_gd, v->h_gd.data(), v->capacity * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
-  if (v->n_tiles)
-    SS_CK(cudaMemcpyAsync(v->d_tile_group, v->tg.data(), v->n_tiles * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (v->n_chunks)
+    SS_CK(cudaMemcpyAsync(v->d_chunk_group, v->cg.data(), v->n_chunks * sizeof(int), cudaMemcpyHostToDevice, s));
   if (v->n_frames)
     SS_CK(cudaMemcpyAsync(v->d_frame_group, v->fg.data(), v->n_frames * sizeof(int), cudaMemcpyHostToDevice, s));
   for (int k = 0; k < v->capacity; k++) {
@@ -1588,18 +1649,26 @@ int Server::step() {
   const int nG = v->capacity;
   SS_CK(smem_attr(k_solve, (int)kSolveSmem));
   v->cycles++;
-  v->ks.eval(kAssemble, v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->max_hb, v->win_bytes);
+  int* sc = v->d_sched;
+  const int nc = v->n_chunks;
+  sched_launch(kAssemble, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
+  v->ks.eval(kAssemble, v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->max_hb, v->win_bytes);
   k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(v->d_gd, v->d_ctl);
   if (v->ks.round) {
     SS_CK(cudaMemsetAsync(v->d_counters, 0, sizeof(int), s));
-    for (int r = 0; r < v->cur_rounds; r++) v->ks.round(v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->win_bytes);
-    v->ks.eval(kCorr, v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->max_hb, v->win_bytes);
+    for (int r = 0; r < v->cur_rounds; r++) {
+      sched_launch(kTrial, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
+      v->ks.round(v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->win_bytes);
+    }
+    sched_launch(kCorr, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
+    v->ks.eval(kCorr, v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->max_hb, v->win_bytes);
   } else {
     v->ks.ls(v->n_frames, s, v->d_gd, v->d_frame_group, v->d_ctl, v->ls_win_bytes);
   }
   k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(v->d_gd, v->d_ctl, nG);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(v->d_gd, v->d_ctl);
-  v->ks.eval(kFinal, v->n_tiles, s, v->d_gd, v->d_tile_group, v->d_ctl, v->max_hb, v->win_bytes);
+  sched_launch(kFinal, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
+  v->ks.eval(kFinal, v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->max_hb, v->win_bytes);
   k_final<<<nG, 256, 0, s>>>(v->d_gd, v->d_ctl, v->d_counters + 1);
   SS_CK(cudaGetLastError());
   SS_CK(cudaMemcpyAsync(v->h_counters, v->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -23,6 +23,7 @@
 #include <cooperative_groups.h>
 
 #include "ss_common.cuh"
+#include "ss_sched.cuh"
 
 namespace ss {
 
@@ -421,26 +422,16 @@ __host__ __device__ constexpr size_t stage_bytes(int hb) {
   return ((size_t)hb * (4 * sizeof(Acc) + 1) + 15) & ~(size_t)15;
 }
 
-// Assembly (at p) and final (at kmask) passes. A CTA takes one block column index cc of one group
-// and G.frames_per_cta of its frames, a warp per frame at a time; the column's geometry is staged in
-// shared memory once for all of them, and the frames share the template rows around the column in L1.
+// Assembly (at p), correlation and final (at kmask) passes of one tile: block column cc of one group
+// and frames fb*fpc .. of its chunk fb, a warp per frame at a time; the column's geometry is staged in
+// shared memory once for all of them (at smem), and the frames share the template rows around the
+// column (a window staged after the geometry, for precision 'S', or L1).
 template <class Acc, class FrameT, class TplT, int MODE>
-__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval(const GroupDesc* __restrict__ gds,
-                                                          const int* __restrict__ tile_group,
-                                                          const GroupCtl* __restrict__ ctl, int stage_rows,
-                                                          int win_bytes) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int g = tile_group[blockIdx.x];
-  const GroupDesc& G = gds[g];
-  const GroupCtl& C = ctl[g];
-  if (C.phase != (MODE == kFinal ? kPhFinal : kPhHalf)) return;
-  if (MODE == kAssemble && C.ls_state != 0) return;  // the group's line search still runs
-  // correlation sums once the line search of the second half-step has finished
-  if (MODE == kCorr && (C.shift != 1 || C.ls_state != 1 || C.ls_pending != 0)) return;
+__device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C, int cc, int fb, unsigned char* smem,
+                                          uint64_t* bar, unsigned& bar_phase, bool& win_ok, int stage_rows,
+                                          int win_bytes) {
+  if (!group_has_work<MODE>(C)) return;
   const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
-  const int nfb = (G.nF + fpc - 1) / fpc;
-  const int local = blockIdx.x - G.tile_base;
-  const int cc = local / nfb, fb = local - cc * nfb;
   const int warp = threadIdx.x >> 5;
 
   ColGeo<Acc> geo = global_geo<Acc>(G, cc);
@@ -470,10 +461,9 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
   TWin win{nullptr, 0, 0, 0};
   if constexpr (sizeof(Acc) == 4) {
     const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
-    if (win_cap >= 2 && !G.gquad && f_end - fb * fpc >= kMinWinFrames) {
+    if (win_ok && win_cap >= 2 && !G.gquad && f_end - fb * fpc >= kMinWinFrames) {
       const size_t geo_bytes = (!affine && Hb <= stage_rows) ? stage_bytes<Acc>(Hb) : 0;
       float* wbuf = reinterpret_cast<float*>(smem + geo_bytes);
-      uint64_t* bar = reinterpret_cast<uint64_t*>(smem + geo_bytes + (size_t)win_bytes);
       float klo = INFINITY, khi = -INFINITY;
       for (int f = fb * fpc + threadIdx.x; f < f_end; f += blockDim.x) {
         const int c = f * W + cc;
@@ -500,10 +490,8 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
       int r0, rows;
       window_rows(G, G.col_yrange[2 * cc] + klo, G.col_yrange[2 * cc + 1] + khi, win_cap, r0, rows);
       if (rows > 0) {
-        if (threadIdx.x == 0) mbar_init(bar);
-        __syncthreads();
-        unsigned phase = 0;
-        if (stage_window(G, wbuf, r0, rows, bar, phase)) win = {wbuf, r0, rows, G.tpitch};
+        if (stage_window(G, wbuf, r0, rows, bar, bar_phase)) win = {wbuf, r0, rows, G.tpitch};
+        else win_ok = false;  // a copy may still be in flight: no further windows in this CTA
       }
     }
   }
@@ -555,6 +543,27 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value) k_eval
       for (int i = 0; i < nsums(MODE); i++) dst[i] = out[i];
       G.colcnt[c] = cnt;
     }
+  }
+}
+
+// The evaluation passes over the tiles of the launch's schedule (ss_sched.cuh), one tile at a time
+// per CTA. Dynamic shared memory: the window's mbarrier (16 bytes), the column geometry, the window.
+template <class Acc, class FrameT, class TplT, int MODE>
+__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value)
+    k_eval(const GroupDesc* __restrict__ gds, int* __restrict__ sched, int cap, const GroupCtl* __restrict__ ctl,
+           int stage_rows, int win_bytes) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_tile[3];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  if (threadIdx.x == 0) mbar_init(bar);
+  __syncthreads();
+  unsigned bar_phase = 0;
+  bool win_ok = true;
+  while (fetch_tile(sched, cap, s_tile)) {
+    const int g = s_tile[0];
+    eval_tile<Acc, FrameT, TplT, MODE>(gds[g], ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok,
+                                       stage_rows, win_bytes);
+    __syncthreads();  // s_tile and the shared buffers are reused by the next tile
   }
 }
 
@@ -948,23 +957,16 @@ __device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f
   }
 }
 
+// One trial of the line search for the searching frames of one tile (block column cc of frame chunk
+// fb); the last column of a frame to arrive decides for the frame (ls_decide).
 template <class FrameT, class TplT>
-__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
-    k_trial_round(const GroupDesc* __restrict__ gds, const int* __restrict__ tile_group, GroupCtl* __restrict__ ctl,
-                  int win_bytes) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_list[kMaxChunk];
-  __shared__ int s_n;
-  const int g = tile_group[blockIdx.x];
-  const GroupDesc& G = gds[g];
-  GroupCtl& C = ctl[g];
+__device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int cc, int fb, unsigned char* smem,
+                                           uint64_t* bar, unsigned& bar_phase, bool& win_ok, int win_bytes,
+                                           int* s_list, int& s_n) {
   // ls_pending falls while the round runs: one decision for the whole CTA (0 means every frame of
   // the group has finished)
   if (!__syncthreads_and(C.phase == kPhHalf && C.ls_state == 1 && *(volatile int*)&C.ls_pending > 0)) return;
   const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
-  const int nfb = (G.nF + fpc - 1) / fpc;
-  const int local = blockIdx.x - G.tile_base;
-  const int cc = local / nfb, fb = local - cc * nfb;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int f0 = fb * fpc, f_end = min(G.nF, f0 + fpc);
 
@@ -1003,7 +1005,7 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
 
   TWin win{nullptr, 0, 0, 0};
   const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
-  if (win_cap >= 2 && !G.gquad && ns >= kMinWinFrames) {
+  if (win_ok && win_cap >= 2 && !G.gquad && ns >= kMinWinFrames) {
     float klo = INFINITY, khi = -INFINITY;
     for (int i = threadIdx.x; i < ns; i += blockDim.x) {
       float x0, x1, y0, y1;
@@ -1016,11 +1018,8 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
     window_rows(G, G.col_yrange[2 * cc] + klo, G.col_yrange[2 * cc + 1] + khi, win_cap, r0, rows);
     if (rows > 0) {
       float* wbuf = reinterpret_cast<float*>(smem);
-      uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (size_t)win_bytes);
-      if (threadIdx.x == 0) mbar_init(bar);
-      __syncthreads();
-      unsigned phase = 0;
-      if (stage_window(G, wbuf, r0, rows, bar, phase)) win = {wbuf, r0, rows, G.tpitch};
+      if (stage_window(G, wbuf, r0, rows, bar, bar_phase)) win = {wbuf, r0, rows, G.tpitch};
+      else win_ok = false;  // a copy may still be in flight: no further windows in this CTA
     }
   }
   if (threadIdx.x == 0) {
@@ -1062,6 +1061,30 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
     }
     prev = __shfl_sync(0xffffffffu, prev, 0);
     if (prev == W - 1) ls_decide(G, C, f);  // acquired every column of the frame
+  }
+}
+
+// One line-search trial round of precision 'S' over the tiles of the round's schedule (the chunks
+// with a searching frame), one tile at a time per CTA. Dynamic shared memory: the window's mbarrier
+// (16 bytes), then the template window.
+template <class FrameT, class TplT>
+__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
+    k_trial_round(const GroupDesc* __restrict__ gds, int* __restrict__ sched, int cap, GroupCtl* __restrict__ ctl,
+                  int win_bytes) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_list[kMaxChunk];
+  __shared__ int s_n;
+  __shared__ int s_tile[3];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  if (threadIdx.x == 0) mbar_init(bar);
+  __syncthreads();
+  unsigned bar_phase = 0;
+  bool win_ok = true;
+  while (fetch_tile(sched, cap, s_tile)) {
+    const int g = s_tile[0];
+    trial_tile<FrameT, TplT>(gds[g], ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok, win_bytes,
+                             s_list, s_n);
+    __syncthreads();  // s_tile, s_list and the window are reused by the next tile
   }
 }
 

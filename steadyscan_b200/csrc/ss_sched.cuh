@@ -1,0 +1,159 @@
+// Tile schedules of the evaluation launches.
+//
+// An evaluation tile is one block column of one chunk of G.frames_per_cta consecutive frames of a
+// group. Before each evaluation launch one CTA of k_schedule lists the (group, frame chunk) entries
+// that have work in that launch (the group's phase for the mode; for a trial round, a frame of the
+// chunk still searching), each standing for the group's W tiles, with the prefix sum of their tiles.
+// The evaluation kernels then run as a grid of resident CTAs that take tiles from the list through
+// an atomic counter, so a launch costs in proportion to the work left, not to the batch's size:
+// late trial rounds of a ragged batch, where a few long searches remain, launch no idle CTAs.
+// Results do not depend on the order in which tiles run (per-column sums land in their own slots
+// and each frame's decision reads them in column order).
+#pragma once
+
+#include "ss_common.cuh"
+
+namespace ss {
+
+constexpr int kSchedThreads = 1024;
+
+// Schedule buffer: header, then group[cap], chunk[cap], prefix[cap + 1] (cap = the batch's chunks).
+enum SchedHeader : int { kSchTiles = 0, kSchEntries = 1, kSchNext = 2, kSchHdr = 4 };
+
+__host__ __device__ constexpr size_t sched_ints(int cap) { return (size_t)kSchHdr + 3 * (size_t)cap + 1; }
+
+// Whether a group has tiles in an evaluation launch of MODE (the phase tests of the evaluation
+// kernels; a trial round also needs a frame still searching).
+template <int MODE>
+__device__ __forceinline__ bool group_has_work(const GroupCtl& C) {
+  if (MODE == kFinal) return C.phase == kPhFinal;
+  if (C.phase != kPhHalf) return false;
+  if (MODE == kAssemble) return C.ls_state == 0;  // not while the group's line search runs
+  if (MODE == kCorr) return C.shift == 1 && C.ls_state == 1 && C.ls_pending == 0;  // after shift 1's search
+  return C.ls_state == 1 && C.ls_pending > 0;       // kTrial
+}
+
+// Builds the schedule of an evaluation launch of MODE (one CTA of kSchedThreads); returns the number
+// of tiles listed in every thread.
+template <int MODE>
+__device__ __forceinline__ int build_schedule(const GroupDesc* __restrict__ gds, const GroupCtl* __restrict__ ctl,
+                                              const int* __restrict__ chunk_group, int n_chunks,
+                                              int* __restrict__ sched, int cap) {
+  constexpr int kWarps = kSchedThreads / 32;
+  __shared__ int s_e[kWarps], s_t[kWarps];
+  __shared__ int s_base_e, s_base_t, s_sum_e, s_sum_t;
+  int* grp = sched + kSchHdr;
+  int* chk = grp + cap;
+  int* pre = chk + cap;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) {
+    s_base_e = 0;
+    s_base_t = 0;
+  }
+  __syncthreads();
+  for (int j0 = 0; j0 < n_chunks; j0 += kSchedThreads) {
+    const int j = j0 + t;
+    int g = -1, fb = 0, w = 0;
+    if (j < n_chunks) {
+      g = chunk_group[j];
+      const GroupDesc& G = gds[g];
+      fb = j - G.chunk_base;
+      bool on = group_has_work<MODE>(ctl[g]);
+      if (on && MODE == kTrial) {
+        const int f0 = fb * G.frames_per_cta, f1 = min(G.nF, f0 + G.frames_per_cta);
+        on = false;
+        for (int f = f0; f < f1 && !on; f++) on = (G.fstate[f] & 2) != 0;
+      }
+      w = on ? G.W : 0;
+    }
+    // exclusive scans of the entries and their tiles over the CTA
+    const unsigned bal = __ballot_sync(0xffffffffu, w > 0);
+    const int e_in = __popc(bal & ((1u << lane) - 1u));
+    int w_inc = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, w_inc, o);
+      if (lane >= o) w_inc += v;
+    }
+    if (lane == 31) {
+      s_e[warp] = __popc(bal);
+      s_t[warp] = w_inc;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const int e = s_e[lane], tt = s_t[lane];
+      int ei = e, ti = tt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int a = __shfl_up_sync(0xffffffffu, ei, o), b = __shfl_up_sync(0xffffffffu, ti, o);
+        if (lane >= o) {
+          ei += a;
+          ti += b;
+        }
+      }
+      s_e[lane] = ei - e;
+      s_t[lane] = ti - tt;
+      if (lane == 31) {
+        s_sum_e = ei;
+        s_sum_t = ti;
+      }
+    }
+    __syncthreads();
+    if (w > 0) {
+      const int e = s_base_e + s_e[warp] + e_in;
+      grp[e] = g;
+      chk[e] = fb;
+      pre[e] = s_base_t + s_t[warp] + w_inc - w;
+    }
+    __syncthreads();
+    if (t == 0) {
+      s_base_e += s_sum_e;
+      s_base_t += s_sum_t;
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    sched[kSchTiles] = s_base_t;
+    sched[kSchEntries] = s_base_e;
+    sched[kSchNext] = 0;
+    pre[s_base_e] = s_base_t;
+  }
+  return s_base_t;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kSchedThreads) k_schedule(const GroupDesc* __restrict__ gds,
+                                                            const GroupCtl* __restrict__ ctl,
+                                                            const int* __restrict__ chunk_group, int n_chunks,
+                                                            int* __restrict__ sched, int cap) {
+  build_schedule<MODE>(gds, ctl, chunk_group, n_chunks, sched, cap);
+}
+
+// The CTA's next tile of a scheduled launch into s_tile = (group, block column, frame chunk); false
+// (in every thread) when the list is exhausted. All threads call; s_tile is read until the caller's
+// next __syncthreads.
+__device__ __forceinline__ bool fetch_tile(int* __restrict__ sched, int cap, int* s_tile) {
+  if (threadIdx.x == 0) {
+    const int idx = atomicAdd(sched + kSchNext, 1);
+    if (idx >= sched[kSchTiles]) {
+      s_tile[0] = -1;
+    } else {
+      const int* grp = sched + kSchHdr;
+      const int* chk = grp + cap;
+      const int* pre = chk + cap;
+      int lo = 0, hi = sched[kSchEntries] - 1;  // the last entry starting at or before idx
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= idx) lo = mid;
+        else hi = mid - 1;
+      }
+      s_tile[0] = grp[lo];
+      s_tile[1] = idx - pre[lo];
+      s_tile[2] = chk[lo];
+    }
+  }
+  __syncthreads();
+  return s_tile[0] >= 0;
+}
+
+}  // namespace ss

@@ -57,3 +57,35 @@ def test_max_over_ranks_gloo_two_ranks():
         assert p.exitcode == 0
     got = dict(q.get(timeout=10) for _ in range(2))
     assert got == {0: 15.0, 1: 15.0}
+
+
+@pytest.mark.parametrize("shape,k", [((16, 24), 1), ((16, 24), 2), ((20, 8), 4)])
+def test_block_columns_match_the_block_matrix_of_the_scan_geometry(shape, k):
+    """The bench's on-device frame layout equals prep.frames_to_blockmatrix for the default
+    geometry of rectangular frames and every knot spacing of the ragged workload."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, ROOT)
+    import bench
+    from steadyscan_b200 import prep
+    h, w = shape
+    img = np.arange(h * w, dtype=np.float64).reshape(h, w)
+    s = prep.init_settings({"nknots": h // k + 1}, np.zeros((h + 4, w + 4)), h, w)
+    lay = prep.block_layout(s)
+    ref = prep.frames_to_blockmatrix(img, lay)
+    got = bench.to_block_columns(torch.tensor(img), k).numpy().reshape(lay.frame_h, lay.frame_w, order="F")
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_ragged_workload_shapes():
+    """The ragged generator draws frame sizes, knot spacings and group lengths from their sets."""
+    import torch  # noqa: F401
+    sys.path.insert(0, ROOT)
+    import bench
+    groups, dev, meta = bench.make_ragged_workload("S", 7, "cpu", n_groups=3)
+    assert len(groups) == len(dev) == len(meta) == 3
+    for g, (t, lay), (h, w, k, nf) in zip(groups, dev, meta):
+        assert (h, w) in [(128, 128), (256, 512), (512, 512), (796, 512)] and k in (1, 2, 4) and 1 <= nf <= 128
+        assert g["bmData"].shape == (k * w, (h // k) * nf)
+        assert t.numel() == h * w * nf
+        assert g["move_thresh"] == 1e-3 and g["max_iter"] == 30
