@@ -224,10 +224,21 @@ def ragged(args, device):
     if args.ragged_lean:
         ms, st, res, launches = timed_batch(dg, device, steps, warmup=args.warmup)
         iters = np.array([r["iter_used"] for r in res])
+        # per-pass device time from one run with event timing (host-launched cycles)
+        from steadyscan_b200 import api
+        b = api.Batch(dg)
+        b.set_timing(True)
+        b.run()
+        rs = b.stats()
+        b.close()
         return {"frames": frames, "groups": len(meta), "value": frames / (ms / 1e3), "unit": "frames/s",
                 "ms_per_run": ms, "kernel_launches_per_run": launches // steps, "cycles": st["cycles"],
                 "linesearch_rounds": st["linesearch_rounds"],
-                "iterations": {"min": int(iters.min()), "max": int(iters.max()), "mean": float(iters.mean())}}
+                "iterations": {"min": int(iters.min()), "max": int(iters.max()), "mean": float(iters.mean())},
+                "timed_run": {"run_ms": rs["run_ms"], "cycles": rs["cycles"], "rounds": rs["linesearch_rounds"],
+                              "eval_ms": dict(zip(("assembly", "trial", "correlation", "final"), rs["eval_ms"])),
+                              "frame_passes": dict(zip(("assembly", "trial", "correlation", "final"),
+                                                       rs["frame_passes"]))}}
     tuner = Autotuner(candidates=(8, 16, 32, 64), reps=2)
     t0 = time.perf_counter()
     tuned = tuner.apply(dg)

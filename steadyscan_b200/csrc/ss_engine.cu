@@ -145,9 +145,13 @@ static cudaError_t smem_attr(F* fn, int bytes) {
 // Dynamic shared memory for staging one block column's geometry (tfrac, basex, basey, the next
 // column's tfrac and base_mask) in k_eval.
 constexpr int kStageBytes = 96 * 1024;
-// Shared memory for one template row window of precision 'S' (36 rows of a 512-pixel template):
-// three resident assembly / trial CTAs per SM, the register limit of those kernels.
-constexpr int kWinBytes = 72 * 1024;
+// Shared memory for one template row window of a precision-'S' evaluation CTA (36 rows of a
+// 512-pixel template): three resident assembly / correlation / final CTAs per SM, the register
+// limit of those kernels (build-time tuning; the trial rounds use kTrialWinBytes).
+#ifndef SS_EVAL_WIN_KB
+#define SS_EVAL_WIN_KB 72
+#endif
+constexpr int kWinBytes = SS_EVAL_WIN_KB * 1024;
 // Shared memory for the template rows of one line-search CTA (98 rows of a 512-pixel template;
 // with the kernel's static shared memory one 1024-thread CTA per SM).
 constexpr int kLsWinBytes = 196 * 1024;
@@ -238,9 +242,9 @@ template <class FrameT, class TplT>
 static cudaError_t round_launch(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
                                 GroupCtl* ctl, int win_bytes) {
   auto* fn = k_trial_round<FrameT, TplT>;
-  cudaError_t ae = smem_attr(fn, kWinBytes + 16);
+  cudaError_t ae = smem_attr(fn, kTrialWinBytes + 16);
   if (ae != cudaSuccess) return ae;
-  win_bytes = std::min(win_bytes, kWinBytes) & ~15;
+  win_bytes = std::min(win_bytes, kTrialWinBytes) & ~15;
   const size_t smem = 16 + (size_t)win_bytes;
   const int th = 32 * kEvalWarps;
   const int grid = resident_grid(fn, th, smem, max_tiles);  // cached before any capture

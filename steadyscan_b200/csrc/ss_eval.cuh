@@ -42,10 +42,24 @@ template <class Acc>
 struct MinBlocks {
   static constexpr int value = 2;
 };
+#ifndef SS_EVAL_MIN_BLOCKS
+#define SS_EVAL_MIN_BLOCKS 3
+#endif
 template <>
 struct MinBlocks<float> {
-  static constexpr int value = 3;
+  static constexpr int value = SS_EVAL_MIN_BLOCKS;
 };
+
+// Trial-round CTAs per SM (register bound) and the bytes of their template window; both must fit
+// one SM's shared memory together (build-time tuning).
+#ifndef SS_TRIAL_MIN_BLOCKS
+#define SS_TRIAL_MIN_BLOCKS 4
+#endif
+#ifndef SS_TRIAL_WIN_KB
+#define SS_TRIAL_WIN_KB 52
+#endif
+constexpr int kTrialMinBlocks = SS_TRIAL_MIN_BLOCKS;
+constexpr int kTrialWinBytes = SS_TRIAL_WIN_KB * 1024;
 
 // Line-search CTA: 256 threads; two (FP64) or four (FP32) CTAs per SM. A launch given window bytes
 // keeps the template rows of the CTA's knot range in shared memory for the whole search.
@@ -1068,7 +1082,7 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
 // with a searching frame), one tile at a time per CTA. Dynamic shared memory: the window's mbarrier
 // (16 bytes), then the template window.
 template <class FrameT, class TplT>
-__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<float>::value)
+__global__ void __launch_bounds__(32 * kEvalWarps, kTrialMinBlocks)
     k_trial_round(const GroupDesc* __restrict__ gds, int* __restrict__ sched, int cap, GroupCtl* __restrict__ ctl,
                   int win_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
