@@ -568,6 +568,7 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value)
            int stage_rows, int win_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_tile[3];
+  __shared__ GroupDesc s_gd;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   if (threadIdx.x == 0) mbar_init(bar);
   __syncthreads();
@@ -575,9 +576,10 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value)
   bool win_ok = true;
   while (fetch_tile(sched, cap, s_tile)) {
     const int g = s_tile[0];
-    eval_tile<Acc, FrameT, TplT, MODE>(gds[g], ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok,
+    load_desc(gds + g, &s_gd);
+    eval_tile<Acc, FrameT, TplT, MODE>(s_gd, ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok,
                                        stage_rows, win_bytes);
-    __syncthreads();  // s_tile and the shared buffers are reused by the next tile
+    __syncthreads();  // s_tile, s_gd and the shared buffers are reused by the next tile
   }
 }
 
@@ -976,7 +978,7 @@ __device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f
 template <class FrameT, class TplT>
 __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int cc, int fb, unsigned char* smem,
                                            uint64_t* bar, unsigned& bar_phase, bool& win_ok, int win_bytes,
-                                           int* s_list, int& s_n) {
+                                           int* s_list, int& s_n, float4* s_kn) {
   // ls_pending falls while the round runs: one decision for the whole CTA (0 means every frame of
   // the group has finished)
   if (!__syncthreads_and(C.phase == kPhHalf && C.ls_state == 1 && *(volatile int*)&C.ls_pending > 0)) return;
@@ -1017,15 +1019,22 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     }
   };
 
+  // every searching frame's trial knots at once (one round trip to memory for the tile)
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+    float x0, x1, y0, y1;
+    knots(s_list[i], x0, x1, y0, y1);
+    s_kn[i] = make_float4(x0, x1, y0, y1);
+  }
+  __syncthreads();
+
   TWin win{nullptr, 0, 0, 0};
   const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
   if (win_ok && win_cap >= 2 && !G.gquad && ns >= kMinWinFrames) {
     float klo = INFINITY, khi = -INFINITY;
     for (int i = threadIdx.x; i < ns; i += blockDim.x) {
-      float x0, x1, y0, y1;
-      knots(s_list[i], x0, x1, y0, y1);
-      klo = fminf(klo, fminf(y0, y1));
-      khi = fmaxf(khi, fmaxf(y0, y1));
+      const float4 k = s_kn[i];
+      klo = fminf(klo, fminf(k.z, k.w));
+      khi = fmaxf(khi, fmaxf(k.z, k.w));
     }
     block_minmax(klo, khi);
     int r0, rows;
@@ -1047,8 +1056,8 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     const int f = s_list[i];
     const int c = f * W + cc;
     const size_t coli = (size_t)c * Hb;
-    float x0, x1, y0, y1;
-    knots(f, x0, x1, y0, y1);
+    const float4 kn = s_kn[i];
+    const float x0 = kn.x, x1 = kn.y, y0 = kn.z, y1 = kn.w;
     double ssd;
     int cnt;
     if (win.p && G.pair_ok) {
@@ -1087,8 +1096,10 @@ __global__ void __launch_bounds__(32 * kEvalWarps, kTrialMinBlocks)
                   int win_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_list[kMaxChunk];
+  __shared__ float4 s_kn[kMaxChunk];
   __shared__ int s_n;
   __shared__ int s_tile[3];
+  __shared__ GroupDesc s_gd;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   if (threadIdx.x == 0) mbar_init(bar);
   __syncthreads();
@@ -1096,9 +1107,10 @@ __global__ void __launch_bounds__(32 * kEvalWarps, kTrialMinBlocks)
   bool win_ok = true;
   while (fetch_tile(sched, cap, s_tile)) {
     const int g = s_tile[0];
-    trial_tile<FrameT, TplT>(gds[g], ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok, win_bytes,
-                             s_list, s_n);
-    __syncthreads();  // s_tile, s_list and the window are reused by the next tile
+    load_desc(gds + g, &s_gd);
+    trial_tile<FrameT, TplT>(s_gd, ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok, win_bytes,
+                             s_list, s_n, s_kn);
+    __syncthreads();  // s_tile, s_gd, s_list, s_kn and the window are reused by the next tile
   }
 }
 

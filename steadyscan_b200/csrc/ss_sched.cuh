@@ -156,4 +156,14 @@ __device__ __forceinline__ bool fetch_tile(int* __restrict__ sched, int cap, int
   return s_tile[0] >= 0;
 }
 
+// The tile's group descriptor into shared memory (all threads call; ends with __syncthreads), so
+// the many descriptor reads of a tile are shared-memory loads rather than dependent global ones.
+__device__ __forceinline__ void load_desc(const GroupDesc* __restrict__ src, GroupDesc* dst) {
+  static_assert(sizeof(GroupDesc) % 8 == 0, "descriptor copied in 8-byte words");
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(GroupDesc) / 8); i += blockDim.x) d[i] = __ldg(s + i);
+  __syncthreads();
+}
+
 }  // namespace ss
