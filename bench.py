@@ -241,7 +241,7 @@ def ragged(args, device):
                                                        rs["frame_passes"]))}}
     tuner = Autotuner(candidates=(8, 16, 32, 64), reps=2)
     t0 = time.perf_counter()
-    tuned = tuner.apply(dg)
+    tuned = tuner.apply(dg, validate=True)
     tune_s = time.perf_counter() - t0
     ms_t, st_t, res_t, launches = timed_batch(tuned, device, steps)
     ms_d, st_d, res_d, _ = timed_batch(dg, device, steps)
@@ -311,7 +311,8 @@ def ragged(args, device):
             "host_launched_cycles": {"value": frames / (ms_h / 1e3), "ms_per_run": ms_h, "cycles": st_h["cycles"]},
             "one_batch_per_group": {"value": fr1 / (ms1 / 1e3), "groups": n1, "frames": fr1},
             "graph_equals_host_cycles": bool(same), "max_px_diff_tuned_vs_default_schedule": sched_diff,
-            "autotune": {"seconds": tune_s, "choices": choices, "median_ms": timings},
+            "autotune": {"seconds": tune_s, "choices": choices, "median_ms": timings,
+                         "validation": tuner.last_validation},
             "fp64_path": {"value": frames / (ms_64 / 1e3), "ms_per_run": ms_64},
             "error_vs_fp64": err}
 

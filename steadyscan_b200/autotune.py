@@ -15,7 +15,10 @@ picks it per shape by timing the candidates on the caller's own groups:
   one batch per candidate, ``reps`` timed runs after one warm-up, and the candidate with the lowest
   median time wins (the tile split changes no precision-D result and precision-S results
   only at FP32 rounding level, so every candidate does essentially the same iterations);
-* choices are kept per tuner and, with ``cache_path``, in a JSON file keyed by device name.
+* choices are kept per tuner and, with ``cache_path``, in a JSON file keyed by device name;
+* ``apply(..., validate=True)`` then times the caller's whole batch once with the tuned split and once
+  with the default split and keeps the faster (per-shape timing misses interactions between shapes
+  that share the GPU in one batch); ``last_validation`` records both times.
 
 The reference has no counterpart (its kernels use fixed launch shapes, task_*.cu).
 """
@@ -68,6 +71,7 @@ class Autotuner:
         self.max_repeat = int(max_repeat)
         self.choices: dict = {}
         self.timings: dict = {}
+        self.last_validation: dict | None = None
         self._device = _device_name()
         if cache_path and os.path.exists(cache_path):
             with open(cache_path) as f:
@@ -103,8 +107,10 @@ class Autotuner:
         rep = min(self.max_repeat, max(1, -(-self.min_tiles // max(1, tiles))))
         return out * rep
 
-    def _time(self, probe: list, fpc: int, template_storage) -> float:
-        gs = [dict(g, frames_per_cta=fpc) for g in probe]
+    def _time(self, probe: list, fpc, template_storage) -> float:
+        """Median seconds of one run of ``probe`` at frames_per_cta ``fpc`` (an int for every group,
+        or None to keep each group's own)."""
+        gs = probe if fpc is None else [dict(g, frames_per_cta=fpc) for g in probe]
         b = api.Batch(gs, template_storage=template_storage)
         try:
             b.run()  # warm-up: graph capture, attributes, caches
@@ -141,7 +147,17 @@ class Autotuner:
             self._save()
         return {k: self.choices[k] for k in by_key}
 
-    def apply(self, groups: list, template_storage=None) -> list:
-        """Copies of ``groups`` with the tuned frames_per_cta (tuning the keys not yet chosen)."""
+    def apply(self, groups: list, template_storage=None, validate: bool = False) -> list:
+        """Copies of ``groups`` with the tuned frames_per_cta (tuning the keys not yet chosen); with
+        ``validate``, the default split instead when it runs the whole batch faster."""
         self.tune(groups, template_storage)
-        return [dict(g, frames_per_cta=self.choices[shape_key(g, template_storage)]) for g in groups]
+        tuned = [dict(g, frames_per_cta=self.choices[shape_key(g, template_storage)]) for g in groups]
+        if not validate:
+            return tuned
+        t_tuned = self._time(tuned, None, template_storage)
+        t_default = self._time(groups, 0, template_storage)
+        self.last_validation = {"tuned_s": t_tuned, "default_s": t_default, "kept": "tuned"}
+        if t_default < t_tuned:
+            self.last_validation["kept"] = "default"
+            return [dict(g, frames_per_cta=0) for g in groups]
+        return tuned

@@ -320,15 +320,16 @@ __global__ void __launch_bounds__(kSolveThreads) k_block_tridiag(int n, const do
 }
 
 // Knot-difference regulariser of frame f (extension; lambda = 0 reproduces the reference): sum of
-// |k_{t+1}-k_t|^2 over its W edges, own knots from own (+N for y), right boundary (bx, by).
-__device__ inline double frame_reg(const double* own, int W, int N, double bx, double by) {
+// |k_{t+1}-k_t|^2 over its W edges, own knots from own (+N for y), right boundary (bx, by). All
+// lanes of a warp call; the result is in every lane.
+__device__ inline double frame_reg_warp(const double* own, int W, int N, double bx, double by) {
   double r = 0;
-  for (int t = 0; t < W; t++) {
+  for (int t = threadIdx.x & 31; t < W; t += 32) {
     double x0 = own[t], y0 = own[t + N];
     double x1 = t + 1 < W ? own[t + 1] : bx, y1 = t + 1 < W ? own[t + 1 + N] : by;
     r += (x1 - x0) * (x1 - x0) + (y1 - y0) * (y1 - y0);
   }
-  return r;
+  return warp_sum(r);
 }
 
 // Chunked scan of SmearingFilter::apply (smearingfilter.cpp:24-33), v_i = s v_{i-1} + (1-s) v_i with
@@ -730,18 +731,23 @@ __global__ void __launch_bounds__(kSolveThreads) k_iter_end(const GroupDesc* __r
   if (G.o_all_params && it <= G.max_iter)
     for (int i = t; i < 2 * N; i += nt) G.o_all_params[(size_t)(it - 1) * 2 * N + i] = G.p[i];
   if (t == 0 && (G.flags & kFlagIterCorr) && G.o_iter_corr && it <= G.max_iter) G.o_iter_corr[it - 1] = corr;
-  if (G.flags & kFlagFrameCorr) {  // task.cpp:287-306
-    for (int f = t; f < nF; f += nt) {
+  if (G.flags & kFlagFrameCorr) {  // task.cpp:287-306, a warp per frame
+    const int lane = t & 31;
+    for (int f = t >> 5; f < nF; f += nt >> 5) {
       double s5[5] = {0, 0, 0, 0, 0};
       double nf = 0;
-      for (int cc = 0; cc < W; cc++) {
+      for (int cc = lane; cc < W; cc += 32) {
         const double* s = G.colsum + (size_t)(f * W + cc) * kCsStride;
         for (int k = 0; k < 5; k++) s5[k] += s[kCsFrD + k];
         nf += G.colcnt[f * W + cc];
       }
-      double r = pearson(nf, s5[0], s5[1], s5[2], s5[3], s5[4]);
-      G.o_frame_corr[f] = r;  // mem->corr
-      if (G.o_frame_corr_hist && it <= G.max_iter) G.o_frame_corr_hist[(size_t)(it - 1) * nF + f] = r;
+      for (int k = 0; k < 5; k++) s5[k] = warp_sum(s5[k]);
+      nf = warp_sum(nf);
+      if (lane == 0) {
+        const double r = pearson(nf, s5[0], s5[1], s5[2], s5[3], s5[4]);
+        G.o_frame_corr[f] = r;  // mem->corr
+        if (G.o_frame_corr_hist && it <= G.max_iter) G.o_frame_corr_hist[(size_t)(it - 1) * nF + f] = r;
+      }
     }
   }
   __syncthreads();
@@ -801,11 +807,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_iter_end(const GroupDesc* __r
     if (it == 1)
       for (int i = t; i < 2 * N; i += nt) G.p_last[i] = G.p[i];
     // the final hd_calculateGroupErrvals(mem, 0) recomputes the difference image of active frames
-    for (int f = t; f < nF; f += nt) {
-      if (!frame_active(G, f, 0)) continue;
-      double* km = G.kmask + (size_t)f * 2 * (W + 1);
-      double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
-      for (int k = 0; k < 2 * (W + 1); k++) kd[k] = km[k];
+    const int W2 = 2 * (W + 1);
+    for (int i = t; i < nF * W2; i += nt) {
+      const int f = i / W2;
+      if (frame_active(G, f, 0)) G.kdiff[i] = G.kmask[i];
     }
     __syncthreads();
     if (t == 0) C.phase = kPhFinal;
@@ -827,26 +832,31 @@ __global__ void __launch_bounds__(256) k_final(const GroupDesc* __restrict__ gds
   __shared__ int sh_nact;
   if (t == 0) sh_nact = 0;
   __syncthreads();
-  for (int f = t; f < nF; f += nt) {
+  const int lane = t & 31;
+  for (int f = t >> 5; f < nF; f += nt >> 5) {  // a warp per frame
     double s5[5] = {0, 0, 0, 0, 0}, ssd = 0;
     double nf = 0;
-    for (int cc = 0; cc < W; cc++) {
+    for (int cc = lane; cc < W; cc += 32) {
       const double* s = G.colsum + (size_t)(f * W + cc) * kCsStride;
       for (int k = 0; k < 5; k++) s5[k] += s[kCsFrD + k];
       ssd += s[kCsFinalSsd];
       nf += G.colcnt[f * W + cc];
     }
-    if (frame_active(G, f, 0)) {
-      double val = ssd / nf;
-      if (G.lambda != 0.0) {
-        const double* ks = G.p + (size_t)f * W;
-        val = (ssd + G.lambda * frame_reg(ks, W, N, ks[W], ks[N + W])) / nf;
+    for (int k = 0; k < 5; k++) s5[k] = warp_sum(s5[k]);
+    ssd = warp_sum(ssd);
+    nf = warp_sum(nf);
+    const double* ks = G.p + (size_t)f * W;
+    const double rg = G.lambda != 0.0 ? frame_reg_warp(ks, W, N, ks[W], ks[N + W]) : 0.0;
+    if (lane == 0) {
+      if (frame_active(G, f, 0)) {
+        double val = ssd / nf;
+        if (G.lambda != 0.0) val = (ssd + G.lambda * rg) / nf;
+        G.errval[f] = val;
+        atomicAdd(&sh_nact, 1);
       }
-      G.errval[f] = val;
-      atomicAdd(&sh_nact, 1);
+      G.o_frame_corr[f] = pearson(nf, s5[0], s5[1], s5[2], s5[3], s5[4]);
+      G.o_residrms[f] = sqrt(G.errval[f]);
     }
-    G.o_frame_corr[f] = pearson(nf, s5[0], s5[1], s5[2], s5[3], s5[4]);
-    G.o_residrms[f] = sqrt(G.errval[f]);
   }
   // ParameterOrganizer::organize1D2 (parameterorganizer.cpp:57-98): the last knot of each frame
   // repeats knot W-1

@@ -66,3 +66,9 @@ def test_autotuner_picks_a_candidate_per_shape_and_caches(tmp_path):
     assert t2.timings == {} and t2.choices == t.choices
     for a, b in zip(api.align_groups(groups), api.align_groups(tuned)):
         np.testing.assert_allclose(a["dx"], b["dx"], atol=1e-2, rtol=0)
+    # validation on the whole batch keeps the faster of the tuned and the default split
+    v = t2.apply(groups, validate=True)
+    lv = t2.last_validation
+    assert lv is not None and lv["kept"] in ("tuned", "default")
+    want = [0] * len(groups) if lv["kept"] == "default" else [t.choices[shape_key(g)] for g in groups]
+    assert [g["frames_per_cta"] for g in v] == want
