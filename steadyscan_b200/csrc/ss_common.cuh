@@ -57,7 +57,8 @@ struct GroupCtl {
   int stop_reason, cap_hit, eig_size, n_used;
   int ls_state;    // 1 from the half-step solve until the line search is post-processed
   int ls_pending;  // frames of the half-step whose line search still runs (trial rounds)
-  int pad0, pad1;
+  int solve_now;          // 1 while the group's half-step solve of this cycle runs (set by k_solve_compact)
+  int pad1;
   double correlation, corr;
   long long n_eval;      // frame evaluations the reference would count: errval passes and trials
   long long passes[4];   // frames read per evaluation kind (EvalMode)

@@ -1065,9 +1065,21 @@ static int reset_state(Batch::Impl* b) {
   return SS_OK;
 }
 
-// Dynamic shared memory of k_solve and k_block_tridiag: the separator system of the partitioned
+// Dynamic shared memory of k_solve_system and k_block_tridiag: the separator system of the partitioned
 // solve and the partitions' first-interior relations.
 constexpr size_t kSolveSmem = (size_t)kSolveThreads * kPartSmemStride * sizeof(double);
+
+// The half-step solve of every group in phase kPhHalf: set-up over kSolveSplit CTAs per group,
+// compaction in one CTA, the blocks over kSolveSplit CTAs, the partitioned solve and filters in one
+// CTA, the expansion over kSolveSplit CTAs (ss_group.cuh).
+static void solve_launch(cudaStream_t s, const GroupDesc* gd, GroupCtl* ctl, int nG) {
+  const dim3 split(kSolveSplit, nG);
+  k_solve_prep<<<split, kSolvePrepThreads, 0, s>>>(gd, ctl);
+  k_solve_compact<<<nG, kSolveThreads, 0, s>>>(gd, ctl);
+  k_solve_planes<<<split, kSolvePrepThreads, 0, s>>>(gd, ctl);
+  k_solve_system<<<nG, kSolveThreads, kSolveSmem, s>>>(gd, ctl);
+  k_solve_expand<<<split, kSolvePrepThreads, 0, s>>>(gd, ctl);
+}
 
 // Opts k_block_tridiag into kSolveSmem of dynamic shared memory.
 static cudaError_t block_tridiag_attr() { return smem_attr(k_block_tridiag, (int)kSolveSmem); }
@@ -1083,7 +1095,7 @@ static int enqueue_cycle(Batch::Impl* b) {
   cudaStream_t s = b->stream;
   const int nG = (int)b->gd.size();
   b->eval_timed(kAssemble);
-  k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
+  solve_launch(s, b->d_gd, b->d_ctl, nG);
   SS_CK(cudaGetLastError());
   if (b->ks.round) {
     // trial rounds without a host round trip: as many as the longest search of the previous
@@ -1109,9 +1121,9 @@ static int enqueue_cycle(Batch::Impl* b) {
 static int launch_cycle(Batch::Impl* b) {
   b->cycles++;
   b->rounds += b->ks.round ? b->cur_rounds : 1;
-  // schedules and evaluation passes (2 each), solve, after-ls, iteration end, final; the line
-  // search (precision 'D') or the correlation pass and two launches per trial round (precision 'S')
-  b->launches += b->ks.round ? 2 * b->cur_rounds + 10 : 9;
+  // schedules and evaluation passes (2 each), the solve (5), after-ls, iteration end, final; the
+  // line search (precision 'D') or the correlation pass and two launches per trial round ('S')
+  b->launches += b->ks.round ? 2 * b->cur_rounds + 14 : 13;
   int rc = enqueue_cycle(b);
   if (rc) return rc;
   if (!b->ev_cycle) SS_CK(cudaEventCreateWithFlags(&b->ev_cycle, cudaEventDisableTiming));
@@ -1181,7 +1193,7 @@ static int capture_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph
 
 // Opts every kernel of the run into its shared memory before capture (no attribute calls inside).
 static int prime_attributes(Batch::Impl* b) {
-  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
+  SS_CK(smem_attr(k_solve_system, (int)kSolveSmem));
   SS_CK(b->ks.eval(kAssemble, 0, b->stream, b->d_gd, b->d_sched, b->n_chunks, b->d_ctl, b->max_hb, b->win_bytes));
   if (b->ks.round) SS_CK(b->ks.round(0, b->stream, b->d_gd, b->d_sched, b->n_chunks, b->d_ctl, b->win_bytes));
   else SS_CK(b->ks.ls(0, b->stream, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes));
@@ -1223,7 +1235,7 @@ static int build_run_graph(Batch::Impl* b) {
   const int nc = b->n_chunks;
   sched_launch(kAssemble, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
   b->ks.eval(kAssemble, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
-  k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
+  solve_launch(s, b->d_gd, b->d_ctl, nG);
   if (b->ks.round) {
     k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc, b->d_counters, 1, h_round);
     rc = capture_while(s, h_round, &rounds_body);
@@ -1274,7 +1286,7 @@ int Batch::start() {
   b->t_start = std::chrono::steady_clock::now();
   SS_CK(cudaSetDevice(b->device));
   if (!b->h_counters) SS_CK(cudaHostAlloc(&b->h_counters, (kCounters + 1) * sizeof(int), cudaHostAllocDefault));
-  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
+  SS_CK(smem_attr(k_solve_system, (int)kSolveSmem));
   int rc = reset_state(b);
   if (rc) return rc;
   b->cycles = 0;
@@ -1332,10 +1344,10 @@ int Batch::poll() {
     b->graph_run = false;
     b->cycles = c[kCtrCycles];
     b->rounds = b->ks.round ? c[kCtrRounds] : c[kCtrCycles];
-    // per cycle: schedules and evaluation passes, solve, after-ls, iteration end, final, cycle
-    // control, and the line search (precision 'D') or the first round schedule and the correlation
-    // pass (precision 'S'); two launches per trial round
-    b->launches = b->ks.round ? 12 * c[kCtrCycles] + 2 * c[kCtrRounds] : 10 * c[kCtrCycles];
+    // per cycle: schedules and evaluation passes, the solve (5), after-ls, iteration end, final,
+    // cycle control, and the line search (precision 'D') or the first round schedule and the
+    // correlation pass (precision 'S'); two launches per trial round
+    b->launches = b->ks.round ? 16 * c[kCtrCycles] + 2 * c[kCtrRounds] : 14 * c[kCtrCycles];
     if (c[kCtrBound] & 1) return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
     b->state = 3;
     int rc = finish_run(b);
@@ -1651,13 +1663,13 @@ int Server::step() {
   if (v->n_tiles == 0) return SS_OK;  // nothing to run
   cudaStream_t s = v->stream;
   const int nG = v->capacity;
-  SS_CK(smem_attr(k_solve, (int)kSolveSmem));
+  SS_CK(smem_attr(k_solve_system, (int)kSolveSmem));
   v->cycles++;
   int* sc = v->d_sched;
   const int nc = v->n_chunks;
   sched_launch(kAssemble, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
   v->ks.eval(kAssemble, v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->max_hb, v->win_bytes);
-  k_solve<<<nG, kSolveThreads, kSolveSmem, s>>>(v->d_gd, v->d_ctl);
+  solve_launch(s, v->d_gd, v->d_ctl, nG);
   if (v->ks.round) {
     SS_CK(cudaMemsetAsync(v->d_counters, 0, sizeof(int), s));
     for (int r = 0; r < v->cur_rounds; r++) {

@@ -405,45 +405,47 @@ __device__ void range_seq(double* v, int n, double strength) {
   }
 }
 
-// Half-step set-up and solve for every group in phase kPhHalf (one CTA per group):
+// The half-step solve of every group in phase kPhHalf runs as five launches: the per-column and
+// per-frame set-up and the block assembly are spread over kSolveSplit CTAs per group
+// (k_solve_prep, k_solve_planes, k_solve_expand), the steps that need the whole group in one CTA
+// (compaction, the partitioned solve and the filters) run one 1024-thread CTA per group
+// (k_solve_compact, k_solve_system). A single CTA per group spent most of its time in the
+// independent per-node work, bound by one SM's global-memory queue.
 //   blocksPresent / paramsUsed / errval (task_applyparameters.cuh:74-81, task_createparametermask.cuh,
 //   task_calcerrval.cu:185), the filter switch-off (mainiteration.cpp:246-256), compaction
 //   (task_generatesubsparseoffset.cu), the block-tridiagonal normal equations
 //   (task_filldiagonals.cu:47-159, task_filljtr.cu:3-58) solved exactly in FP64, the solver's
 //   filter (smearingfilter.cpp, rangefilter.cpp), the expansion with fixed knots
 //   (task_expandresults.cu:9-36) and the line-search start.
-__global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __restrict__ gds, GroupCtl* __restrict__ ctl) {
-  const GroupDesc& G = gds[blockIdx.x];
-  GroupCtl& C = ctl[blockIdx.x];
-  if (C.phase != kPhHalf || C.ls_state != 0) return;  // a line search of the group still runs
-  const int t = threadIdx.x, nt = blockDim.x;
-  const int W = G.W, N = G.N, nF = G.nF, fW = G.fW, shift = C.shift;
-  __shared__ double sh_a[kSolveThreads], sh_b[kSolveThreads];
-  __shared__ int sh_i[kSolveThreads];
-  __shared__ int sh_h, sh_nact;
+constexpr int kSolveSplit = 32;     // CTAs per group of the parallel phases
+constexpr int kSolvePrepThreads = 256;
 
-  __shared__ int sh_rebuild;
-  if (t == 0) {
-    if (C.n_filter_iter != 0 && C.iteration > C.n_filter_iter) {
-      C.filter_active = 0;
-      C.filter_id = 0;
-      C.n_filter_iter = 0;
-    }
-    sh_nact = 0;
-  }
-  // (1) block presence for all columns; parameter use and errval for active frames
-  for (int c = t; c < fW; c += nt) G.blocks_present[c] = G.colcnt[c] >= G.min_points[c % W];
-  if (t == 0) G.blocks_present[N - 1] = 0;
-  __syncthreads();
-  for (int c = t; c < fW; c += nt) {
-    int f = c / W;
+// A group solves in this cycle: its half-step starts (no line search of it still runs).
+__device__ __forceinline__ bool solve_starts(const GroupCtl& C) { return C.phase == kPhHalf && C.ls_state == 0; }
+
+// Block presence, parameter use, knot copies, line-search state, errval of the active frames and
+// the committed knots (grid: kSolveSplit x groups).
+__global__ void __launch_bounds__(kSolvePrepThreads) k_solve_prep(const GroupDesc* __restrict__ gds,
+                                                                  const GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.y];
+  const GroupCtl& C = ctl[blockIdx.y];
+  if (!solve_starts(C)) return;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+  const int W = G.W, N = G.N, nF = G.nF, fW = G.fW, shift = C.shift;
+  // a column's block is present with enough valid pixels; a knot is used when a block next to it is
+  for (int c = gt; c < fW; c += gn) {
+    const bool present = G.colcnt[c] >= G.min_points[c % W];
+    G.blocks_present[c] = present;
+    const int f = c / W;
     if (!frame_active(G, f, shift)) continue;
-    G.params_used[c] = (c == 0) ? G.blocks_present[0] : (G.blocks_present[c] | G.blocks_present[c - 1]);
+    const bool before = c > 0 && G.colcnt[c - 1] >= G.min_points[(c - 1) % W];
+    G.params_used[c] = present || before;
   }
+  if (gt == 0) G.blocks_present[N - 1] = 0;
   // knot copies: kmask of every frame, kdiff of the active ones (the state the line search starts
   // from); line-search state
   const int W1 = W + 1;
-  for (int idx = t; idx < nF * W1; idx += nt) {
+  for (int idx = gt; idx < nF * W1; idx += gn) {
     const int f = idx / W1, k = idx - f * W1;
     const double x = G.p[(size_t)f * W + k], y = G.p[(size_t)N + (size_t)f * W + k];
     double* km = G.kmask + (size_t)f * 2 * W1;
@@ -455,16 +457,14 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
       kd[W1 + k] = y;
     }
   }
-  for (int f = t; f < nF; f += nt) {
-    const bool act = frame_active(G, f, shift);
-    G.fstate[f] = act ? 2 : 0;  // searching once the step is known
+  for (int f = gt; f < nF; f += gn) {
+    G.fstate[f] = frame_active(G, f, shift) ? 2 : 0;  // searching once the step is known
     G.ls_trials[f] = 0;
-    if (act) atomicAdd(&sh_nact, 1);
   }
   // errval of the active frames (task_calcerrval.cu:185), a warp per frame
   {
-    const int warp = t >> 5, lane = t & 31, nwarps = nt >> 5;
-    for (int f = warp; f < nF; f += nwarps) {
+    const int lane = threadIdx.x & 31;
+    for (int f = gt >> 5; f < nF; f += gn >> 5) {
       if (!frame_active(G, f, shift)) continue;
       const double* ks = G.p + (size_t)f * W;
       double e = 0, rg = 0;
@@ -483,7 +483,35 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
       if (lane == 0) G.errval[shift * nF + f] = (G.lambda != 0.0) ? (e + G.lambda * rg) / (double)n : e / (double)n;
     }
   }
-  for (int i = t; i < 2 * N; i += nt) G.p_snap[i] = G.p[i];
+  for (int i = gt; i < 2 * N; i += gn) G.p_snap[i] = G.p[i];
+}
+
+// Filter switch-off, line-search start, compaction and the solver's coupling state (one CTA per
+// group). Marks the groups that solve in this cycle (solve_now) for the launches that follow.
+__global__ void __launch_bounds__(kSolveThreads) k_solve_compact(const GroupDesc* __restrict__ gds,
+                                                                 GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.x];
+  GroupCtl& C = ctl[blockIdx.x];
+  const bool starts = solve_starts(C);
+  __syncthreads();  // every thread has read the phase before thread 0 changes the state below
+  if (threadIdx.x == 0) C.solve_now = starts ? 1 : 0;
+  if (!starts) return;
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int N = G.N, nF = G.nF, shift = C.shift;
+  __shared__ int sh_i[kSolveThreads];
+  __shared__ int sh_h, sh_nact;
+  __shared__ int sh_rebuild;
+  if (t == 0) {
+    if (C.n_filter_iter != 0 && C.iteration > C.n_filter_iter) {
+      C.filter_active = 0;
+      C.filter_id = 0;
+      C.n_filter_iter = 0;
+    }
+    sh_nact = 0;
+  }
+  __syncthreads();
+  for (int f = t; f < nF; f += nt)
+    if (frame_active(G, f, shift)) atomicAdd(&sh_nact, 1);
   __syncthreads();
   if (t == 0) {
     C.n_eval += sh_nact;
@@ -542,16 +570,24 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
     for (int i = t; i < N; i += nt) G.eig_valid[i] = 0;
   __syncthreads();
 
-  // (3) blocks of the compact system, coupling to the next list position, written in the plane
-  // layout of the partitioned solve (each thread its partition's nodes)
+}
+
+// Blocks of the compact system and the coupling to the next list position, written in the plane
+// layout of the partitioned solve (node i at PartLayout(h, kSolveThreads).pos_of(i)); one node per
+// thread of kSolveSplit CTAs per group.
+__global__ void __launch_bounds__(kSolvePrepThreads) k_solve_planes(const GroupDesc* __restrict__ gds,
+                                                                    const GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.y];
+  const GroupCtl& C = ctl[blockIdx.y];
+  if (!C.solve_now) return;
+  const int h = C.n_used >> 1, N = G.N, fW = G.fW;
+  if (h <= 0) return;
   const double lam = G.lambda;
-  if (h > 0 && t < min(nt, h)) {
-    const PartLayout PLy(h, nt);
-    double* const pl = G.cr;
-    const int a0 = PLy.a(t), mt = PLy.m(t);
-    for (int kk = 0; kk < mt; kk++) {
-      const int i = a0 + kk;
-      const size_t q = PLy.pos(t, kk);
+  const PartLayout PLy(h, kSolveThreads);
+  double* const pl = G.cr;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < h; i += gridDim.x * blockDim.x) {
+    {
+      const size_t q = PLy.pos_of(i);
       const int k = G.list[i];
       double d0 = 0, d1 = 0, d2 = 0, r0 = 0, r1 = 0;
       double2 o78 = make_double2(0, 0), o9 = make_double2(0, 0);
@@ -607,7 +643,17 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
       pl[(size_t)kPB1 * h + q] = r1;
     }
   }
-  __syncthreads();
+}
+
+// The partitioned FP64 solve, the solver's filter and the median of flag R (one CTA per group).
+__global__ void __launch_bounds__(kSolveThreads) k_solve_system(const GroupDesc* __restrict__ gds,
+                                                                GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.x];
+  GroupCtl& C = ctl[blockIdx.x];
+  if (!C.solve_now) return;
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int h = C.n_used >> 1;
+  __shared__ double sh_a[kSolveThreads], sh_b[kSolveThreads];
 
   // (4) FP64 partitioned block-tridiagonal solve into the compact step [x_0..x_h-1, y_0..y_h-1]
   extern __shared__ double sh_red[];  // kSolveThreads x kPartSmemStride
@@ -637,9 +683,17 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(const GroupDesc* __rest
     }
     __syncthreads();
   }
-  // (8) expansion with the red/green fixed knots
+}
+
+// Expansion of the step with the red/green fixed knots (kSolveSplit CTAs per group).
+__global__ void __launch_bounds__(kSolvePrepThreads) k_solve_expand(const GroupDesc* __restrict__ gds,
+                                                                    const GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.y];
+  const GroupCtl& C = ctl[blockIdx.y];
+  if (!C.solve_now) return;
+  const int N = G.N, h = C.n_used >> 1, shift = C.shift;
   const int half = G.group_size >> 1;
-  for (int idx = t; idx < 2 * N; idx += nt) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < 2 * N; idx += gridDim.x * blockDim.x) {
     int j = idx >= N ? idx - N : idx;
     bool fixed = (((idx + 1) - shift * half) % G.group_size) == 0;
     if (fixed) continue;
