@@ -127,6 +127,48 @@ def make_workload(n_frames, size, group, precision, seed, device):
     return groups, dev, s, lay
 
 
+def plain_small(device, threads):
+    """The plain-method small workload: 50 uint16 frames of a 256x256 template (80 blobs, sigma 2-5
+    px), walk N(0, 0.15 px/line) clipped to +-6 px with one jump of up to 4 px per frame, Poisson
+    noise, knots every 4 lines (65 knots), lambda 1e-2, at most 30 iterations. The FP64 CPU
+    restatement on all host threads against one GPU call in precision D and in precision S."""
+    import torch
+
+    from oracle import oracle
+    from steadyscan_b200 import api, prep, synth
+    sp = synth.WORKLOADS[1]
+    rng = np.random.default_rng(sp["seed"])
+    h, w, nf, nk = sp["h"], sp["w"], sp["n_frames"], sp["nknots"]
+    tmpl = synth.make_template(h, w, sp["n_blobs"], sp["sigma"], rng)
+    walk = synth.make_walk(h * (nf + 1), sp["walk_sigma"], sp["clip_px"], sp["jumps_per_frame"], h, sp["jump_px"], rng)
+    s = prep.init_settings({"nknots": nk, "lambda": sp["lam"], "max_iter": sp["max_iter"]}, tmpl, h, w)
+    lay = prep.block_layout(s)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(sp["seed"])
+    flat = torch.cat(render_block_frames(tmpl, walk, nf, h, w, h // (nk - 1), gen, device))
+    host = flat.cpu().numpy().reshape(lay.frame_h, lay.frame_w * nf, order="F")
+    a = prep.boundary_arguments(s, tmpl, host, nf, layout=lay)
+    oracle.build()
+    t0 = time.perf_counter()
+    o = oracle.align_group(dict(a, flags="D"), n_threads=threads, want_mask=False)
+    cpu_s = time.perf_counter() - t0
+    out = {"workload": "50 frames 256x256 uint16, knots every 4 lines (65 knots), lambda 1e-2, at most 30 "
+                       "iterations", "fp64_oracle": {"frames_per_s": nf / cpu_s, "cores": threads,
+                                                     "iterations": int(o["iterations"])}}
+    ref = np.concatenate([o["dx"], o["dy"]])
+    for prec in ("D", "S"):
+        api.align_group(dict(a, flags=prec), want_mask=False)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = api.align_group(dict(a, flags=prec), want_mask=False)
+        dt = time.perf_counter() - t0
+        e = np.concatenate([g["dx"], g["dy"]]) - ref
+        out[prec] = {"frames_per_s_one_call": nf / dt, "iterations": int(g["iter_used"]),
+                     "rms_px_vs_fp64_oracle": float(np.sqrt(np.mean(e * e))),
+                     "max_px_vs_fp64_oracle": float(np.max(np.abs(e)))}
+    return out
+
+
 RAGGED_SETTINGS = {"lambda": 1e-2, "move_thresh": 1e-3, "max_iter": 30}
 
 
@@ -691,6 +733,10 @@ def main():
         if e2e:
             plain["e2e_vs_plain_D"] = e2e["value"] / plain["D"]["value"]
 
+    small_line = None
+    if rank == 0 and not args.no_cpu:
+        small_line = plain_small(device, threads)
+
     ragged_line = None
     if rank == 0 and not args.no_ragged:
         ragged_line = ragged(args, device)
@@ -707,7 +753,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32" if args.precision == "S" else "f64", "data": "synthetic",
                 "config": workload_config(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc, "plain_gpu": plain,
-                "ragged": ragged_line, "serving": serving_line,
+                "plain_method_small": small_line, "ragged": ragged_line, "serving": serving_line,
                 "run": {"cycles": st["cycles"], "linesearch_rounds": st["linesearch_rounds"],
                         "iterations_min": int(min(iters)), "iterations_max": int(max(iters)),
                         "arena_bytes": st["arena_bytes"]}}
