@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define SS_ABI_VERSION 1
+#define SS_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define SS_API __attribute__((visibility("default")))

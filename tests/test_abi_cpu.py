@@ -36,7 +36,7 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.ss_abi_version() == 1
+    assert lib.ss_abi_version() == 2  # ss_inputs gained frames_per_cta
 
 
 def _expect_invalid(args, match):
