@@ -841,7 +841,8 @@ static void layout(Batch::Impl* b, char* base) {
     G.eig_c = cv.take<double>(4 * N);
     G.eig_valid = cv.take<uint8_t>(N);
     G.list = cv.take<int>(2 * N);
-    G.cr = cv.take<double>(kCrStride * N);
+    // the solve's planes; between solves, the partial sums of the iteration end (k_iter_sums)
+    G.cr = cv.take<double>(std::max<size_t>((size_t)kCrStride * N, 8 * (size_t)kIterSplit));
     const ss_outputs* o = b->outs[i];
     const int mi = in->max_iter;
     G.o_frame_corr = cv.take<double>(nF);
@@ -1109,9 +1110,10 @@ static int enqueue_cycle(Batch::Impl* b) {
   }
   SS_CK(cudaGetLastError());
   k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+  k_iter_sums<<<dim3(kIterSplit, nG), 256, 0, s>>>(b->d_gd, b->d_ctl);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
   b->eval_timed(kFinal);
-  k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
+  k_final<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
   SS_CK(cudaGetLastError());
   SS_CK(cudaMemcpyAsync(b->h_counters, b->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   return SS_OK;
@@ -1121,9 +1123,9 @@ static int enqueue_cycle(Batch::Impl* b) {
 static int launch_cycle(Batch::Impl* b) {
   b->cycles++;
   b->rounds += b->ks.round ? b->cur_rounds : 1;
-  // schedules and evaluation passes (2 each), the solve (5), after-ls, iteration end, final; the
+  // schedules and evaluation passes (2 each), the solve (5), after-ls, iteration end (2), final; the
   // line search (precision 'D') or the correlation pass and two launches per trial round ('S')
-  b->launches += b->ks.round ? 2 * b->cur_rounds + 14 : 13;
+  b->launches += b->ks.round ? 2 * b->cur_rounds + 15 : 14;
   int rc = enqueue_cycle(b);
   if (rc) return rc;
   if (!b->ev_cycle) SS_CK(cudaEventCreateWithFlags(&b->ev_cycle, cudaEventDisableTiming));
@@ -1247,10 +1249,11 @@ static int build_run_graph(Batch::Impl* b) {
     b->ks.ls(b->n_frames_total, s, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes);
   }
   k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+  k_iter_sums<<<dim3(kIterSplit, nG), 256, 0, s>>>(b->d_gd, b->d_ctl);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
   sched_launch(kFinal, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
   b->ks.eval(kFinal, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
-  k_final<<<nG, 256, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + kCtrDone);
+  k_final<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + kCtrDone);
   k_cycle_ctl<<<1, 32, 0, s>>>(b->d_counters, nG, max_cycles, h_cycle);
   e = cudaStreamEndCapture(s, &out);
   if (rc) return rc;
@@ -1344,10 +1347,10 @@ int Batch::poll() {
     b->graph_run = false;
     b->cycles = c[kCtrCycles];
     b->rounds = b->ks.round ? c[kCtrRounds] : c[kCtrCycles];
-    // per cycle: schedules and evaluation passes, the solve (5), after-ls, iteration end, final,
+    // per cycle: schedules and evaluation passes, the solve (5), after-ls, iteration end (2), final,
     // cycle control, and the line search (precision 'D') or the first round schedule and the
     // correlation pass (precision 'S'); two launches per trial round
-    b->launches = b->ks.round ? 16 * c[kCtrCycles] + 2 * c[kCtrRounds] : 14 * c[kCtrCycles];
+    b->launches = b->ks.round ? 17 * c[kCtrCycles] + 2 * c[kCtrRounds] : 15 * c[kCtrCycles];
     if (c[kCtrBound] & 1) return fail(SS_ERR_CUDA, "alignment did not finish within the iteration bound");
     b->state = 3;
     int rc = finish_run(b);
@@ -1682,10 +1685,11 @@ int Server::step() {
     v->ks.ls(v->n_frames, s, v->d_gd, v->d_frame_group, v->d_ctl, v->ls_win_bytes);
   }
   k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(v->d_gd, v->d_ctl, nG);
+  k_iter_sums<<<dim3(kIterSplit, nG), 256, 0, s>>>(v->d_gd, v->d_ctl);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(v->d_gd, v->d_ctl);
   sched_launch(kFinal, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
   v->ks.eval(kFinal, v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->max_hb, v->win_bytes);
-  k_final<<<nG, 256, 0, s>>>(v->d_gd, v->d_ctl, v->d_counters + 1);
+  k_final<<<nG, kSolveThreads, 0, s>>>(v->d_gd, v->d_ctl, v->d_counters + 1);
   SS_CK(cudaGetLastError());
   SS_CK(cudaMemcpyAsync(v->h_counters, v->d_counters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
   SS_CK(cudaMemcpyAsync(v->h_ctl, v->d_ctl, nG * sizeof(GroupCtl), cudaMemcpyDeviceToHost, s));

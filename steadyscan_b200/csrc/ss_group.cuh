@@ -739,38 +739,51 @@ __device__ inline double pearson(double n, double sd, double si, double sdd, dou
   return q / sqrt(a * b);
 }
 
-// End of an iteration (task.cpp:281-373) for groups in kPhIterEnd, after k_eval<kCorr>.
+// Partial sums of the global correlation (task_correlation.cu:62-99) over the per-column sums, for
+// groups in kPhIterEnd: kIterSplit CTAs per group, each writing its 7 sums and valid count to
+// G.cr[8 * blockIdx.x ...] (the solve's plane memory, free between the solve and the next one).
+constexpr int kIterSplit = 32;
+__global__ void __launch_bounds__(256) k_iter_sums(const GroupDesc* __restrict__ gds,
+                                                   const GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.y];
+  if (ctl[blockIdx.y].phase != kPhIterEnd) return;
+  const int t = threadIdx.x;
+  __shared__ double sh[8][8];
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int c = blockIdx.x * blockDim.x + t; c < G.fW; c += gridDim.x * blockDim.x) {
+    const double* s = G.colsum + (size_t)c * kCsStride;
+    v[0] += s[kCsSumD]; v[1] += s[kCsSetN]; v[2] += s[kCsSetD]; v[3] += s[kCsSetDD];
+    v[4] += s[kCsSetI]; v[5] += s[kCsSetII]; v[6] += s[kCsSetDI];
+    v[7] += (double)G.colcnt[c];
+  }
+  for (int k = 0; k < 8; k++) v[k] = warp_sum(v[k]);
+  if ((t & 31) == 0)
+    for (int k = 0; k < 8; k++) sh[k][t >> 5] = v[k];
+  __syncthreads();
+  if (t < 8) {
+    double a = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) a += sh[t][w];
+    G.cr[8 * blockIdx.x + t] = a;
+  }
+}
+
+// End of an iteration (task.cpp:281-373) for groups in kPhIterEnd, after k_eval<kCorr> and
+// k_iter_sums.
 __global__ void __launch_bounds__(kSolveThreads) k_iter_end(const GroupDesc* __restrict__ gds, GroupCtl* __restrict__ ctl) {
   const GroupDesc& G = gds[blockIdx.x];
   GroupCtl& C = ctl[blockIdx.x];
   if (C.phase != kPhIterEnd) return;
   const int t = threadIdx.x, nt = blockDim.x, W = G.W, N = G.N, nF = G.nF;
-  __shared__ double sh[8][kSolveThreads / 32];
-  __shared__ long long sh_n[kSolveThreads / 32];
   __shared__ int sh_action;
-  // global correlation (task_correlation.cu:62-99) from the per-column sums
-  double v[7] = {0, 0, 0, 0, 0, 0, 0};
-  long long n = 0;
-  for (int c = t; c < G.fW; c += nt) {
-    const double* s = G.colsum + (size_t)c * kCsStride;
-    v[0] += s[kCsSumD]; v[1] += s[kCsSetN]; v[2] += s[kCsSetD]; v[3] += s[kCsSetDD];
-    v[4] += s[kCsSetI]; v[5] += s[kCsSetII]; v[6] += s[kCsSetDI];
-    n += G.colcnt[c];
-  }
-  for (int k = 0; k < 7; k++) v[k] = warp_sum(v[k]);
-  n = (long long)warp_sum((int)n);
-  if ((t & 31) == 0) {
-    for (int k = 0; k < 7; k++) sh[k][t >> 5] = v[k];
-    sh_n[t >> 5] = n;
-  }
-  __syncthreads();
+  // global correlation from the partial sums, combined in a fixed order
   if (t == 0) {
     double a[7] = {0, 0, 0, 0, 0, 0, 0};
-    long long nn = 0;
-    for (int w = 0; w < nt / 32; w++) {
-      for (int k = 0; k < 7; k++) a[k] += sh[k][w];
-      nn += sh_n[w];
+    double nd = 0;
+    for (int b = 0; b < kIterSplit; b++) {
+      for (int k = 0; k < 7; k++) a[k] += G.cr[8 * b + k];
+      nd += G.cr[8 * b + 7];
     }
+    const long long nn = (long long)nd;
     double A = *G.sum_image / (double)nn, B = a[0] / (double)nn;
     double S = a[1];
     double assq = a[3] - 2 * A * a[2] + S * A * A;
@@ -877,7 +890,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_iter_end(const GroupDesc* __r
 }
 
 // Outputs of a finished group (task.cpp:381-411, :202-219), after k_eval<kFinal>.
-__global__ void __launch_bounds__(256) k_final(const GroupDesc* __restrict__ gds, GroupCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(kSolveThreads) k_final(const GroupDesc* __restrict__ gds, GroupCtl* __restrict__ ctl,
                                                int* __restrict__ n_done) {
   const GroupDesc& G = gds[blockIdx.x];
   GroupCtl& C = ctl[blockIdx.x];
