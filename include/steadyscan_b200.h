@@ -185,9 +185,10 @@ SS_API int ss_batch_measure(int32_t n_groups, const ss_inputs* in, ss_outputs* o
  * ss_batch_measure returned) instead of an allocation of its own. */
 SS_API int ss_batch_create_ex(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_session* const* sessions,
                               void* arena, int64_t arena_bytes, ss_batch** batch);
-/* ss_batch_run one cycle at a time without blocking: ss_batch_start resets every group to its
- * initial knots (asynchronous); ss_batch_step launches one cycle of every group (assembly, solve,
- * line search, iteration control); ss_batch_poll returns 0 while that cycle runs, 1 when it has
+/* ss_batch_run without blocking: ss_batch_start resets every group to its initial knots
+ * (asynchronous); ss_batch_step launches the run: the whole run as one CUDA graph (the default,
+ * see ss_batch_set_graph), else one cycle of every group (assembly, solve, line search, iteration
+ * control); ss_batch_poll returns 0 while that launch runs, 1 when a host-launched cycle has
  * finished and the next ss_batch_step is due, 2 when every group has stopped (then
  * ss_batch_collect), or an error. */
 SS_API int ss_batch_start(ss_batch* batch);

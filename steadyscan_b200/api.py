@@ -320,7 +320,7 @@ class Batch:
         check(self._lib.ss_batch_step(self._h))
 
     def poll(self) -> int:
-        """0 while the launched cycle runs, 1 when the next step is due, 2 when every group stopped."""
+        """0 while the launch runs, 1 when the next (host-launched) cycle is due, 2 when every group stopped."""
         rc = self._lib.ss_batch_poll(self._h)
         if rc < 0:
             check(rc)
