@@ -9,7 +9,7 @@ import os
 import re
 import sys
 
-SRC = "/root/reference/setup/source/task"
+SRC = os.path.join(os.environ.get("STEADYSCAN_REFERENCE_SOURCE", "/root/reference/setup/source"), "task")
 WANT = {
     "task_updategradients.cu": ["d_updateGradients"],
     "task_filldiagonals.cu": ["d_insertValue", "d_fillDiagonals"],

@@ -10,7 +10,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.abspath(os.path.join(HERE, "..", "_ref", "libssref.so"))
-REF_TREE = "/root/reference/setup/source"
+REF_TREE = os.environ.get("STEADYSCAN_REFERENCE_SOURCE", "/root/reference/setup/source")
 _lib = None
 
 

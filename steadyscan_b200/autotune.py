@@ -8,7 +8,8 @@ window over more frames but fill fewer SMs. The best split depends on the block 
 block column), the number of block columns, the frame storage type and the precision, so the tuner
 picks it per shape by timing the candidates on the caller's own groups:
 
-* groups are keyed by (block height, block columns, template shape, frame type, precision);
+* groups are keyed by (block height, block columns, template shape, frame type, precision, template
+  storage, caller-given gradients);
 * for a key not yet tuned, up to ``probe_groups`` of its groups (at most ``probe_frames`` frames in
   all), repeated until the batch has ``min_tiles`` tiles at the default split (so that, as inside a
   large ragged batch, the GPU is full and the time measures throughput rather than latency), run as
@@ -42,13 +43,29 @@ def _frame_type(a: dict) -> str:
     return np.asarray(d).dtype.str
 
 
+def _gradients_given(a: dict) -> bool:
+    """True when xgrad / ygrad are not the template's forward differences (the library then samples
+    separate gradient quads and stages no template windows, a different per-pixel cost)."""
+    if "xgrad" not in a or "ygrad" not in a:
+        return False
+    t = np.asarray(a["template_image"], dtype=np.float64)
+    xg, yg = np.asarray(a["xgrad"], dtype=np.float64), np.asarray(a["ygrad"], dtype=np.float64)
+    if xg.shape != t.shape or yg.shape != t.shape:
+        return True
+    return not (np.array_equal(xg[:, :-1], np.diff(t, axis=1)) and np.array_equal(yg[:-1, :], np.diff(t, axis=0)))
+
+
 def shape_key(a: dict, template_storage=None) -> str:
-    """The tuning key of one group's argument dict."""
+    """The tuning key of one group's argument dict: block height and columns, template shape, frame
+    type, precision, template storage and whether the gradients are the caller's own. Settings that
+    change how many iterations a group runs but not the work of one evaluation tile (filters,
+    lambda, thresholds, iteration limits) are not part of the key."""
     tf = np.asarray(a["tfrac"])
     flags = a["flags"] if isinstance(a["flags"], str) else bytes(a["flags"]).decode()
     prec = "S" if "S" in flags else "D"
     th, tw = np.asarray(a["template_image"]).shape
-    return f"hb{tf.shape[0]}_w{tf.shape[1]}_t{th}x{tw}_{_frame_type(a)}_{prec}_{template_storage or 'f32'}"
+    grads = "_gq" if _gradients_given(a) else ""
+    return f"hb{tf.shape[0]}_w{tf.shape[1]}_t{th}x{tw}_{_frame_type(a)}_{prec}_{template_storage or 'f32'}{grads}"
 
 
 def _device_name() -> str:

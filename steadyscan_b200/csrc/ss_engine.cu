@@ -4,6 +4,7 @@
 // call's worth of frames) and runs them to completion together: every kernel covers all groups,
 // and a device-side state machine per group (GroupCtl) decides what each group does next, so
 // groups of different sizes and convergence speeds share launches.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -126,17 +127,47 @@ __global__ void k_fill(double* p, size_t n, double v) {
 // ---------------------------------------------------------------------------------------------
 // kernel dispatch by (compute, frame type, template type)
 
-// Opts a kernel into `bytes` of dynamic shared memory on the current device, once per device.
+// Identifier of the calling thread's current CUDA context, unique for the life of the process (the
+// context the runtime creates after a cudaDeviceReset gets a new one); 0 when none is current or the
+// driver does not report one. Read through the runtime's driver entry points (no link to libcuda).
+static unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    f = nullptr;
+    q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Opts a kernel into `bytes` of dynamic shared memory on the current device, once per device and
+// context (the attribute does not survive a reset of the device's context).
 template <class F>
 static cudaError_t smem_attr(F* fn, int bytes) {
   static std::mutex mu;
-  static std::set<std::pair<int, const void*>> done;
+  static std::set<std::tuple<int, unsigned long long, const void*>> done;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  const std::pair<int, const void*> key(dev, reinterpret_cast<const void*>(fn));
+  const auto key = std::make_tuple(dev, current_context_id(), reinterpret_cast<const void*>(fn));
   std::lock_guard<std::mutex> lock(mu);
-  if (done.count(key)) return cudaSuccess;
+  if (std::get<1>(key) != 0 && done.count(key)) return cudaSuccess;
   e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e == cudaSuccess) done.insert(key);
   return e;
@@ -1942,28 +1973,37 @@ namespace ss {
 // Workspace of ss_solve_block_tridiagonal_noalloc: the cyclic-reduction nodes of up to
 // kNoAllocMaxBlocks blocks (3.4 MB). It is file-scope device memory, so every GPU that loads this
 // library holds it until the process exits. Its host-side name is only a handle; the device
-// address comes from cudaGetSymbolAddress, looked up once per device below.
+// address comes from cudaGetSymbolAddress, looked up on the first call per device and context
+// below (a context created after cudaDeviceReset has its own copy of the array at its own address).
 constexpr int kNoAllocMaxBlocks = 32768;
 static __device__ __align__(256) double g_noalloc_work[(size_t)kNoAllocMaxBlocks * kCrStride];
 
+struct NoAllocSlot {
+  unsigned long long ctx = 0;  // context the address belongs to (0: not looked up)
+  double* addr = nullptr;
+};
 static std::mutex g_noalloc_mu;
-static double* g_noalloc_addr[128];  // per device ordinal
+static NoAllocSlot g_noalloc_addr[128];  // per device ordinal
 
-// Device address of g_noalloc_work on the current device, looked up on the first call per device.
+// Device address of g_noalloc_work on the current device and context, looked up on the first call
+// in that context.
 static int noalloc_workspace(double** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= 128) return fail(SS_ERR_NO_DEVICE, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  NoAllocSlot& slot = g_noalloc_addr[dev];
+  const unsigned long long ctx = current_context_id();
+  if (!slot.addr || ctx == 0 || slot.ctx != ctx) {
     double* p = nullptr;
     e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_work);
     if (e != cudaSuccess || !p)
       return fail(SS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_noalloc_addr[dev] = p;
+    slot.addr = p;
+    slot.ctx = current_context_id();  // the lookup makes the device's context current if none was
   }
-  *out = g_noalloc_addr[dev];
+  *out = slot.addr;
   return SS_OK;
 }
 

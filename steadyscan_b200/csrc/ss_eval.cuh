@@ -581,6 +581,7 @@ __global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value)
                                        stage_rows, win_bytes);
     __syncthreads();  // s_tile, s_gd and the shared buffers are reused by the next tile
   }
+  if (!win_ok) drain_window(bar, bar_phase);  // a timed-out copy may still write this CTA's memory
 }
 
 // Line search of one frame per thread-block cluster (task_linesearch.cu:76-149), for every frame of
@@ -644,6 +645,8 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
   // and the correlation pass can evaluate (trial knots lie between p and p + deltaP; kmask and
   // kdiff are earlier states); a range that does not fit uses the global template.
   TWin win{nullptr, 0, 0, 0};
+  uint64_t* stage_bar = nullptr;  // set when a staging copy timed out (drained before the CTA exits)
+  unsigned stage_phase = 0;
   if constexpr (sizeof(Acc) == 4) {
     const int win_cap = G.tplain ? win_bytes / (G.tpitch * (int)sizeof(float)) : 0;
     if (win_cap >= 2 && !G.gquad && hi > lo) {
@@ -668,8 +671,8 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
         uint64_t* bar = reinterpret_cast<uint64_t*>(ls_smem + (size_t)win_bytes);
         if (threadIdx.x == 0) mbar_init(bar);
         __syncthreads();
-        unsigned phase = 0;
-        if (stage_window(G, wbuf, r0, rows, bar, phase)) win = {wbuf, r0, rows, G.tpitch};
+        if (stage_window(G, wbuf, r0, rows, bar, stage_phase)) win = {wbuf, r0, rows, G.tpitch};
+        else stage_bar = bar;
       }
     }
   }
@@ -869,6 +872,7 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
       }
     }
   }
+  if (stage_bar) drain_window(stage_bar, stage_phase);  // uniform over the CTA
   cluster.sync();  // no CTA leaves while others may still read its shared memory
 }
 
@@ -892,6 +896,13 @@ __device__ __forceinline__ int atomic_add_acq_rel(int* p, int v) {
   int old;
   asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
+}
+
+// Device-scope load with acquire order.
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
 // Decision for frame f after all its columns of the round were evaluated (one warp).
@@ -1083,7 +1094,13 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
       prev = atomic_add_acq_rel(G.ls_done + f, 1);  // releases this column's results
     }
     prev = __shfl_sync(0xffffffffu, prev, 0);
-    if (prev == W - 1) ls_decide(G, C, f);  // acquired every column of the frame
+    if (prev == W - 1) {
+      // lane 0's acquire covers lane 0 only and a shuffle orders no memory: every lane reads the
+      // arrival count with acquire order (it reads the value of lane 0's add, the last in the
+      // count's release sequence) before it reads the other CTAs' column results
+      (void)ld_acquire(G.ls_done + f);
+      ls_decide(G, C, f);  // acquired every column of the frame
+    }
   }
 }
 
@@ -1112,6 +1129,7 @@ __global__ void __launch_bounds__(32 * kEvalWarps, kTrialMinBlocks)
                              s_list, s_n, s_kn);
     __syncthreads();  // s_tile, s_gd, s_list, s_kn and the window are reused by the next tile
   }
+  if (!win_ok) drain_window(bar, bar_phase);  // a timed-out copy may still write this CTA's memory
 }
 
 }  // namespace ss

@@ -74,7 +74,10 @@ __device__ __forceinline__ void window_rows(const GroupDesc& G, float ylo, float
 }
 
 // Stages rows [r0, r0 + rows) of the FP32 template into win (whole CTA; barrier already
-// initialised, phase tracked by the caller). Returns false after recording a timeout.
+// initialised, phase tracked by the caller). Returns false after recording a timeout in bit 0 of the
+// batch's error word: the copy may then still be in flight, so the phase is left as it is, the
+// caller stages no further window in this CTA (its later tiles and passes sample the global
+// template instead) and calls drain_window before the CTA exits.
 __device__ __forceinline__ bool stage_window(const GroupDesc& G, float* win, int r0, int rows, uint64_t* bar,
                                            unsigned& phase) {
   __syncthreads();  // the previous window is no longer read
@@ -82,9 +85,17 @@ __device__ __forceinline__ bool stage_window(const GroupDesc& G, float* win, int
     bulk_copy(win, G.tplain + (size_t)r0 * G.tpitch, (unsigned)((size_t)rows * G.tpitch * sizeof(float)), bar);
   bool ok = mbar_wait(bar, phase);
   if (!ok) ok = mbar_wait(bar, phase);  // second bounded wait for the copy still in flight
-  phase ^= 1u;
   if (!ok && threadIdx.x == 0) atomicOr(G.err, 1);
-  return __syncthreads_and(ok ? 1 : 0) != 0;
+  ok = __syncthreads_and(ok ? 1 : 0) != 0;
+  if (ok) phase ^= 1u;
+  return ok;
+}
+
+// Before a CTA whose staging timed out exits: one more bounded wait for the copy into its shared
+// memory (whole CTA).
+__device__ __forceinline__ void drain_window(uint64_t* bar, unsigned phase) {
+  (void)mbar_wait(bar, phase);
+  __syncthreads();
 }
 
 // CTA-wide min of lo and max of hi (all threads call; result in every thread).

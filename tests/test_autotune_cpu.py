@@ -17,6 +17,13 @@ def test_shape_key_separates_shapes_precisions_and_storage():
     assert autotune.shape_key(a) != autotune.shape_key(dict(a, flags="D"))
     assert autotune.shape_key(a) != autotune.shape_key(a, template_storage="f16")
     assert autotune.shape_key(a) == autotune.shape_key(dict(a, nFrames=9))  # length is not part of the key
+    # gradients that are the template's forward differences sample the template window; others not
+    t = np.arange(1600.0).reshape(40, 40) % 7
+    xg = np.hstack([np.diff(t, axis=1), np.full((40, 1), np.nan)])
+    yg = np.vstack([np.diff(t, axis=0), np.full((1, 40), np.nan)])
+    derived = dict(a, template_image=t, xgrad=xg, ygrad=yg)
+    assert autotune.shape_key(derived) == autotune.shape_key(dict(a, template_image=t))
+    assert autotune.shape_key(derived) != autotune.shape_key(dict(derived, xgrad=2 * xg))
 
 
 def test_probe_takes_the_largest_groups_and_fills_the_gpu():
