@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define SS_ABI_VERSION 2
+#define SS_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define SS_API __attribute__((visibility("default")))
@@ -120,6 +120,8 @@ typedef struct ss_outputs {
   int32_t trial_cap_hit;      /* a line search hit its trial bound (the reference loops without one) */
   int64_t n_frame_passes;     /* frame evaluations read from memory (assembly, trials, correlation, final) */
   double elapsed_ms;          /* wall time of the call */
+  uint8_t* blocks_used;       /* W x n_frames column-major: the block has a valid pixel in the final
+                                 mask (output 5), the caller's blocksused (steady_scan.m:264-265) */
 } ss_outputs;
 
 /* align_group_to_template: one group of frames (replaces mexFunction,
@@ -240,6 +242,60 @@ SS_API int ss_solve_block_tridiagonal(int32_t n, const double* diag, const doubl
  * of the workspace it reads before reading it. */
 SS_API int ss_solve_block_tridiagonal_noalloc(int32_t n, const double* diag, const double* coupling,
                                               const double* rhs, double* x, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Recording-level estimate: the caller loop of the reference's MATLAB driver
+ * (estimate_displacements, steady_scan.m:157-288, with the set split of steady_scan.m:97-108),
+ * run as one batch on the GPU with its post-estimate validity rules applied on the device.
+ *
+ * The recording's frames are split into sets of at most frames_per_set frames; every set except
+ * the last is extended by the first frame of the next set, and that overlap frame's estimate is
+ * discarded (steady_scan.m:216-244, "last frame of set is estimated incorrectly"), so the last
+ * frame of the recording is never estimated: its outputs stay NaN. Per kept frame, from the set's
+ * final mask: blocks_used (a valid pixel in the block, steady_scan.m:265); no block used ->
+ * failed, corr NaN (:269-273); otherwise the knots before the first and after the last used block
+ * repeat those blocks' knots (extend_firstandlast, :277-281, :615-623) and
+ * failed = !(corr >= corr_thresh) || nknots-1 / (nknots-1) < minblockfrac (:283; the reference
+ * divides numel(blocksused), i.e. the block count, not the used count).
+ *
+ * As in the reference every set is started from the first columns of est_dx_knots / est_dy_knots
+ * (the driver passes the whole matrix to each set's MEX call, steady_scan.m:239-240, and
+ * ParameterOrganizer::organize2D1 reads the first n_set_frames columns); per_set_estimates = 1
+ * starts each set from its own frames' columns instead (extension).
+ */
+typedef struct ss_recording {
+  ss_inputs group;             /* settings, template and geometry; bm_data holds every frame of the
+                                  recording (Hb x (W * n_frames)), n_frames their count, est_dx/dy
+                                  (W+1) x n_frames (or (W+1) x k with k >= the largest set) */
+  int32_t frames_per_set;      /* settings.frames_per_set (default 500) */
+  int32_t min_frames_per_set;  /* settings.min_frames_per_set (default 100; see ss_recording_sets) */
+  double corr_thresh;          /* settings.corr_thresh (default 0.75) */
+  double minblockfrac;         /* settings.minblockfrac (default 0.25) */
+  int32_t per_set_estimates;   /* 0: the reference's start (first columns), 1: each set's own */
+} ss_recording;
+
+/* Outputs of ss_estimate_displacements (host memory; NULL pointers are not produced). */
+typedef struct ss_recording_outputs {
+  double* dx_knots;    /* (W+1) x n_frames column-major (steady_scan.m:1 dx_knots) */
+  double* dy_knots;
+  double* corr;        /* n_frames */
+  double* iter_used;   /* n_frames (the set's iteration count; NaN where not estimated) */
+  double* residrms;    /* n_frames */
+  uint8_t* failed;     /* n_frames */
+  uint8_t* blocks_used; /* W x n_frames column-major */
+  int32_t n_sets;      /* sets the recording was split into */
+} ss_recording_outputs;
+
+SS_API int ss_estimate_displacements(const ss_recording* rec, ss_recording_outputs* out);
+
+/* The set split of steady_scan.m:97-108 as used by estimate_displacements (:216-220): set s covers
+ * frames first[s] .. first[s] + count[s] - 1 (0-based, the overlap frame included). The driver
+ * also rebalances the sizes of the last two sets when the last holds fewer than
+ * min_frames_per_set frames, but the estimate loop reads the unchanged set starts, so that
+ * rebalancing moves no frame (reproduced here). No device work. Returns the number of sets in
+ * *n_sets and fills at most max_sets entries. */
+SS_API int ss_recording_sets(int32_t n_frames, int32_t frames_per_set, int32_t min_frames_per_set, int32_t* first,
+                             int32_t* count, int32_t max_sets, int32_t* n_sets);
 
 /* Message of the calling thread's last error ("" if none). */
 SS_API const char* ss_last_error(void);

@@ -581,6 +581,35 @@ static void ilu0_solve(St* s) {
             }
         }
     }
+    /* the knot-difference regulariser (extension) on the same entries as for the exact solvers
+     * (add_regulariser): lambda * deg on the xx and yy diagonals, -lambda on the xx and yy
+     * couplings of consecutive used knots, -lambda * L p on the right-hand side */
+    if (s->in->lambda != 0 && m > 0) {
+        double lam = s->in->lambda;
+        int h = m / 2, N = s->N;
+        int* knot_of = (int*)malloc(sizeof(int) * h);
+        for (int k = 0, i = 0; k < N && i < h; k++)
+            if (s->params_used[k]) knot_of[i++] = k;
+        for (int i = 0; i < h; i++) {
+            int k = knot_of[i];
+            int deg = (k > 0) + (k < N - 1);
+            int fresh = i + 1 < h && knot_of[i + 1] == k + 1;
+            for (int c = 0; c < 2; c++) {
+                int r = i + c * h;
+                const double* p = s->p + c * N;
+                double lp = deg * p[k] - (k > 0 ? p[k - 1] : 0) - (k < N - 1 ? p[k + 1] : 0);
+                s->jtr[r] -= lam * lp;
+                for (int a = rowcnt[r]; a < rowcnt[r + 1]; a++) {
+                    if (col[a] == r) val[a] += lam * deg;
+                    if (fresh && col[a] == r + 1) val[a] -= lam;
+                }
+                if (fresh)
+                    for (int a = rowcnt[r + 1]; a < rowcnt[r + 2]; a++)
+                        if (col[a] == r) val[a] -= lam;
+            }
+        }
+        free(knot_of);
+    }
     int* diag = (int*)malloc(sizeof(int) * m);
     int* pos_of = (int*)malloc(sizeof(int) * m);
     for (int i = 0; i < m; i++) pos_of[i] = -1;

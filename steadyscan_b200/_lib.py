@@ -42,8 +42,19 @@ class SSOutputs(C.Structure):
         ("iteration_corr", C.c_void_p), ("frame_corr_history", C.c_void_p), ("iteration_errvals", C.c_void_p),
         ("raw_params", C.c_void_p), ("all_params", C.c_void_p), ("frame_params", C.c_void_p),
         ("stop_reason", C.c_int32), ("trial_cap_hit", C.c_int32), ("n_frame_passes", C.c_int64),
-        ("elapsed_ms", C.c_double),
+        ("elapsed_ms", C.c_double), ("blocks_used", C.c_void_p),
     ]
+
+
+class SSRecording(C.Structure):
+    _fields_ = [("group", SSInputs), ("frames_per_set", C.c_int32), ("min_frames_per_set", C.c_int32),
+                ("corr_thresh", C.c_double), ("minblockfrac", C.c_double), ("per_set_estimates", C.c_int32)]
+
+
+class SSRecordingOutputs(C.Structure):
+    _fields_ = [("dx_knots", C.c_void_p), ("dy_knots", C.c_void_p), ("corr", C.c_void_p), ("iter_used", C.c_void_p),
+                ("residrms", C.c_void_p), ("failed", C.c_void_p), ("blocks_used", C.c_void_p),
+                ("n_sets", C.c_int32)]
 
 
 class SSBatchStats(C.Structure):
@@ -121,6 +132,11 @@ def load(build_if_missing: bool = True):
     lib.ss_solve_block_tridiagonal_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                        C.c_void_p]
     lib.ss_solve_block_tridiagonal_noalloc.restype = C.c_int
+    lib.ss_estimate_displacements.argtypes = [C.POINTER(SSRecording), C.POINTER(SSRecordingOutputs)]
+    lib.ss_estimate_displacements.restype = C.c_int
+    lib.ss_recording_sets.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                      C.c_int32, C.POINTER(C.c_int32)]
+    lib.ss_recording_sets.restype = C.c_int
     _lib = lib
     return lib
 

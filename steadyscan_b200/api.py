@@ -21,8 +21,8 @@ import numpy as np
 from ._lib import (SS_DEVICE, SS_F16, SS_F32, SS_F64, SS_HOST, SS_I32, SS_U8, SS_U16, STOP_NAMES, SSInputs,
                    SSMatrix, SSOutputs, SteadyScanError, check, load)
 
-__all__ = ["align_group_to_template", "align_group", "align_groups", "DeviceMatrix", "SteadyScanError",
-           "ARG_NAMES", "STOP_NAMES"]
+__all__ = ["align_group_to_template", "align_group", "align_groups", "estimate_displacements", "recording_sets",
+           "DeviceMatrix", "SteadyScanError", "ARG_NAMES", "STOP_NAMES"]
 
 ARG_NAMES = ["flags", "template_image", "xgrad", "ygrad", "tfrac", "basex", "basey", "base_mask", "bmData",
              "est_dx_knots", "est_dy_knots", "group_size", "nFrames", "min_points_per_block", "max_iter",
@@ -110,7 +110,8 @@ def _outputs(args: dict, want_mask=True, want_history=False):
     mi = int(args["max_iter"])
     a = dict(dx=np.zeros((w + 1) * nF), dy=np.zeros((w + 1) * nF), frame_corr=np.zeros(nF),
              iter_used=np.zeros(1, np.int32), residrms=np.zeros(nF), device_init_time=np.zeros(1),
-             raw_params=np.zeros(2 * N), frame_params=np.zeros(2 * (w + 1) * nF))
+             raw_params=np.zeros(2 * N), frame_params=np.zeros(2 * (w + 1) * nF),
+             blocks_used=np.zeros(w * nF, np.uint8))
     if want_mask:
         a["mask"] = np.zeros(hb * w * nF, np.uint8)
     if want_history:
@@ -121,7 +122,7 @@ def _outputs(args: dict, want_mask=True, want_history=False):
     p = lambda k: a[k].ctypes.data if k in a else None
     o = SSOutputs(p("dx"), p("dy"), p("frame_corr"), p("iter_used"), p("mask"), p("residrms"),
                   p("device_init_time"), p("iteration_corr"), p("frame_corr_history"), p("iteration_errvals"),
-                  p("raw_params"), p("all_params"), p("frame_params"), 0, 0, 0, 0.0)
+                  p("raw_params"), p("all_params"), p("frame_params"), 0, 0, 0, 0.0, p("blocks_used"))
     return o, a, (hb, w, nF, N, mi)
 
 
@@ -132,7 +133,8 @@ def _result(o: SSOutputs, a: dict, dims) -> dict:
              stop_reason=int(o.stop_reason), stop_name=STOP_NAMES[o.stop_reason] if 0 <= o.stop_reason < 5 else "?",
              trial_cap_hit=bool(o.trial_cap_hit), n_frame_passes=int(o.n_frame_passes),
              elapsed_ms=float(o.elapsed_ms), raw_params=a["raw_params"],
-             frame_params=a["frame_params"].reshape(nF, 2 * (w + 1), order="F"))
+             frame_params=a["frame_params"].reshape(nF, 2 * (w + 1), order="F"),
+             blocks_used=a["blocks_used"].reshape(w, nF, order="F").astype(bool))
     if "mask" in a:
         r["mask"] = a["mask"].reshape(hb, w * nF, order="F").astype(bool)
     if "iteration_corr" in a:
@@ -202,6 +204,46 @@ def align_group_to_template(*argv, nargout: int = 6, template_storage=None):
         outs += [r["iteration_corr"], None, None, r["frame_corr_history"], r["iteration_errvals"], r["raw_params"],
                  None, r["all_params"]]
     return tuple(outs[:nargout])
+
+
+def recording_sets(n_frames: int, frames_per_set: int = 500, min_frames_per_set: int = 100):
+    """The set split of the reference's driver as its estimate loop uses it (ss_recording_sets):
+    a list of (first frame, frame count) per set, 0-based, the overlap frame included."""
+    lib = load()
+    n = C.c_int32()
+    check(lib.ss_recording_sets(int(n_frames), int(frames_per_set), int(min_frames_per_set), None, None, 0,
+                                C.byref(n)))
+    first = (C.c_int32 * n.value)()
+    count = (C.c_int32 * n.value)()
+    check(lib.ss_recording_sets(int(n_frames), int(frames_per_set), int(min_frames_per_set), first, count, n.value,
+                                C.byref(n)))
+    return [(int(first[k]), int(count[k])) for k in range(n.value)]
+
+
+def estimate_displacements(args: dict, frames_per_set: int = 500, min_frames_per_set: int = 100,
+                           corr_thresh: float = 0.75, minblockfrac: float = 0.25, per_set_estimates: bool = False,
+                           template_storage=None) -> dict:
+    """The reference driver's estimate loop over a whole recording (ss_estimate_displacements,
+    steady_scan.m:157-288): ``args`` are the boundary arguments with every frame of the recording in
+    ``bmData`` and ``nFrames`` their count. Returns ``dx_knots``/``dy_knots`` (nknots x n_frames),
+    ``corr``, ``iter_used``, ``residrms`` (NaN where not estimated: the recording's last frame),
+    ``failed``, ``blocks_used`` ((nknots-1) x n_frames) and ``n_sets``."""
+    from ._lib import SSRecording, SSRecordingOutputs
+    lib = load()
+    i, keep = _inputs(args, template_storage)
+    rec = SSRecording(i, int(frames_per_set), int(min_frames_per_set), float(corr_thresh), float(minblockfrac),
+                      1 if per_set_estimates else 0)
+    hb, w = np.shape(args["tfrac"])
+    n = int(args["nFrames"])
+    a = dict(dx=np.zeros((w + 1) * n), dy=np.zeros((w + 1) * n), corr=np.zeros(n), iter_used=np.zeros(n),
+             residrms=np.zeros(n), failed=np.zeros(n, np.uint8), blocks_used=np.zeros(w * n, np.uint8))
+    o = SSRecordingOutputs(*[a[k].ctypes.data for k in ("dx", "dy", "corr", "iter_used", "residrms", "failed",
+                                                        "blocks_used")], 0)
+    check(lib.ss_estimate_displacements(C.byref(rec), C.byref(o)))
+    del keep
+    return dict(dx_knots=a["dx"].reshape(w + 1, n, order="F"), dy_knots=a["dy"].reshape(w + 1, n, order="F"),
+                corr=a["corr"], iter_used=a["iter_used"], residrms=a["residrms"], failed=a["failed"].astype(bool),
+                blocks_used=a["blocks_used"].reshape(w, n, order="F").astype(bool), n_sets=int(o.n_sets))
 
 
 def solve_block_tridiagonal(diag, coupling, rhs, stream: int = 0):

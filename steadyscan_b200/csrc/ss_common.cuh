@@ -116,10 +116,12 @@ struct GroupDesc {
   uint8_t* eig_valid;       // N
   int* list;                // 2N: knot of each list position, then list position of each knot
   double* cr;               // N x 13
+  double* ilu;              // 11 N: ILU(0) factors and forward solve (solver id 0 only)
   // outputs on the device
   double *o_frame_corr, *o_residrms, *o_iter_corr, *o_frame_corr_hist, *o_iter_errvals, *o_all_params;
   double *o_dx, *o_dy, *o_frame_params, *o_raw;
   uint8_t* o_mask;          // Hb x fW column-major, may be null
+  uint8_t* o_blocks_used;   // fW: block column has a valid pixel in the final mask, may be null
 };
 
 // ---------------------------------------------------------------------------------------------

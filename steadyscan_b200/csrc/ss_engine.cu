@@ -23,6 +23,7 @@
 #include "ss_engine.h"
 #include "ss_eval.cuh"
 #include "ss_group.cuh"
+#include "ss_recording.cuh"
 #include "steadyscan_b200.h"
 
 namespace ss {
@@ -874,6 +875,7 @@ static void layout(Batch::Impl* b, char* base) {
     G.list = cv.take<int>(2 * N);
     // the solve's planes; between solves, the partial sums of the iteration end (k_iter_sums)
     G.cr = cv.take<double>(std::max<size_t>((size_t)kCrStride * N, 8 * (size_t)kIterSplit));
+    G.ilu = in->solver_id == 0 ? cv.take<double>(11 * N) : nullptr;
     const ss_outputs* o = b->outs[i];
     const int mi = in->max_iter;
     G.o_frame_corr = cv.take<double>(nF);
@@ -887,6 +889,7 @@ static void layout(Batch::Impl* b, char* base) {
     G.o_frame_params = (o && o->frame_params) ? cv.take<double>(2 * (size_t)(g.W + 1) * nF) : nullptr;
     G.o_raw = (o && o->raw_params) ? cv.take<double>(2 * N) : nullptr;
     G.o_mask = (o && o->mask) ? cv.take<uint8_t>(npx) : nullptr;
+    G.o_blocks_used = (o && o->blocks_used) ? cv.take<uint8_t>(g.fW) : nullptr;
   }
   b->d_gd = cv.take<GroupDesc>(gd.size());
   b->d_ctl = cv.take<GroupCtl>(gd.size());
@@ -1454,6 +1457,7 @@ int Batch::collect() {
     if (o->frame_corr) SS_CK(cudaMemcpyAsync(o->frame_corr, G.o_frame_corr, nF * 8, cudaMemcpyDeviceToHost, s));
     if (o->residrms) SS_CK(cudaMemcpyAsync(o->residrms, G.o_residrms, nF * 8, cudaMemcpyDeviceToHost, s));
     if (o->mask) SS_CK(cudaMemcpyAsync(o->mask, G.o_mask, (size_t)g.Hb * g.fW, cudaMemcpyDeviceToHost, s));
+    if (o->blocks_used) SS_CK(cudaMemcpyAsync(o->blocks_used, G.o_blocks_used, g.fW, cudaMemcpyDeviceToHost, s));
     const size_t mi = g.in->max_iter;
     if (o->iteration_corr) SS_CK(cudaMemcpyAsync(o->iteration_corr, G.o_iter_corr, mi * 8, cudaMemcpyDeviceToHost, s));
     if (o->frame_corr_history)
@@ -1764,6 +1768,106 @@ int Server::active() const {
   return n;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Recording-level estimate (the caller loop of steady_scan.m:157-288)
+
+int recording_sets(int n_frames, int frames_per_set, int min_frames_per_set, int* first, int* count, int max_sets,
+                   int* n_sets) {
+  if (n_frames < 1) return fail(SS_ERR_INVALID_ARGUMENT, "recording has no frames");
+  if (frames_per_set < 1) return fail(SS_ERR_INVALID_ARGUMENT, "frames_per_set must be positive");
+  if (min_frames_per_set < 0) return fail(SS_ERR_INVALID_ARGUMENT, "min_frames_per_set must not be negative");
+  // set_start = 1:frames_per_set:nframes, then nframes + 1 (steady_scan.m:97-99, 1-based); the
+  // size rebalancing of the last two sets (:101-106) changes set_size, which the estimate loop
+  // does not read: set iset covers set_start(iset) : min(set_start(iset + 1), nframes) (:220)
+  int k = 0;
+  for (int s = 1; s <= n_frames; s += frames_per_set, k++) {
+    const int next = s + frames_per_set <= n_frames ? s + frames_per_set : n_frames + 1;
+    const int end = std::min(next, n_frames);
+    if (k < max_sets) {
+      if (first) first[k] = s - 1;
+      if (count) count[k] = end - s + 1;
+    }
+  }
+  if (n_sets) *n_sets = k;
+  return SS_OK;
+}
+
+int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out) {
+  if (!rec || !out) return fail(SS_ERR_INVALID_ARGUMENT, "recording or outputs is NULL");
+  const ss_inputs& g = rec->group;
+  const int n = g.n_frames;
+  const int64_t Hb = g.basex.rows, W = g.basex.cols;
+  if (n < 1 || Hb < 1 || W < 1) return fail(SS_ERR_INVALID_ARGUMENT, "recording has no frames or no blocks");
+  if (g.bm_data.rows != Hb || g.bm_data.cols != W * n)
+    return fail(SS_ERR_INVALID_ARGUMENT, "bm_data must be frameH x (frameW * n_frames)");
+  const size_t esz = dtype_size(g.bm_data.dtype);
+  if (!esz || !g.bm_data.data) return fail(SS_ERR_INVALID_ARGUMENT, "bm_data is NULL or of an unknown dtype");
+  int n_sets = 0;
+  int rc = recording_sets(n, rec->frames_per_set, rec->min_frames_per_set, nullptr, nullptr, 0, &n_sets);
+  if (rc) return rc;
+  std::vector<int> first(n_sets), count(n_sets);
+  recording_sets(n, rec->frames_per_set, rec->min_frames_per_set, first.data(), count.data(), n_sets, &n_sets);
+  // initial knots: the first columns for every set (the reference), or each set's own
+  const int64_t est_vals = std::min(g.est_dx_knots.rows * g.est_dx_knots.cols, g.est_dy_knots.rows * g.est_dy_knots.cols);
+  const size_t ex_sz = dtype_size(g.est_dx_knots.dtype), ey_sz = dtype_size(g.est_dy_knots.dtype);
+  if (!ex_sz || !ey_sz || g.est_dx_knots.location != SS_HOST || g.est_dy_knots.location != SS_HOST)
+    return fail(SS_ERR_INVALID_ARGUMENT, "est_dx_knots and est_dy_knots must be host matrices of a known dtype");
+  std::vector<ss_inputs> ins(n_sets, g);
+  for (int s = 0; s < n_sets; s++) {
+    ss_inputs& in = ins[s];
+    in.n_frames = count[s];
+    const char* base = static_cast<const char*>(g.bm_data.data);
+    in.bm_data.data = base + (size_t)first[s] * W * Hb * esz;
+    in.bm_data.cols = W * count[s];
+    const int64_t col0 = rec->per_set_estimates ? first[s] : 0;
+    if ((col0 + count[s]) * (W + 1) > est_vals)
+      return fail(SS_ERR_INVALID_ARGUMENT, "est_dx_knots / est_dy_knots hold too few columns for the sets");
+    in.est_dx_knots = {static_cast<const char*>(g.est_dx_knots.data) + (size_t)col0 * (W + 1) * ex_sz, W + 1, count[s],
+                       g.est_dx_knots.dtype, SS_HOST};
+    in.est_dy_knots = {static_cast<const char*>(g.est_dy_knots.data) + (size_t)col0 * (W + 1) * ey_sz, W + 1, count[s],
+                       g.est_dy_knots.dtype, SS_HOST};
+  }
+  Batch b;
+  if ((rc = b.prepare(n_sets, ins.data(), nullptr, nullptr, 0))) return rc;
+  if ((rc = b.run())) return rc;
+  Batch::Impl* bi = b.d;
+  cudaStream_t s = bi->stream;
+  // the recording's outputs on the device: NaN / 0 where no set estimates a frame
+  const size_t nk = (size_t)(W + 1) * n, nd = 2 * nk + 3 * (size_t)n, nb = (size_t)n + (size_t)W * n;
+  std::vector<SetSpan> spans(n_sets);
+  for (int k = 0; k < n_sets; k++) spans[k] = {first[k], count[k] - 1};
+  char* buf = nullptr;
+  const size_t span_off = (nd * 8 + nb + 255) & ~size_t(255);
+  SS_CK(cudaMalloc(&buf, span_off + spans.size() * sizeof(SetSpan)));
+  struct Free {
+    char* p;
+    ~Free() { cudaFree(p); }
+  } guard{buf};
+  double* d_dx = reinterpret_cast<double*>(buf);
+  double* d_dy = d_dx + nk;
+  double* d_corr = d_dy + nk;
+  double* d_it = d_corr + n;
+  double* d_rr = d_it + n;
+  uint8_t* d_failed = reinterpret_cast<uint8_t*>(d_rr + n);
+  uint8_t* d_used = d_failed + n;
+  SetSpan* d_spans = reinterpret_cast<SetSpan*>(buf + span_off);
+  k_fill_nan_u8<<<148, 256, 0, s>>>(d_dx, nd, d_failed, nb);
+  SS_CK(cudaMemcpyAsync(d_spans, spans.data(), spans.size() * sizeof(SetSpan), cudaMemcpyHostToDevice, s));
+  k_post_estimate<<<n_sets, 256, 0, s>>>(bi->d_gd, bi->d_ctl, d_spans, rec->corr_thresh, rec->minblockfrac, d_dx, d_dy,
+                                         d_corr, d_it, d_rr, d_failed, d_used);
+  SS_CK(cudaGetLastError());
+  if (out->dx_knots) SS_CK(cudaMemcpyAsync(out->dx_knots, d_dx, nk * 8, cudaMemcpyDeviceToHost, s));
+  if (out->dy_knots) SS_CK(cudaMemcpyAsync(out->dy_knots, d_dy, nk * 8, cudaMemcpyDeviceToHost, s));
+  if (out->corr) SS_CK(cudaMemcpyAsync(out->corr, d_corr, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  if (out->iter_used) SS_CK(cudaMemcpyAsync(out->iter_used, d_it, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  if (out->residrms) SS_CK(cudaMemcpyAsync(out->residrms, d_rr, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  if (out->failed) SS_CK(cudaMemcpyAsync(out->failed, d_failed, (size_t)n, cudaMemcpyDeviceToHost, s));
+  if (out->blocks_used) SS_CK(cudaMemcpyAsync(out->blocks_used, d_used, (size_t)W * n, cudaMemcpyDeviceToHost, s));
+  SS_CK(cudaStreamSynchronize(s));
+  out->n_sets = n_sets;
+  return SS_OK;
+}
+
 int Batch::cycles() const { return d->cycles; }
 int Batch::rounds() const { return d->rounds; }
 int Batch::n_groups() const { return (int)d->gd.size(); }
@@ -2055,6 +2159,19 @@ int ss_solve_block_tridiagonal(int32_t n, const double* diag, const double* coup
                                      cudaGetErrorString(e != cudaSuccess ? e : (e2 != cudaSuccess ? e2 : e3)));
   ss::g_err.clear();
   return SS_OK;
+}
+
+int ss_estimate_displacements(const ss_recording* rec, ss_recording_outputs* out) {
+  int rc = ss::estimate_displacements(rec, out);
+  if (!rc) ss::g_err.clear();
+  return rc;
+}
+
+int ss_recording_sets(int32_t n_frames, int32_t frames_per_set, int32_t min_frames_per_set, int32_t* first,
+                      int32_t* count, int32_t max_sets, int32_t* n_sets) {
+  int rc = ss::recording_sets(n_frames, frames_per_set, min_frames_per_set, first, count, max_sets, n_sets);
+  if (!rc) ss::g_err.clear();
+  return rc;
 }
 
 void ss_batch_destroy(ss_batch* batch) { delete batch; }

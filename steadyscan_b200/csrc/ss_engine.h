@@ -55,8 +55,16 @@ class Batch {
 
  private:
   friend class Server;
+  friend int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out);
   Impl* d;
 };
+
+// The recording-level estimate of ss_estimate_displacements: every set of the recording as one
+// group of one batch, then the caller's post-estimate rules on the device.
+int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out);
+// Set split of ss_recording_sets (0-based first frame and frame count per set, overlap included).
+int recording_sets(int n_frames, int frames_per_set, int min_frames_per_set, int* first, int* count, int max_sets,
+                   int* n_sets);
 
 // Continuous batching: a table of `capacity` group slots on one stream. admit() prepares a group
 // (in the caller's arena, with a session's resident buffers) into a free slot; step() applies the

@@ -585,9 +585,10 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_planes(const GroupD
   const double lam = G.lambda;
   const PartLayout PLy(h, kSolveThreads);
   double* const pl = G.cr;
+  const bool natural = G.solver_id == 0;  // the ILU(0) walk reads the planes in list order
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < h; i += gridDim.x * blockDim.x) {
     {
-      const size_t q = PLy.pos_of(i);
+      const size_t q = natural ? (size_t)i : PLy.pos_of(i);
       const int k = G.list[i];
       double d0 = 0, d1 = 0, d2 = 0, r0 = 0, r1 = 0;
       double2 o78 = make_double2(0, 0), o9 = make_double2(0, 0);
@@ -645,6 +646,115 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_planes(const GroupD
   }
 }
 
+// Solver id 0: the reference's cuSPARSE path (cusparsesolver.cu:119-158), an incomplete LU
+// factorisation without fill, ILU(0), of the compact system in [x_0..x_{h-1}, y_0..y_{h-1}] order
+// (rows and their columns sorted, task_filldiagonals.cu:185-214), then the unit-lower and the upper
+// triangular solve. Each row's pattern is its 2x2 diagonal block and, where list positions i and
+// i+1 are consecutive knots (a "fresh" coupling), the coupling block: row x_i holds x_{i-1}, x_i,
+// x_{i+1}, y_{i-1}, y_i, y_{i+1}; row y_i the same columns. Row by row (IKJ order) the x rows
+// reduce to a tridiagonal LU whose updates of the y columns are kept where the pattern has them
+// (the update of (x_i, y_{i-2}) is dropped); each y row eliminates x_{i-1}, x_i, x_{i+1} and
+// y_{i-1} in column order. The recurrences run along the whole knot chain, so one thread walks
+// them; the updates are unfused multiply and subtract, as the reference's libraries and the
+// host-compiled oracle evaluate them. Inputs: the planes of k_solve_planes in list order (plane f
+// at f * h); scratch: 11 h doubles at ilu; solution into xo[0..h) and yo[0..h).
+__device__ void ilu0_solve_seq(const double* __restrict__ pl, int h, const int* __restrict__ list,
+                               double* __restrict__ ilu, double* __restrict__ xo, double* __restrict__ yo) {
+  const double* Dxx = pl + (size_t)kPD0 * h;
+  const double* Dyy = pl + (size_t)kPD1 * h;
+  const double* Dxy = pl + (size_t)kPD2 * h;
+  const double* c0 = pl + (size_t)kPR0 * h;  // (x_i, x_{i+1})
+  const double* c2 = pl + (size_t)kPR1 * h;  // (x_i, y_{i+1})
+  const double* c3 = pl + (size_t)kPR2 * h;  // (y_i, x_{i+1})
+  const double* c1 = pl + (size_t)kPR3 * h;  // (y_i, y_{i+1})
+  const double* bx = pl + (size_t)kPB0 * h;
+  const double* by = pl + (size_t)kPB1 * h;
+  double* uxx = ilu;          // U (x_i, x_i)
+  double* uxyp = uxx + h;     // U (x_i, y_{i-1})
+  double* uxy = uxyp + h;     // U (x_i, y_i)
+  double* lx = uxy + h;       // L (x_i, x_{i-1})
+  double* l1 = lx + h;        // L (y_i, x_{i-1})
+  double* l2 = l1 + h;        // L (y_i, x_i)
+  double* l3 = l2 + h;        // L (y_i, x_{i+1})
+  double* l4 = l3 + h;        // L (y_i, y_{i-1})
+  double* uyy = l4 + h;       // U (y_i, y_i)
+  double* uyn = uyy + h;      // U (y_i, y_{i+1})
+  double* zx = uyn + h;       // L z = b, x half (the y half goes to yo first)
+  auto fresh = [&](int i) { return i >= 0 && i + 1 < h && list[i + 1] == list[i] + 1; };
+  auto sub = [](double a, double b, double c) { return __dsub_rn(a, __dmul_rn(b, c)); };
+  // x rows: lower entry x_{i-1}; upper entries of row x_{i-1}: x_i, y_{i-2} (not in row x_i),
+  // y_{i-1}, y_i
+  for (int i = 0; i < h; i++) {
+    double a_xx = Dxx[i], a_xyp = 0.0, a_xy = Dxy[i], l = 0.0;
+    if (fresh(i - 1)) {
+      a_xyp = c3[i - 1];
+      l = __ddiv_rn(c0[i - 1], uxx[i - 1]);
+      a_xx = sub(a_xx, l, c0[i - 1]);
+      a_xyp = sub(a_xyp, l, uxy[i - 1]);
+      a_xy = sub(a_xy, l, c2[i - 1]);
+    }
+    lx[i] = l;
+    uxx[i] = a_xx;
+    uxyp[i] = a_xyp;
+    uxy[i] = a_xy;
+  }
+  // y rows: lower entries x_{i-1}, x_i, x_{i+1}, y_{i-1} in column order
+  for (int i = 0; i < h; i++) {
+    const bool fp = fresh(i - 1), fn = fresh(i);
+    double a2 = Dxy[i], a3 = fn ? c3[i] : 0.0, a4 = fp ? c1[i - 1] : 0.0, ayy = Dyy[i], ayn = fn ? c1[i] : 0.0;
+    double q1 = 0.0, q3 = 0.0, q4 = 0.0;
+    if (fp) {  // row x_{i-1}: x_i, y_{i-1}, y_i
+      q1 = __ddiv_rn(c2[i - 1], uxx[i - 1]);
+      a2 = sub(a2, q1, c0[i - 1]);
+      a4 = sub(a4, q1, uxy[i - 1]);
+      ayy = sub(ayy, q1, c2[i - 1]);
+    }
+    const double q2 = __ddiv_rn(a2, uxx[i]);  // row x_i: x_{i+1}, y_{i-1}, y_i, y_{i+1}
+    if (fn) a3 = sub(a3, q2, c0[i]);
+    if (fp) a4 = sub(a4, q2, uxyp[i]);
+    ayy = sub(ayy, q2, uxy[i]);
+    if (fn) ayn = sub(ayn, q2, c2[i]);
+    if (fn) {  // row x_{i+1}: y_i, y_{i+1}
+      q3 = __ddiv_rn(a3, uxx[i + 1]);
+      ayy = sub(ayy, q3, uxyp[i + 1]);
+      ayn = sub(ayn, q3, uxy[i + 1]);
+    }
+    if (fp) {  // row y_{i-1}: y_i
+      q4 = __ddiv_rn(a4, uyy[i - 1]);
+      ayy = sub(ayy, q4, uyn[i - 1]);
+    }
+    l1[i] = q1; l2[i] = q2; l3[i] = q3; l4[i] = q4;
+    uyy[i] = ayy;
+    uyn[i] = ayn;
+  }
+  // L z = b (unit diagonal), entries in column order
+  for (int i = 0; i < h; i++) zx[i] = fresh(i - 1) ? sub(bx[i], lx[i], zx[i - 1]) : bx[i];
+  for (int i = 0; i < h; i++) {
+    const bool fp = fresh(i - 1), fn = fresh(i);
+    double acc = by[i];
+    if (fp) acc = sub(acc, l1[i], zx[i - 1]);
+    acc = sub(acc, l2[i], zx[i]);
+    if (fn) acc = sub(acc, l3[i], zx[i + 1]);
+    if (fp) acc = sub(acc, l4[i], yo[i - 1]);
+    yo[i] = acc;
+  }
+  // U v = z, entries from the last column down
+  for (int i = h - 1; i >= 0; i--) {
+    double acc = yo[i];
+    if (fresh(i)) acc = sub(acc, uyn[i], yo[i + 1]);
+    yo[i] = __ddiv_rn(acc, uyy[i]);
+  }
+  for (int i = h - 1; i >= 0; i--) {
+    const bool fp = fresh(i - 1), fn = fresh(i);
+    double acc = zx[i];
+    if (fn) acc = sub(acc, c2[i], yo[i + 1]);
+    acc = sub(acc, uxy[i], yo[i]);
+    if (fp) acc = sub(acc, uxyp[i], yo[i - 1]);
+    if (fn) acc = sub(acc, c0[i], xo[i + 1]);
+    xo[i] = __ddiv_rn(acc, uxx[i]);
+  }
+}
+
 // The partitioned FP64 solve, the solver's filter and the median of flag R (one CTA per group).
 __global__ void __launch_bounds__(kSolveThreads) k_solve_system(const GroupDesc* __restrict__ gds,
                                                                 GroupCtl* __restrict__ ctl) {
@@ -655,9 +765,15 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_system(const GroupDesc*
   const int h = C.n_used >> 1;
   __shared__ double sh_a[kSolveThreads], sh_b[kSolveThreads];
 
-  // (4) FP64 partitioned block-tridiagonal solve into the compact step [x_0..x_h-1, y_0..y_h-1]
+  // (4) FP64 solve into the compact step [x_0..x_h-1, y_0..y_h-1]: ILU(0) for solver id 0, else the
+  // exact partitioned block-tridiagonal solve
   extern __shared__ double sh_red[];  // kSolveThreads x kPartSmemStride
-  part_solve(G.cr, h, sh_red, G.ndp, 1, G.ndp + h, 1);
+  if (G.solver_id == 0) {
+    if (t == 0 && h > 0) ilu0_solve_seq(G.cr, h, G.list, G.ilu, G.ndp, G.ndp + h);
+    __syncthreads();
+  } else {
+    part_solve(G.cr, h, sh_red, G.ndp, 1, G.ndp + h, 1);
+  }
   // (6) the solver's filter on the x half and the y half (eigensolver.cu:54-55)
   if (C.filter_active) {
     if (C.filter_kind == 1) {
@@ -939,6 +1055,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_final(const GroupDesc* __rest
   }
   if (G.o_raw)
     for (int i = t; i < 2 * N; i += nt) G.o_raw[i] = G.p_last[i];
+  // blocksused of the caller (steady_scan.m:264-265): a block column with a valid pixel in the
+  // final mask, whose per-column count the final pass left in colcnt
+  if (G.o_blocks_used)
+    for (int c = t; c < G.fW; c += nt) G.o_blocks_used[c] = G.colcnt[c] > 0 ? 1 : 0;
   __syncthreads();
   if (t == 0) {
     C.n_eval += sh_nact;

@@ -36,7 +36,14 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.ss_abi_version() == 2  # ss_inputs gained frames_per_cta
+    assert lib.ss_abi_version() == 3  # ss_outputs gained blocks_used; recording-level entry points
+
+
+def test_struct_sizes_match_header(lib):
+    """The ctypes mirrors have the C structs' layout: the last field sits where the header puts it."""
+    assert C.sizeof(_lib.SSOutputs) == 13 * 8 + 4 + 4 + 8 + 8 + 8
+    assert _lib.SSRecording.corr_thresh.offset == C.sizeof(_lib.SSInputs) + 8
+    assert C.sizeof(_lib.SSRecordingOutputs) == 7 * 8 + 8
 
 
 def _expect_invalid(args, match):

@@ -41,6 +41,10 @@ CASES = {
     "solver1_nofilter": dict(settings={"gpu_solver_id": 1, "gpu_filter_id": 0}),
     "range_filter": dict(settings={"gpu_filter_id": 2}),
     "ilu_solver0": dict(settings={"gpu_solver_id": 0}),
+    # 3-tap median of the solved step before the line search (flag R; d_medianfilter.cu:3-20)
+    "median_before_linesearch": dict(settings={"gpu_flags": "R"}, seed=15),
+    "median_before_linesearch_solver1": dict(settings={"gpu_flags": "R", "gpu_solver_id": 1, "gpu_filter_id": 0},
+                                             n_frames=6, seed=16),
     "big_motion": dict(clip_px=6.0, jumps=2, jump_px=4.0, seed=11),
     "template_larger": dict(template_size=(40, 44), seed=5),
     "uint16_frames": dict(frame_dtype=np.uint16, seed=8),
@@ -52,16 +56,25 @@ CASES = {
 @pytest.mark.parametrize("name", list(CASES))
 def test_precision_d_matches_oracle(name):
     kw = dict(CASES[name])
-    if name == "ilu_solver0":
-        pytest.skip("solver 0 (ILU(0) in x|y order) runs on the GPU as the exact solve; compared separately")
     args, _, _ = make_args(**kw)
     _compare_d(args)
 
 
-def test_lambda_regulariser():
+@pytest.mark.parametrize("solver", [0, 2])
+def test_lambda_regulariser(solver):
     args, _, _ = make_args(seed=21)
     args["lambda"] = 50.0
+    args["solver_id"] = solver
     _compare_d(args)
+
+
+def test_ilu_solver0_long_chain_and_precision_s():
+    """ILU(0) (solver id 0) over a chain longer than the exact solve's partitions, in precision D
+    against the oracle, and in precision S within the bound."""
+    args, _, _ = make_args(n_frames=24, nknots=17, seed=62, settings={"gpu_solver_id": 0}, frame_dtype=np.uint16)
+    o, _ = _compare_d(args)
+    g = api.align_group(dict(args, flags="S"))
+    assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([o["dx"], o["dy"]])) <= KNOT_RMS_S
 
 
 def test_flags_history_outputs():
