@@ -151,6 +151,9 @@ typedef struct ss_batch_stats {
    * line-search CTAs, of them with a window, of them on the packed pixel-pair path, and assembly
    * block columns evaluated as pixel pairs */
   int64_t staging[6];
+  /* frame block columns of the last run's assembly passes whose knots were those of their previous
+   * assembly, so they kept its sums and read no frame data */
+  int64_t assembly_columns_kept;
 } ss_batch_stats;
 
 SS_API int ss_batch_create(int32_t n_groups, const ss_inputs* in, ss_outputs* out, ss_batch** batch);

@@ -60,7 +60,8 @@ class SSRecordingOutputs(C.Structure):
 class SSBatchStats(C.Structure):
     _fields_ = [("n_groups", C.c_int32), ("cycles", C.c_int32), ("linesearch_rounds", C.c_int32),
                 ("kernel_launches", C.c_int32), ("frame_passes", C.c_int64 * 4), ("eval_ms", C.c_double * 4),
-                ("arena_bytes", C.c_int64), ("run_ms", C.c_double), ("staging", C.c_int64 * 6)]
+                ("arena_bytes", C.c_int64), ("run_ms", C.c_double), ("staging", C.c_int64 * 6),
+                ("assembly_columns_kept", C.c_int64)]
 
 
 _lib = None

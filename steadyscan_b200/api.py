@@ -387,7 +387,8 @@ class Batch:
                     kernel_launches=st.kernel_launches, frame_passes=list(st.frame_passes),
                     eval_ms=list(st.eval_ms), arena_bytes=st.arena_bytes, run_ms=st.run_ms,
                     staging=dict(zip(("eval_ctas", "eval_windowed", "ls_ctas", "ls_windowed", "ls_pairs",
-                                      "eval_pair_columns"), list(st.staging))))
+                                      "eval_pair_columns"), list(st.staging))),
+                    assembly_columns_kept=int(st.assembly_columns_kept))
 
     @property
     def stream_ptr(self) -> int:

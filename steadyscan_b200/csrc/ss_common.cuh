@@ -51,6 +51,12 @@ enum ColSum : int {
   kCsStride = 16,
 };
 
+// Batch counters of shared-memory staging and column reuse (ss_batch_stats.staging and
+// .assembly_columns_kept): assembly/final CTAs, of them with a template row window, line-search
+// CTAs, of them with a window, of them on the packed pixel-pair path, assembly block columns
+// evaluated as pixel pairs, assembly block columns that kept their sums.
+constexpr int kStagingCounters = 7;
+
 struct GroupCtl {
   int phase, iteration, shift, improved, exec_result;
   int filter_active, filter_kind, filter_id, n_filter_iter;
@@ -93,6 +99,8 @@ struct GroupDesc {
   const float* col_yrange;  // W x 2
   int* err;                 // device error word of the batch (bit 0: a staging copy timed out)
   int pair_ok;              // precision 'S' pixel pairs: affine geometry, Hb % 64 == 0, aligned frames
+  int quad_ok;              // pair_ok with 16-bit frames, knots every 1 or 2 lines, Hb % 256 == 0 and
+                            // 16-byte aligned frames: trial columns by 16-byte loads
   unsigned long long* staging;  // batch counters of shared-memory staging (ss_batch_stats.staging)
   int ls_rounds;            // 1: the line search runs in trial rounds (precision 'S')
   int* ls_max_trials;       // batch: most trials of a frame whose search ended in the current cycle
@@ -107,6 +115,12 @@ struct GroupDesc {
   double *p, *p_last, *p_snap, *delta_p, *ndp;
   double* colsum;           // fW x kCsStride
   int* colcnt;              // fW
+  // Assembly sums kept apart from the other passes' column sums, with the 8 knots each column was
+  // assembled at (mask knots, then difference-image knots): a column whose knots are unchanged at
+  // the next assembly keeps its sums instead of reading its frame again.
+  double* asmsum;           // fW x kCsStride
+  int* asmcnt;              // fW
+  double* asmk;             // fW x 8
   uint8_t *params_used, *blocks_present, *grp_active;
   double* errval;           // 2 nF
   double *kmask, *kdiff;    // nF x 2 x (W+1)

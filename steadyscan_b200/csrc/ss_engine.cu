@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <tuple>
 #include <mutex>
 #include <set>
@@ -266,13 +267,14 @@ static cudaError_t ls_launch(int frames, cudaStream_t s, const GroupDesc* gd, co
   return cudaLaunchKernelEx(&cfg, k_linesearch<Acc, FrameT, TplT>, gd, fg, ctl, win_bytes);
 }
 
-using RoundFn = cudaError_t (*)(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
-                                GroupCtl* ctl, int win_bytes);
+using RoundFn = cudaError_t (*)(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* tsched, int n_frames,
+                                int n_groups, GroupCtl* ctl, int win_bytes);
 
-// One line-search trial round of precision 'S' over the tiles of the round's schedule.
+// One line-search trial round of precision 'S' over the tiles of the round's trial schedule
+// (tsched of a batch of n_frames frames in n_groups groups).
 template <class FrameT, class TplT>
-static cudaError_t round_launch(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* sched, int cap,
-                                GroupCtl* ctl, int win_bytes) {
+static cudaError_t round_launch(int max_tiles, cudaStream_t s, const GroupDesc* gd, int* tsched, int n_frames,
+                                int n_groups, GroupCtl* ctl, int win_bytes) {
   auto* fn = k_trial_round<FrameT, TplT>;
   cudaError_t ae = smem_attr(fn, kTrialWinBytes + 16);
   if (ae != cudaSuccess) return ae;
@@ -281,7 +283,14 @@ static cudaError_t round_launch(int max_tiles, cudaStream_t s, const GroupDesc* 
   const int th = 32 * kEvalWarps;
   const int grid = resident_grid(fn, th, smem, max_tiles);  // cached before any capture
   if (max_tiles <= 0) return cudaSuccess;
-  fn<<<grid, th, smem, s>>>(gd, sched, cap, ctl, win_bytes);
+  fn<<<grid, th, smem, s>>>(gd, tsched, n_frames, n_groups, ctl, win_bytes);
+  return cudaGetLastError();
+}
+
+// The trial schedule of the next round (one CTA).
+static cudaError_t trial_sched_launch(cudaStream_t s, const GroupDesc* gd, const GroupCtl* ctl, const int* frame_group,
+                                      int n_frames, int n_groups, int* tsched) {
+  k_trial_schedule<<<1, kSchedThreads, 0, s>>>(gd, ctl, frame_group, n_frames, n_groups, tsched);
   return cudaGetLastError();
 }
 
@@ -683,16 +692,18 @@ struct Batch::Impl {
   GroupCtl* d_ctl = nullptr;
   int* d_chunk_group = nullptr;  // group of each frame chunk (the schedules' source)
   int* d_sched = nullptr;        // the schedule of the next evaluation launch (ss_sched.cuh)
+  int* d_tsched = nullptr;       // the trial schedule of the next trial round (ss_sched.cuh)
   int* d_frame_group = nullptr;
   int* d_counters = nullptr;  // kCounters run counters (kCtr*)
   int* d_err = nullptr;       // device error word (bit 0: a shared-memory staging copy timed out)
   unsigned long long* d_staging = nullptr;  // staging counters of the run
   double* d_sum_parts = nullptr;            // partial sums of k_sum_image
-  unsigned long long h_staging[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long h_staging[kStagingCounters] = {};
   int win_bytes = 0;          // template window bytes per assembly/final CTA (0: no windows)
   int ls_win_bytes = 0;       // template window bytes per line-search CTA (0: no windows)
   int* h_counters = nullptr;  // pinned
   int n_tiles = 0, n_chunks = 0, n_frames_total = 0;
+  int n_trial_tiles = 0;  // most tiles a trial round can have
   int max_hb = 0;  // largest block height among groups whose geometry k_eval stages in shared memory
   KernelSet ks = {nullptr, nullptr, nullptr};
   SumFn sum = nullptr;
@@ -718,7 +729,10 @@ struct Batch::Impl {
   cudaStream_t cap_stream = nullptr;
 
   void eval_timed(int mode) {
-    if (mode != kTrial || ks.round) sched_launch(mode, stream, d_gd, d_ctl, d_chunk_group, n_chunks, d_sched);
+    if (mode == kTrial && ks.round)
+      trial_sched_launch(stream, d_gd, d_ctl, d_frame_group, n_frames_total, (int)gd.size(), d_tsched);
+    else if (mode != kTrial)
+      sched_launch(mode, stream, d_gd, d_ctl, d_chunk_group, n_chunks, d_sched);
     if (timing) {
       if (event_used + 2 > events.size()) {
         for (int k = 0; k < 64; k++) {
@@ -730,7 +744,8 @@ struct Batch::Impl {
       }
       cudaEventRecord(events[event_used], stream);
     }
-    if (mode == kTrial && ks.round) ks.round(n_tiles, stream, d_gd, d_sched, n_chunks, d_ctl, win_bytes);
+    if (mode == kTrial && ks.round)
+      ks.round(n_trial_tiles, stream, d_gd, d_tsched, n_frames_total, (int)gd.size(), d_ctl, win_bytes);
     else if (mode == kTrial) ks.ls(n_frames_total, stream, d_gd, d_frame_group, d_ctl, ls_win_bytes);
     else ks.eval(mode, n_tiles, stream, d_gd, d_sched, n_chunks, d_ctl, max_hb, win_bytes);
     if (timing) {
@@ -762,13 +777,14 @@ static void layout(Batch::Impl* b, char* base) {
   cv.base = base;
   const size_t tsz = dtype_size(b->tpl_dt);
   b->n_tiles = 0;
+  b->n_trial_tiles = 0;
   b->n_chunks = 0;
   b->n_frames_total = 0;
   std::vector<GroupDesc>& gd = b->gd;
   gd.assign(b->hg.size(), GroupDesc{});
   b->d_err = cv.take<int>(1);
   b->d_counters = cv.take<int>(kCounters);
-  b->d_staging = cv.take<unsigned long long>(6);
+  b->d_staging = cv.take<unsigned long long>(kStagingCounters);
   b->d_sum_parts = cv.take<double>(kSumBlocks);
   b->win_bytes = 0;
   b->ls_win_bytes = 0;
@@ -784,6 +800,7 @@ static void layout(Batch::Impl* b, char* base) {
     G.geo_ax = (float)g.geo_ax; G.geo_bx = (float)g.geo_bx; G.geo_ay = (float)g.geo_ay; G.geo_by = (float)g.geo_by;
     G.geo_fs = (float)g.geo_fs;
     b->n_tiles += g.W * ((g.nF + g.frames_per_cta - 1) / g.frames_per_cta);
+    b->n_trial_tiles += g.W * ((g.nF + kTrialTileFrames - 1) / kTrialTileFrames);
     b->n_chunks += (g.nF + g.frames_per_cta - 1) / g.frames_per_cta;
     if (!(b->compute == 1 && g.geo_k > 0)) b->max_hb = std::max(b->max_hb, g.Hb);  // affine: no tables
     G.frame_base = b->n_frames_total;
@@ -828,6 +845,8 @@ static void layout(Batch::Impl* b, char* base) {
       const size_t fsz = dtype_size(g.frame_dt);
       G.pair_ok = (b->compute == 1 && g.geo_k > 0 && g.Hb % 64 == 0 &&
                    reinterpret_cast<uintptr_t>(G.image) % (2 * fsz) == 0) ? 1 : 0;
+      G.quad_ok = (G.pair_ok && fsz == 2 && g.geo_k <= 2 && g.Hb % 256 == 0 &&
+                   reinterpret_cast<uintptr_t>(G.image) % 16 == 0) ? 1 : 0;
     }
     if (g.tpl_src != -1) {
       const GroupDesc& S = g.tpl_src == kFromSession ? *g.ses_gd : gd[g.tpl_src];
@@ -861,6 +880,9 @@ static void layout(Batch::Impl* b, char* base) {
     G.ndp = cv.take<double>(2 * N);
     G.colsum = cv.take<double>((size_t)g.fW * kCsStride);
     G.colcnt = cv.take<int>(g.fW);
+    G.asmsum = cv.take<double>((size_t)g.fW * kCsStride);
+    G.asmcnt = cv.take<int>(g.fW);
+    G.asmk = cv.take<double>((size_t)g.fW * 8);
     G.params_used = cv.take<uint8_t>(N);
     G.blocks_present = cv.take<uint8_t>(N);
     G.grp_active = cv.take<uint8_t>(2 * (size_t)g.n_rg + 1);
@@ -895,12 +917,13 @@ static void layout(Batch::Impl* b, char* base) {
   b->d_ctl = cv.take<GroupCtl>(gd.size());
   b->d_chunk_group = cv.take<int>(std::max(1, b->n_chunks));
   b->d_sched = cv.take<int>(sched_ints(b->n_chunks));
+  b->d_tsched = cv.take<int>(tsched_ints(b->n_frames_total, (int)gd.size()));
   b->d_frame_group = cv.take<int>(std::max(1, b->n_frames_total));
   b->arena_bytes = cv.off + 256;
 }
 
 int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
-                   const Batch* const* sessions, bool measure_only, void* borrow_stream) {
+                   const Batch* const* sessions, bool measure_only, void* borrow_stream, bool no_wait) {
   Impl* b = d;
   if (n < 1) return fail(SS_ERR_INVALID_ARGUMENT, "no groups");
   b->hg.assign(n, HostGroup{});
@@ -1045,8 +1068,14 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
   SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_chunk_group, chunk_group.data(), chunk_group.size() * 4, cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_frame_group, frame_group.data(), frame_group.size() * 4, cudaMemcpyHostToDevice, s));
-  // pageable sources are staged before the copies return; an own stream is also drained
-  if (b->own_stream) SS_CK(cudaStreamSynchronize(s));
+  // pageable sources are staged before the copies return; an own stream is also drained unless the
+  // caller runs the batch behind its uploads
+  if (b->own_stream && !no_wait) SS_CK(cudaStreamSynchronize(s));
+  return SS_OK;
+}
+
+int Batch::pin() {
+  if (!d->h_counters) SS_CK(cudaHostAlloc(&d->h_counters, (kCounters + 1) * sizeof(int), cudaHostAllocDefault));
   return SS_OK;
 }
 
@@ -1073,6 +1102,7 @@ static int reset_state(Batch::Impl* b) {
     // mask and a zero difference image
     k_fill<<<64, 256, 0, s>>>(G.kmask, nF * 2 * (g.W + 1), NAN);
     k_fill<<<64, 256, 0, s>>>(G.kdiff, nF * 2 * (g.W + 1), NAN);
+    k_fill<<<64, 256, 0, s>>>(G.asmk, (size_t)g.fW * 8, NAN);  // no column keeps sums of an earlier run
     SS_CK(cudaGetLastError());
     GroupCtl& C = b->h_ctl[i];
     std::memset(&C, 0, sizeof(C));
@@ -1096,7 +1126,7 @@ static int reset_state(Batch::Impl* b) {
   SS_CK(cudaMemcpyAsync(b->d_ctl, b->h_ctl.data(), b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemsetAsync(b->d_counters, 0, kCounters * sizeof(int), s));
   SS_CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), s));
-  SS_CK(cudaMemsetAsync(b->d_staging, 0, 6 * sizeof(unsigned long long), s));
+  SS_CK(cudaMemsetAsync(b->d_staging, 0, kStagingCounters * sizeof(unsigned long long), s));
   return SS_OK;
 }
 
@@ -1180,10 +1210,11 @@ constexpr int kGraphRounds = 64;
 // a frame is searching and the cycle is under its round bound. `first` starts the cycle's count.
 __global__ void __launch_bounds__(kSchedThreads) k_sched_rounds(const GroupDesc* __restrict__ gds,
                                                                 const GroupCtl* __restrict__ ctl,
-                                                                const int* __restrict__ chunk_group, int n_chunks,
-                                                                int* __restrict__ sched, int* __restrict__ ctr,
-                                                                int first, cudaGraphConditionalHandle h) {
-  const int tiles = build_schedule<kTrial>(gds, ctl, chunk_group, n_chunks, sched, n_chunks);
+                                                                const int* __restrict__ frame_group, int n_frames,
+                                                                int n_groups, int* __restrict__ tsched,
+                                                                int* __restrict__ ctr, int first,
+                                                                cudaGraphConditionalHandle h) {
+  const int tiles = build_trial_schedule(gds, ctl, frame_group, n_frames, n_groups, tsched);
   if (threadIdx.x == 0) {
     if (first) ctr[kCtrRound] = 0;
     const bool more = tiles > 0 && ctr[kCtrRound] < kGraphRounds;
@@ -1231,7 +1262,9 @@ static int capture_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph
 static int prime_attributes(Batch::Impl* b) {
   SS_CK(smem_attr(k_solve_system, (int)kSolveSmem));
   SS_CK(b->ks.eval(kAssemble, 0, b->stream, b->d_gd, b->d_sched, b->n_chunks, b->d_ctl, b->max_hb, b->win_bytes));
-  if (b->ks.round) SS_CK(b->ks.round(0, b->stream, b->d_gd, b->d_sched, b->n_chunks, b->d_ctl, b->win_bytes));
+  if (b->ks.round)
+    SS_CK(b->ks.round(0, b->stream, b->d_gd, b->d_tsched, b->n_frames_total, (int)b->gd.size(), b->d_ctl,
+                      b->win_bytes));
   else SS_CK(b->ks.ls(0, b->stream, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes));
   return SS_OK;
 }
@@ -1273,7 +1306,8 @@ static int build_run_graph(Batch::Impl* b) {
   b->ks.eval(kAssemble, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
   solve_launch(s, b->d_gd, b->d_ctl, nG);
   if (b->ks.round) {
-    k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc, b->d_counters, 1, h_round);
+    k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_frame_group, b->n_frames_total, nG,
+                                               b->d_tsched, b->d_counters, 1, h_round);
     rc = capture_while(s, h_round, &rounds_body);
     if (!rc) {
       sched_launch(kCorr, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
@@ -1295,8 +1329,9 @@ static int build_run_graph(Batch::Impl* b) {
   // one trial round
   if (b->ks.round) {
     SS_CK(cudaStreamBeginCaptureToGraph(s, rounds_body, nullptr, nullptr, 0, mode));
-    b->ks.round(b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->win_bytes);
-    k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc, b->d_counters, 0, h_round);
+    b->ks.round(b->n_trial_tiles, s, b->d_gd, b->d_tsched, b->n_frames_total, nG, b->d_ctl, b->win_bytes);
+    k_sched_rounds<<<1, kSchedThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_frame_group, b->n_frames_total, nG,
+                                               b->d_tsched, b->d_counters, 0, h_round);
     e = cudaStreamEndCapture(s, &out);
     if (e != cudaSuccess) return fail(SS_ERR_CUDA, std::string("run graph rounds: ") + cudaGetErrorString(e));
   }
@@ -1439,6 +1474,7 @@ void Batch::stats(ss_batch_stats* st) const {
   st->arena_bytes = (int64_t)d->arena_bytes;
   st->run_ms = d->run_ms;
   for (int i = 0; i < 6; i++) st->staging[i] = (int64_t)d->h_staging[i];
+  st->assembly_columns_kept = (int64_t)d->h_staging[6];
 }
 
 int Batch::collect() {
@@ -1492,7 +1528,7 @@ struct Server::Impl {
     Batch* batch = nullptr;  // the group's buffers (its arena) and host metadata
     bool active = false;
     bool joining = false;    // admitted since the last cycle was launched
-    int tiles = 0, chunks = 0, frames = 0;
+    int tiles = 0, chunks = 0, frames = 0, trial_tiles = 0;
     GroupCtl init;           // initial control state, uploaded when the slot joins
   };
   int device = 0, capacity = 0;
@@ -1510,8 +1546,9 @@ struct Server::Impl {
   GroupCtl* d_ctl = nullptr;
   int* d_chunk_group = nullptr;
   int* d_sched = nullptr;
+  int* d_tsched = nullptr;
   int* d_frame_group = nullptr;
-  int chunk_cap = 0, frame_cap = 0, n_tiles = 0, n_chunks = 0, n_frames = 0;
+  int chunk_cap = 0, frame_cap = 0, n_tiles = 0, n_chunks = 0, n_frames = 0, n_trial_tiles = 0;
   std::vector<int> cg, fg;
   int* d_counters = nullptr;  // [0] most trials of a search that ended in the cycle, [1] finished groups
   int* h_counters = nullptr;  // pinned
@@ -1539,6 +1576,7 @@ Server::~Server() {
   cudaFree(v->d_ctl);
   cudaFree(v->d_chunk_group);
   cudaFree(v->d_sched);
+  cudaFree(v->d_tsched);
   cudaFree(v->d_frame_group);
   cudaFree(v->d_counters);
   cudaFree(v->d_err);
@@ -1570,10 +1608,10 @@ int Server::create(int capacity, int device) {
   SS_CK(cudaMalloc(&v->d_ctl, capacity * sizeof(GroupCtl)));
   SS_CK(cudaMalloc(&v->d_counters, 4 * sizeof(int)));
   SS_CK(cudaMalloc(&v->d_err, sizeof(int)));
-  SS_CK(cudaMalloc(&v->d_staging, 6 * sizeof(unsigned long long)));
+  SS_CK(cudaMalloc(&v->d_staging, kStagingCounters * sizeof(unsigned long long)));
   SS_CK(cudaMemset(v->d_counters, 0, 4 * sizeof(int)));
   SS_CK(cudaMemset(v->d_err, 0, sizeof(int)));
-  SS_CK(cudaMemset(v->d_staging, 0, 6 * sizeof(unsigned long long)));
+  SS_CK(cudaMemset(v->d_staging, 0, kStagingCounters * sizeof(unsigned long long)));
   // empty slots are in the done phase: every kernel passes them by
   for (int k = 0; k < capacity; k++) {
     std::memset(&v->h_ctl[k], 0, sizeof(GroupCtl));
@@ -1625,6 +1663,7 @@ int Server::admit(const ss_inputs* in, ss_outputs* out, const Batch* session, vo
   const HostGroup& g = bi->hg[0];
   sl.chunks = (g.nF + g.frames_per_cta - 1) / g.frames_per_cta;
   sl.tiles = g.W * sl.chunks;
+  sl.trial_tiles = g.W * ((g.nF + kTrialTileFrames - 1) / kTrialTileFrames);
   sl.frames = g.nF;
   GroupDesc G = bi->gd[0];
   G.err = v->d_err;
@@ -1641,6 +1680,7 @@ int Server::admit(const ss_inputs* in, ss_outputs* out, const Batch* session, vo
 static int server_tables(Server::Impl* v) {
   cudaStream_t s = v->stream;
   v->n_tiles = 0;
+  v->n_trial_tiles = 0;
   v->n_chunks = 0;
   v->n_frames = 0;
   for (int k = 0; k < v->capacity; k++) {
@@ -1649,6 +1689,7 @@ static int server_tables(Server::Impl* v) {
     v->h_gd[k].chunk_base = v->n_chunks;
     v->h_gd[k].frame_base = v->n_frames;
     v->n_tiles += sl.tiles;
+    v->n_trial_tiles += sl.trial_tiles;
     v->n_chunks += sl.chunks;
     v->n_frames += sl.frames;
   }
@@ -1656,11 +1697,13 @@ static int server_tables(Server::Impl* v) {
     SS_CK(cudaStreamSynchronize(s));
     cudaFree(v->d_chunk_group);
     cudaFree(v->d_sched);
+    cudaFree(v->d_tsched);
     cudaFree(v->d_frame_group);
     v->chunk_cap = std::max(2 * v->chunk_cap, v->n_chunks);
     v->frame_cap = std::max(2 * v->frame_cap, v->n_frames);
     SS_CK(cudaMalloc(&v->d_chunk_group, (size_t)v->chunk_cap * sizeof(int)));
     SS_CK(cudaMalloc(&v->d_sched, sched_ints(v->chunk_cap) * sizeof(int)));
+    SS_CK(cudaMalloc(&v->d_tsched, tsched_ints(v->frame_cap, v->capacity) * sizeof(int)));
     SS_CK(cudaMalloc(&v->d_frame_group, (size_t)v->frame_cap * sizeof(int)));
   }
   v->cg.assign(std::max(1, v->n_chunks), 0);
@@ -1711,8 +1754,8 @@ int Server::step() {
   if (v->ks.round) {
     SS_CK(cudaMemsetAsync(v->d_counters, 0, sizeof(int), s));
     for (int r = 0; r < v->cur_rounds; r++) {
-      sched_launch(kTrial, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
-      v->ks.round(v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->win_bytes);
+      trial_sched_launch(s, v->d_gd, v->d_ctl, v->d_frame_group, v->n_frames, nG, v->d_tsched);
+      v->ks.round(v->n_trial_tiles, s, v->d_gd, v->d_tsched, v->n_frames, nG, v->d_ctl, v->win_bytes);
     }
     sched_launch(kCorr, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);
     v->ks.eval(kCorr, v->n_tiles, s, v->d_gd, sc, nc, v->d_ctl, v->max_hb, v->win_bytes);
@@ -1868,6 +1911,88 @@ int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out) {
   return SS_OK;
 }
 
+// ss_align_groups for groups whose frames are in host memory: the groups are split into up to
+// kPipelineParts consecutive parts of about equal frame counts, each a batch on its own stream in
+// one device allocation. Every part's uploads are queued first, then every part's run is launched
+// behind its own uploads, so the copies of the later parts overlap the runs of the earlier ones and
+// the runs overlap each other. A group's result does not depend on the other groups of its batch,
+// so it is the one of a single batch.
+constexpr int kPipelineParts = 4;
+
+int align_groups_pipelined(int n, const ss_inputs* in, ss_outputs* out) {
+  long long total = 0;
+  for (int i = 0; i < n; i++) total += in[i].n_frames;
+  const int parts = std::min(n, kPipelineParts);
+  std::vector<int> start(parts + 1, n);
+  {
+    long long acc = 0;
+    int k = 0;
+    start[0] = 0;
+    for (int i = 0; i < n && k + 1 < parts; i++) {
+      acc += in[i].n_frames;
+      if (acc * parts >= total * (k + 1) && i + 1 < n) start[++k] = i + 1;
+    }
+    for (int j = k + 1; j <= parts; j++) start[j] = n;
+  }
+  std::vector<std::unique_ptr<Batch>> bs;
+  std::vector<size_t> bytes;
+  size_t sum = 0;
+  for (int k = 0; k < parts; k++) {
+    const int a = start[k], m = start[k + 1] - start[k];
+    if (m <= 0) continue;
+    Batch meas;
+    int rc = meas.prepare(m, in + a, out ? out + a : nullptr, nullptr, 0, nullptr, true);
+    if (rc) return rc;
+    const size_t nb = (meas.arena_bytes() + 255) & ~size_t(255);
+    bytes.push_back(nb);
+    sum += nb;
+    bs.emplace_back(new Batch);
+  }
+  int dev = in[0].gpu_device_id, ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
+  if (dev < 0 || dev >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
+  SS_CK(cudaSetDevice(dev));
+  char* arena = nullptr;
+  SS_CK(cudaMalloc(&arena, sum));
+  struct Free {
+    std::vector<std::unique_ptr<Batch>>* b;
+    char* p;
+    ~Free() {
+      b->clear();  // batches drain their streams first
+      cudaFree(p);
+    }
+  } guard{&bs, arena};
+  // every part's uploads, then every part's run behind them
+  size_t off = 0;
+  for (size_t k = 0, a = 0; k < bs.size(); k++) {
+    while (start[a + 1] - start[a] <= 0) a++;
+    const int first = start[a], m = start[a + 1] - start[a];
+    a++;
+    int rc = bs[k]->prepare(m, in + first, out ? out + first : nullptr, arena + off, bytes[k], nullptr, false,
+                            nullptr, true);
+    if (!rc) rc = bs[k]->pin();
+    if (rc) return rc;
+    off += bytes[k];
+  }
+  for (auto& b : bs) {
+    int rc = b->start();
+    if (!rc) rc = b->step();
+    if (rc) return rc;
+  }
+  for (auto& b : bs) {
+    for (;;) {
+      SS_CK(cudaStreamSynchronize(static_cast<cudaStream_t>(b->stream())));
+      int rc = b->poll();
+      if (rc < 0) return rc;
+      if (rc == 2) break;
+      if ((rc = b->step())) return rc;  // host-launched cycles (timing on) need the next one
+    }
+    int rc = b->collect();
+    if (rc) return rc;
+  }
+  return SS_OK;
+}
+
 int Batch::cycles() const { return d->cycles; }
 int Batch::rounds() const { return d->rounds; }
 int Batch::n_groups() const { return (int)d->gd.size(); }
@@ -1884,12 +2009,17 @@ extern "C" {
 int ss_align_groups(int32_t n_groups, const ss_inputs* in, ss_outputs* out) {
   auto t0 = std::chrono::steady_clock::now();
   if (!in || n_groups < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "no groups");
-  ss::Batch b;
-  int rc = b.prepare(n_groups, in, out, nullptr, 0);
-  if (rc) return rc;
-  rc = b.run();
-  if (rc) return rc;
-  rc = b.collect();
+  int rc = SS_OK;
+  bool host_frames = n_groups >= 2;
+  for (int i = 0; i < n_groups && host_frames; i++) host_frames = in[i].bm_data.location == SS_HOST;
+  if (host_frames) {
+    rc = ss::align_groups_pipelined(n_groups, in, out);
+  } else {
+    ss::Batch b;
+    rc = b.prepare(n_groups, in, out, nullptr, 0);
+    if (!rc) rc = b.run();
+    if (!rc) rc = b.collect();
+  }
   if (rc) return rc;
   double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (out)

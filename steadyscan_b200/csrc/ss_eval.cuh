@@ -436,6 +436,22 @@ __host__ __device__ constexpr size_t stage_bytes(int hb) {
   return ((size_t)hb * (4 * sizeof(Acc) + 1) + 15) & ~(size_t)15;
 }
 
+// Knots of block column cc of frame f in the assembly pass: the mask knots (p) and the knots of the
+// difference image (p, or the stale kdiff of a frame that is not active in this half-step).
+__device__ __forceinline__ void assembly_knots(const GroupDesc& G, int f, int cc, int shift, double (&k)[8]) {
+  const int W = G.W, N = G.N, c = f * W + cc;
+  k[0] = G.p[c];
+  k[1] = G.p[c + 1];
+  k[2] = G.p[N + c];
+  k[3] = G.p[N + c + 1];
+  if (frame_active(G, f, shift)) {
+    k[4] = k[0]; k[5] = k[1]; k[6] = k[2]; k[7] = k[3];
+  } else {
+    const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
+    k[4] = kd[cc]; k[5] = kd[cc + 1]; k[6] = kd[W + 1 + cc]; k[7] = kd[W + 1 + cc + 1];
+  }
+}
+
 // Assembly (at p), correlation and final (at kmask) passes of one tile: block column cc of one group
 // and frames fb*fpc .. of its chunk fb, a warp per frame at a time; the column's geometry is staged in
 // shared memory once for all of them (at smem), and the frames share the template rows around the
@@ -447,6 +463,38 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
   if (!group_has_work<MODE>(C)) return;
   const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
   const int warp = threadIdx.x >> 5;
+  const int f0 = fb * fpc;
+
+  // assembly: the frames of the tile whose column knots differ from those of the column's last
+  // assembly (bit f - f0); the others keep their sums (the same knots give the same sums)
+  unsigned long long need = ~0ull;
+  if (MODE == kAssemble) {
+    __shared__ unsigned long long s_need;
+    const int lane = threadIdx.x & 31, fe = min(G.nF, f0 + fpc);
+    if (warp == 0) {
+      unsigned long long m = 0;
+      for (int fa = f0; fa < fe; fa += 32) {
+        const int f = fa + lane;
+        bool changed = false;
+        if (f < fe) {
+          double k[8];
+          assembly_knots(G, f, cc, C.shift, k);
+          const double* prev = G.asmk + (size_t)(f * W + cc) * 8;
+#pragma unroll
+          for (int i = 0; i < 8; i++) changed |= __double_as_longlong(k[i]) != __double_as_longlong(prev[i]);
+        }
+        m |= (unsigned long long)__ballot_sync(0xffffffffu, changed) << (fa - f0);
+      }
+      if (lane == 0) {
+        s_need = m;
+        const int kept = (fe - f0) - __popcll(m);
+        if (kept) atomicAdd(G.staging + 6, (unsigned long long)kept);
+      }
+    }
+    __syncthreads();
+    need = s_need;
+    if (need == 0) return;  // uniform over the CTA
+  }
 
   ColGeo<Acc> geo = global_geo<Acc>(G, cc);
   const bool affine = sizeof(Acc) == 4 && G.geo_k > 0;
@@ -517,14 +565,11 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
   for (int f = fb * fpc + warp; f < f_end; f += kEvalWarps) {
     const int c = f * W + cc;
     ColKnots<Acc> k;
+    double ka[8];
     if (MODE == kAssemble) {
-      const double ax0 = G.p[c], ax1 = G.p[c + 1], ay0 = G.p[N + c], ay1 = G.p[N + c + 1];
-      if (frame_active(G, f, C.shift)) {
-        set_knots(k, ax0, ax1, ay0, ay1, ax0, ax1, ay0, ay1);
-      } else {  // the difference image of an inactive frame is stale
-        const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
-        set_knots(k, ax0, ax1, ay0, ay1, kd[cc], kd[cc + 1], kd[W + 1 + cc], kd[W + 1 + cc + 1]);
-      }
+      if (!((need >> (f - f0)) & 1ull)) continue;
+      assembly_knots(G, f, cc, C.shift, ka);  // (the difference image of an inactive frame is stale)
+      set_knots(k, ka[0], ka[1], ka[2], ka[3], ka[4], ka[5], ka[6], ka[7]);
     } else {
       const double* km = G.kmask + (size_t)f * 2 * (W + 1);
       const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
@@ -552,10 +597,16 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
       eval_column<Acc, FrameT, TplT, MODE>(G, coli, geo, k, out, cnt, mo);
     }
     if ((threadIdx.x & 31) == 0) {
-      double* dst = G.colsum + (size_t)c * kCsStride;
+      double* dst = (MODE == kAssemble ? G.asmsum : G.colsum) + (size_t)c * kCsStride;
 #pragma unroll
       for (int i = 0; i < nsums(MODE); i++) dst[i] = out[i];
-      G.colcnt[c] = cnt;
+      if (MODE == kAssemble) {
+        G.asmcnt[c] = cnt;
+#pragma unroll
+        for (int i = 0; i < 8; i++) G.asmk[(size_t)c * 8 + i] = ka[i];
+      } else {
+        G.colcnt[c] = cnt;
+      }
     }
   }
 }
@@ -984,35 +1035,20 @@ __device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f
   }
 }
 
-// One trial of the line search for the searching frames of one tile (block column cc of frame chunk
-// fb); the last column of a frame to arrive decides for the frame (ls_decide).
+// One trial of the line search for the frames of one trial tile: block column cc of the ns <= 8
+// searching frames listed at list[pos..pos+ns) (batch frame indices, ss_sched.cuh); the last column
+// of a frame to arrive decides for the frame (ls_decide).
 template <class FrameT, class TplT>
-__device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int cc, int fb, unsigned char* smem,
-                                           uint64_t* bar, unsigned& bar_phase, bool& win_ok, int win_bytes,
-                                           int* s_list, int& s_n, float4* s_kn) {
-  // ls_pending falls while the round runs: one decision for the whole CTA (0 means every frame of
-  // the group has finished)
-  if (!__syncthreads_and(C.phase == kPhHalf && C.ls_state == 1 && *(volatile int*)&C.ls_pending > 0)) return;
-  const int W = G.W, N = G.N, Hb = G.Hb, fpc = G.frames_per_cta;
+__device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int cc, int pos, int ns,
+                                           const int* __restrict__ list, unsigned char* smem, uint64_t* bar,
+                                           unsigned& bar_phase, bool& win_ok, int win_bytes, int* s_list,
+                                           float4* s_kn) {
+  const int W = G.W, N = G.N, Hb = G.Hb;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int f0 = fb * fpc, f_end = min(G.nF, f0 + fpc);
-
-  // the chunk's searching frames; fstate of a frame changes only in its decision, which follows
-  // the evaluation of all its columns of the round
-  if (warp == 0) {
-    int n = 0;
-    for (int fa = f0; fa < f_end; fa += 32) {
-      const int f = fa + lane;
-      const bool s = f < f_end && (G.fstate[f] & 2);
-      const unsigned bal = __ballot_sync(0xffffffffu, s);
-      if (s) s_list[n + __popc(bal & ((1u << lane) - 1u))] = f;
-      n += __popc(bal);
-    }
-    if (lane == 0) s_n = n;
-  }
+  // the tile's frames (searching when the round's schedule was built; a frame's fstate changes only
+  // in its decision, which follows the evaluation of all its columns of the round)
+  if (threadIdx.x < ns) s_list[threadIdx.x] = list[pos + threadIdx.x] - G.frame_base;
   __syncthreads();
-  const int ns = s_n;
-  if (ns == 0) return;
 
   // trial knots of this column: own knots p + deltaP, the frame's right boundary fixed
   auto knots = [&](int f, float& x0, float& x1, float& y0, float& y1) {
@@ -1071,7 +1107,12 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     const float x0 = kn.x, x1 = kn.y, y0 = kn.z, y1 = kn.w;
     double ssd;
     int cnt;
-    if (win.p && G.pair_ok) {
+    bool quads = false;
+    if constexpr (sizeof(FrameT) == 2) quads = win.p && G.quad_ok;
+    if (quads) {
+      if constexpr (sizeof(FrameT) == 2)
+        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane), pair_win(win), ssd, cnt);
+    } else if (win.p && G.pair_ok) {
       trial_pairs<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(win), ssd, cnt);
     } else {
       ColKnots<float> k;
@@ -1104,29 +1145,30 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
   }
 }
 
-// One line-search trial round of precision 'S' over the tiles of the round's schedule (the chunks
-// with a searching frame), one tile at a time per CTA. Dynamic shared memory: the window's mbarrier
-// (16 bytes), then the template window.
+// One line-search trial round of precision 'S' over the tiles of the round's trial schedule (the
+// searching frames, ss_sched.cuh), one tile at a time per CTA. Dynamic shared memory: the window's
+// mbarrier (16 bytes), then the template window.
 template <class FrameT, class TplT>
 __global__ void __launch_bounds__(32 * kEvalWarps, kTrialMinBlocks)
-    k_trial_round(const GroupDesc* __restrict__ gds, int* __restrict__ sched, int cap, GroupCtl* __restrict__ ctl,
-                  int win_bytes) {
+    k_trial_round(const GroupDesc* __restrict__ gds, int* __restrict__ ts, int n_frames, int n_groups,
+                  GroupCtl* __restrict__ ctl, int win_bytes) {
+  static_assert(kTrialTileFrames <= kEvalWarps * 32, "one thread per tile frame");
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_list[kMaxChunk];
-  __shared__ float4 s_kn[kMaxChunk];
-  __shared__ int s_n;
-  __shared__ int s_tile[3];
+  __shared__ int s_list[kTrialTileFrames];
+  __shared__ float4 s_kn[kTrialTileFrames];
+  __shared__ int s_tile[4];
   __shared__ GroupDesc s_gd;
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   if (threadIdx.x == 0) mbar_init(bar);
   __syncthreads();
   unsigned bar_phase = 0;
   bool win_ok = true;
-  while (fetch_tile(sched, cap, s_tile)) {
+  const int* list = ts + kTsHdr;
+  while (fetch_trial_tile(ts, n_frames, n_groups, s_tile)) {
     const int g = s_tile[0];
     load_desc(gds + g, &s_gd);
-    trial_tile<FrameT, TplT>(s_gd, ctl[g], s_tile[1], s_tile[2], smem + 16, bar, bar_phase, win_ok, win_bytes,
-                             s_list, s_n, s_kn);
+    trial_tile<FrameT, TplT>(s_gd, ctl[g], s_tile[1], s_tile[2], s_tile[3], list, smem + 16, bar, bar_phase, win_ok,
+                             win_bytes, s_list, s_kn);
     __syncthreads();  // s_tile, s_gd, s_list, s_kn and the window are reused by the next tile
   }
   if (!win_ok) drain_window(bar, bar_phase);  // a timed-out copy may still write this CTA's memory

@@ -434,11 +434,11 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_prep(const GroupDes
   const int W = G.W, N = G.N, nF = G.nF, fW = G.fW, shift = C.shift;
   // a column's block is present with enough valid pixels; a knot is used when a block next to it is
   for (int c = gt; c < fW; c += gn) {
-    const bool present = G.colcnt[c] >= G.min_points[c % W];
+    const bool present = G.asmcnt[c] >= G.min_points[c % W];
     G.blocks_present[c] = present;
     const int f = c / W;
     if (!frame_active(G, f, shift)) continue;
-    const bool before = c > 0 && G.colcnt[c - 1] >= G.min_points[(c - 1) % W];
+    const bool before = c > 0 && G.asmcnt[c - 1] >= G.min_points[(c - 1) % W];
     G.params_used[c] = present || before;
   }
   if (gt == 0) G.blocks_present[N - 1] = 0;
@@ -470,8 +470,8 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_prep(const GroupDes
       double e = 0, rg = 0;
       int n = 0;
       for (int cc = lane; cc < W; cc += 32) {
-        e += G.colsum[(size_t)(f * W + cc) * kCsStride + kCsSsd];
-        n += G.colcnt[f * W + cc];
+        e += G.asmsum[(size_t)(f * W + cc) * kCsStride + kCsSsd];
+        n += G.asmcnt[f * W + cc];
         if (G.lambda != 0.0) {  // knot-difference regulariser (extension); the right boundary is ks[W]
           const double dx = ks[cc + 1] - ks[cc], dy = ks[N + cc + 1] - ks[N + cc];
           rg += dx * dx + dy * dy;
@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_planes(const GroupD
       double d0 = 0, d1 = 0, d2 = 0, r0 = 0, r1 = 0;
       double2 o78 = make_double2(0, 0), o9 = make_double2(0, 0);
       if (k < fW) {
-        const double2* a = reinterpret_cast<const double2*>(G.colsum + (size_t)k * kCsStride);
+        const double2* a = reinterpret_cast<const double2*>(G.asmsum + (size_t)k * kCsStride);
         const double2 v01 = a[0], v23 = a[1], v1011 = a[5];
         o78 = a[3];
         o9 = a[4];
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_planes(const GroupD
         r0 += v1011.x; r1 += v1011.y;            // kCsJ1x kCsJ1y
       }
       if (k > 0) {
-        const double2* b = reinterpret_cast<const double2*>(G.colsum + (size_t)(k - 1) * kCsStride);
+        const double2* b = reinterpret_cast<const double2*>(G.asmsum + (size_t)(k - 1) * kCsStride);
         const double2 v45 = b[2], v67 = b[3], v1213 = b[6];
         d0 += v45.x; d1 += v45.y; d2 += v67.x;   // kCsBxx kCsByy kCsBxy
         r0 += v1213.x; r1 += v1213.y;            // kCsJ2x kCsJ2y

@@ -81,10 +81,12 @@ struct PairCol {
   float dj;                 // j advance per step (64 / k)
 };
 
-// Column constants for knots (kx0, kx1, ky0, ky1) of block column cc (lane-dependent halves).
-__device__ __forceinline__ PairCol pair_col(const GroupDesc& G, int cc, float kx0, float kx1, float ky0, float ky1) {
+// Column constants for knots (kx0, kx1, ky0, ky1) of block column cc (lane-dependent halves); the
+// lane's first pair holds rows row0 and row0 + 1 (default 2 lane).
+__device__ __forceinline__ PairCol pair_col(const GroupDesc& G, int cc, float kx0, float kx1, float ky0, float ky1,
+                                            int row0 = -1) {
   const int lane = threadIdx.x & 31, k = G.geo_k, L = G.geo_L, ks = __ffs(k) - 1;  // k = 2^ks
-  const int rA = 2 * lane, rB = 2 * lane + 1;
+  const int rA = row0 >= 0 ? row0 : 2 * lane, rB = rA + 1;
   const int lA = rA & (k - 1), lB = rB & (k - 1);
   const float fs = G.geo_fs;
   const float f0A = ((float)(lA * L) + 0.5f) * fs, f0B = ((float)(lB * L) + 0.5f) * fs;
@@ -250,6 +252,59 @@ __device__ __forceinline__ void trial_pairs(const GroupDesc& G, size_t coli, con
       float2 d2 = sub2(PL::cvt(cur), wI);
       d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
       ssd = fma2(d2, d2, ssd);
+    }
+  }
+  cnt_out = warp_sum(cnt);
+  ssd_out = (double)warp_sumf(ssd.x + ssd.y);
+}
+
+// trial_pairs for 16-bit frame samples with knots every 1 or 2 lines, Hb a multiple of 256 and a
+// 16-byte aligned column: each lane loads rows 8 lane .. 8 lane + 7 of every 256-row step as one
+// 16-byte load (four pixel pairs), two steps ahead (the trial kernel's 64 registers hold no more). The lane's pairs keep the line offsets of rows 8 lane and 8 lane + 1 (k <= 2),
+// so pc is pair_col's with its first row at 8 lane; pair m of step t sits at j0 + m (2 >> ks) +
+// t (256 >> ks). Same arithmetic per pixel as trial_pairs.
+template <class FrameT>
+__device__ __forceinline__ void trial_pairs16(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
+                                              double& ssd_out, int& cnt_out) {
+  static_assert(sizeof(FrameT) == 2, "16-bit frame samples");
+  using PL = PairLoad<FrameT>;
+  const int lane = threadIdx.x & 31;
+  const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
+  const uint4* col = reinterpret_cast<const uint4*>(reinterpret_cast<const FrameT*>(G.image) + coli);
+  const int steps = G.Hb >> 8;
+  const int ks = __ffs(G.geo_k) - 1;
+  const float dm = (float)(2 >> ks), dt = (float)(256 >> ks);
+  float2 ssd = f2(0.f);
+  int cnt = 0;
+  constexpr int kPf = 2;
+  uint4 ring[kPf];
+#pragma unroll
+  for (int d = 0; d < kPf; d++) ring[d] = d < steps ? __ldg(col + d * 32 + lane) : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll 1
+  for (int t0 = 0; t0 < steps; t0 += kPf) {
+#pragma unroll
+    for (int d = 0; d < kPf; d++) {
+      const int t = t0 + d;
+      if (t >= steps) break;
+      const uint4 cur = ring[d];
+      if (t + kPf < steps) ring[d] = __ldg(col + (t + kPf) * 32 + lane);
+      const float2 jb = add2(pc.j0, f2(dt * (float)t));
+      const uint32_t wv[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        const float2 j = add2(jb, f2(dm * (float)m));
+        const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
+        const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+        const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+        cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+        float2 xf, yf, t00, t01, t10, t11;
+        pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+        const float2 a = fma2(yf, sub2(t10, t00), t00), b = fma2(yf, sub2(t11, t01), t01);
+        const float2 wI = fma2(xf, sub2(b, a), a);
+        float2 d2 = sub2(PL::cvt(wv[m]), wI);
+        d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
+        ssd = fma2(d2, d2, ssd);
+      }
     }
   }
   cnt_out = warp_sum(cnt);

@@ -68,6 +68,24 @@ def test_lambda_regulariser(solver):
     _compare_d(args)
 
 
+@pytest.mark.parametrize("flags", ["D", "S"])
+def test_assembly_keeps_columns_with_unchanged_knots(flags):
+    """Block columns whose knots did not move since their last assembly keep its sums instead of
+    reading the frame again; the run still matches the oracle (D) or the bound (S)."""
+    args, _, _ = make_args(n_frames=8, seed=23, frame_dtype=np.uint16)
+    o = oracle.align_group(args)
+    b = api.Batch([dict(args, flags=flags)], want_mask=True)
+    b.run()
+    g = b.collect()[0]
+    st = b.stats()
+    b.close()
+    assert st["assembly_columns_kept"] > 0
+    if flags == "D":
+        _compare_d(args, o=o, g=g)
+    else:
+        assert knot_rms(np.concatenate([g["dx"], g["dy"]]), np.concatenate([o["dx"], o["dy"]])) <= KNOT_RMS_S
+
+
 def test_ilu_solver0_long_chain_and_precision_s():
     """ILU(0) (solver id 0) over a chain longer than the exact solve's partitions, in precision D
     against the oracle, and in precision S within the bound."""
