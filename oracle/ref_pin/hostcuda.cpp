@@ -1,0 +1,240 @@
+// Host implementations of the CUDA runtime, cuSPARSE and cuSOLVER entry points that the reference's
+// task layer calls, and the cooperative-fiber block emulation behind SS_LAUNCH: TEST INFRASTRUCTURE
+// ONLY (see hostcuda.h). Device memory is host memory; cudaMalloc returns zero-filled memory, as
+// fresh device memory reads on the GPUs the reference targets (its buffers are filled where it
+// relies on a value; the one buffer it reads unwritten, paramsUsed[N-1], then reads as zero).
+#include "hostcuda.h"
+
+#include <cusolverSp.h>
+#include <cusparse.h>
+#include <ucontext.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+ss_dim3 ss_threadIdx, ss_blockIdx, ss_blockDim, ss_gridDim;
+alignas(16) char s_mem[1 << 20];
+
+// ---------------------------------------------------------------------------------------------
+// blocks as cooperative fibers
+
+namespace {
+
+constexpr size_t kStack = 256 * 1024;
+
+struct Fiber {
+  ucontext_t ctx;
+  std::vector<char> stack;
+  bool done = false;
+  unsigned tid = 0;
+};
+
+ucontext_t g_sched;
+Fiber* g_cur = nullptr;
+const std::function<void()>* g_body = nullptr;
+std::vector<Fiber> g_pool;
+
+void fiber_main() {
+  (*g_body)();
+  g_cur->done = true;
+  swapcontext(&g_cur->ctx, &g_sched);
+}
+
+}  // namespace
+
+void ss_syncthreads() {
+  if (!g_cur) return;  // host code outside a launch
+  swapcontext(&g_cur->ctx, &g_sched);
+}
+
+void ss_lockstep_point() { ss_syncthreads(); }
+
+void ss_launch(ss_dim3 g, ss_dim3 b, const std::function<void()>& body) {
+  const unsigned nb = g.x * g.y * g.z, nt = b.x * b.y * b.z;
+  ss_gridDim = g;
+  ss_blockDim = b;
+  if (g_pool.size() < nt) g_pool.resize(nt);
+  for (unsigned blk = 0; blk < nb; blk++) {
+    ss_blockIdx = ss_dim3{blk % g.x, (blk / g.x) % g.y, blk / (g.x * g.y)};
+    g_body = &body;
+    for (unsigned t = 0; t < nt; t++) {
+      Fiber& f = g_pool[t];
+      if (f.stack.size() < kStack) f.stack.resize(kStack);
+      getcontext(&f.ctx);
+      f.ctx.uc_stack.ss_sp = f.stack.data();
+      f.ctx.uc_stack.ss_size = f.stack.size();
+      f.ctx.uc_link = nullptr;
+      f.done = false;
+      f.tid = t;
+      makecontext(&f.ctx, fiber_main, 0);
+    }
+    // rounds: every live thread runs to its next barrier (or its end), in thread order
+    for (bool live = true; live;) {
+      live = false;
+      for (unsigned t = 0; t < nt; t++) {
+        Fiber& f = g_pool[t];
+        if (f.done) continue;
+        ss_threadIdx = ss_dim3{t % b.x, (t / b.x) % b.y, t / (b.x * b.y)};
+        g_cur = &f;
+        swapcontext(&g_sched, &f.ctx);
+        g_cur = nullptr;
+        live |= !f.done;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// runtime
+
+extern "C" {
+
+cudaError_t cudaMalloc(void** p, size_t n) {
+  *p = std::calloc(n ? n : 1, 1);
+  return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+cudaError_t cudaFree(void* p) {
+  std::free(p);
+  return cudaSuccess;
+}
+cudaError_t cudaHostAlloc(void** p, size_t n, unsigned int) { return cudaMalloc(p, n); }
+cudaError_t cudaMallocHost(void** p, size_t n) { return cudaMalloc(p, n); }
+cudaError_t cudaFreeHost(void* p) { return cudaFree(p); }
+cudaError_t cudaHostRegister(void*, size_t, unsigned int) { return cudaSuccess; }
+cudaError_t cudaHostUnregister(void*) { return cudaSuccess; }
+cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) {
+  std::memmove(d, s, n);
+  return cudaSuccess;
+}
+cudaError_t cudaMemset(void* d, int v, size_t n) {
+  std::memset(d, v, n);
+  return cudaSuccess;
+}
+cudaError_t cudaDeviceSynchronize(void) { return cudaSuccess; }
+cudaError_t cudaDeviceReset(void) { return cudaSuccess; }
+cudaError_t cudaSetDevice(int) { return cudaSuccess; }
+cudaError_t cudaGetDevice(int* d) {
+  *d = 0;
+  return cudaSuccess;
+}
+cudaError_t cudaGetDeviceCount(int* n) {
+  *n = 1;
+  return cudaSuccess;
+}
+cudaError_t cudaGetLastError(void) { return cudaSuccess; }
+cudaError_t cudaPeekAtLastError(void) { return cudaSuccess; }
+cudaError_t cudaMemGetInfo(size_t* f, size_t* t) {
+  *f = (size_t)1 << 36;
+  *t = (size_t)1 << 36;
+  return cudaSuccess;
+}
+cudaError_t cudaGetDeviceProperties_v2(cudaDeviceProp* p, int) {
+  std::memset(p, 0, sizeof(*p));
+  std::strcpy(p->name, "host");
+  p->major = 3;
+  p->minor = 5;
+  p->maxThreadsPerBlock = 1024;
+  p->multiProcessorCount = 1;
+  return cudaSuccess;
+}
+const char* cudaGetErrorName(cudaError_t e) { return e == cudaSuccess ? "cudaSuccess" : "cudaError"; }
+const char* cudaGetErrorString(cudaError_t e) { return cudaGetErrorName(e); }
+
+// cuSPARSE: handles and the COO -> CSR row pointer conversion
+cusparseStatus_t cusparseCreate(cusparseHandle_t* h) {
+  *h = reinterpret_cast<cusparseHandle_t>(new int(0));
+  return CUSPARSE_STATUS_SUCCESS;
+}
+cusparseStatus_t cusparseDestroy(cusparseHandle_t h) {
+  delete reinterpret_cast<int*>(h);
+  return CUSPARSE_STATUS_SUCCESS;
+}
+cusparseStatus_t cusparseCreateMatDescr(cusparseMatDescr_t* d) {
+  *d = reinterpret_cast<cusparseMatDescr_t>(new int(0));
+  return CUSPARSE_STATUS_SUCCESS;
+}
+cusparseStatus_t cusparseDestroyMatDescr(cusparseMatDescr_t d) {
+  delete reinterpret_cast<int*>(d);
+  return CUSPARSE_STATUS_SUCCESS;
+}
+cusparseStatus_t cusparseSetMatType(cusparseMatDescr_t, cusparseMatrixType_t) { return CUSPARSE_STATUS_SUCCESS; }
+cusparseStatus_t cusparseSetMatIndexBase(cusparseMatDescr_t, cusparseIndexBase_t) { return CUSPARSE_STATUS_SUCCESS; }
+cusparseStatus_t cusparseXcoo2csr(cusparseHandle_t, const int* coo_row, int nnz, int m, int* csr_row,
+                                  cusparseIndexBase_t base) {
+  for (int i = 0; i <= m; i++) csr_row[i] = 0;
+  for (int z = 0; z < nnz; z++) csr_row[coo_row[z] - base + 1]++;
+  for (int i = 0; i < m; i++) csr_row[i + 1] += csr_row[i];
+  for (int i = 0; i <= m; i++) csr_row[i] += base;
+  return CUSPARSE_STATUS_SUCCESS;
+}
+
+// cuSOLVER: handles and the sparse Cholesky solve of an SPD CSR system, here by a dense Cholesky
+// factorisation (the test systems have at most a few hundred unknowns)
+cusolverStatus_t cusolverSpCreate(cusolverSpHandle_t* h) {
+  *h = reinterpret_cast<cusolverSpHandle_t>(new int(0));
+  return CUSOLVER_STATUS_SUCCESS;
+}
+cusolverStatus_t cusolverSpDestroy(cusolverSpHandle_t h) {
+  delete reinterpret_cast<int*>(h);
+  return CUSOLVER_STATUS_SUCCESS;
+}
+
+}  // extern "C"
+
+// Solves whose matrix was not positive definite. cuSOLVER reports such a matrix through
+// `singularity` and leaves x unspecified; the reference ignores the report (cusolversolver.cu:55-57),
+// so a run that meets one follows no defined trajectory and is not a pin.
+int ss_hostcuda_singular_solves = 0;
+
+template <class T>
+static cusolverStatus_t dense_chol_solve(int m, int nnz, const T* val, const int* row, const int* col, const T* b,
+                                         T* x, int* singularity) {
+  (void)nnz;
+  std::vector<double> a((size_t)m * m, 0.0), y(m);
+  for (int i = 0; i < m; i++)
+    for (int z = row[i]; z < row[i + 1]; z++) a[(size_t)i * m + col[z]] += (double)val[z];
+  *singularity = -1;
+  for (int j = 0; j < m; j++) {  // A = L L^T (lower triangle)
+    double d = a[(size_t)j * m + j];
+    for (int k = 0; k < j; k++) d -= a[(size_t)j * m + k] * a[(size_t)j * m + k];
+    if (!(d > 0)) {
+      *singularity = j;
+      ss_hostcuda_singular_solves++;
+      return CUSOLVER_STATUS_SUCCESS;
+    }
+    d = std::sqrt(d);
+    a[(size_t)j * m + j] = d;
+    for (int i = j + 1; i < m; i++) {
+      double s = a[(size_t)i * m + j];
+      for (int k = 0; k < j; k++) s -= a[(size_t)i * m + k] * a[(size_t)j * m + k];
+      a[(size_t)i * m + j] = s / d;
+    }
+  }
+  for (int i = 0; i < m; i++) {
+    double s = (double)b[i];
+    for (int k = 0; k < i; k++) s -= a[(size_t)i * m + k] * y[k];
+    y[i] = s / a[(size_t)i * m + i];
+  }
+  for (int i = m - 1; i >= 0; i--) {
+    double s = y[i];
+    for (int k = i + 1; k < m; k++) s -= a[(size_t)k * m + i] * (double)x[k];
+    x[i] = (T)(s / a[(size_t)i * m + i]);
+  }
+  return CUSOLVER_STATUS_SUCCESS;
+}
+
+extern "C" {
+
+cusolverStatus_t cusolverSpDcsrlsvchol(cusolverSpHandle_t, int m, int nnz, const cusparseMatDescr_t, const double* val,
+                                       const int* row, const int* col, const double* b, double, int, double* x,
+                                       int* singularity) {
+  return dense_chol_solve<double>(m, nnz, val, row, col, b, x, singularity);
+}
+cusolverStatus_t cusolverSpScsrlsvchol(cusolverSpHandle_t, int m, int nnz, const cusparseMatDescr_t, const float* val,
+                                       const int* row, const int* col, const float* b, float, int, float* x,
+                                       int* singularity) {
+  return dense_chol_solve<float>(m, nnz, val, row, col, b, x, singularity);
+}
+
+}  // extern "C"

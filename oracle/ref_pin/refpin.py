@@ -131,3 +131,84 @@ def range_filter(v, strength):
     a = np.ascontiguousarray(v, dtype=np.float64).copy()
     lib().ssref_range_filter(_p(a), a.size, float(strength))
     return a
+
+
+# ------------------------------------------------------------------------------------------------
+# The reference's whole task layer on the host (oracle/_ref/libssrefrun.so, refrun.cpp)
+
+RUN_LIB = os.path.abspath(os.path.join(HERE, "..", "_ref", "libssrefrun.so"))
+_run_lib = None
+
+
+class RunIn(C.Structure):
+    _fields_ = [("flags", C.c_char_p), ("templ_h", C.c_int), ("templ_w", C.c_int), ("templ", C.c_void_p),
+                ("xgrad", C.c_void_p), ("ygrad", C.c_void_p), ("frame_h", C.c_int), ("frame_w", C.c_int),
+                ("n_frames", C.c_int), ("frac", C.c_void_p), ("basex", C.c_void_p), ("basey", C.c_void_p),
+                ("base_mask", C.c_void_p), ("image", C.c_void_p), ("est_dx", C.c_void_p), ("est_dy", C.c_void_p),
+                ("min_points", C.c_void_p), ("group_size", C.c_int), ("max_iter", C.c_int),
+                ("move_thresh", C.c_double), ("halt_corr", C.c_double), ("corr_inc_thresh", C.c_double),
+                ("filter_strength", C.c_double), ("max_filter_iter", C.c_int), ("filter_corr_thresh", C.c_double),
+                ("lam", C.c_double), ("ls_mult", C.c_double), ("solver_id", C.c_int), ("filter_id", C.c_int)]
+
+
+class RunOut(C.Structure):
+    _fields_ = [("dx", C.c_void_p), ("dy", C.c_void_p), ("frame_corr", C.c_void_p), ("residrms", C.c_void_p),
+                ("mask", C.c_void_p), ("all_params", C.c_void_p), ("iter_errvals", C.c_void_p),
+                ("iter_corr", C.c_void_p), ("frame_corr_hist", C.c_void_p), ("iterations", C.c_int),
+                ("stop_reason", C.c_int), ("singular_solves", C.c_int)]
+
+
+def run_available() -> bool:
+    return os.path.exists(RUN_LIB) or os.path.isdir(REF_TREE)
+
+
+def run_lib():
+    global _run_lib
+    if _run_lib is None:
+        if not os.path.exists(RUN_LIB):
+            subprocess.check_call(["make", "-s", "-C", HERE])
+        _run_lib = C.CDLL(RUN_LIB)
+        _run_lib.ssrun_align.argtypes = [C.POINTER(RunIn), C.POINTER(RunOut)]
+        _run_lib.ssrun_align.restype = C.c_int
+    return _run_lib
+
+
+def run_align(args: dict) -> dict:
+    """The reference's align_group_to_template task (Task::alignFrames with MainIteration, its
+    kernels and filters, solver id 1) on the 26 boundary arguments; returns its outputs: knots,
+    frame correlations, residrms, mask, the knot chain after every iteration (all_params) and, with
+    flags e / C, the errvals of every half-step and the global correlation of every iteration."""
+    rm = lambda a, dt=np.float64: np.ascontiguousarray(np.asarray(a, dtype=dt))
+    t, xg, yg = rm(args["template_image"]), rm(args["xgrad"]), rm(args["ygrad"])
+    frac, bx, by = rm(args["tfrac"]), rm(args["basex"]), rm(args["basey"])
+    bm, img = rm(args["base_mask"], np.uint8), rm(args["bmData"])
+    hb, w = frac.shape
+    nF = int(args["nFrames"])
+    edx = np.asarray(args["est_dx_knots"], dtype=np.float64).reshape(-1, order="F").copy()
+    edy = np.asarray(args["est_dy_knots"], dtype=np.float64).reshape(-1, order="F").copy()
+    mp = np.ascontiguousarray(np.asarray(args["min_points_per_block"]).reshape(-1)[:w], dtype=np.int32)
+    flags = args["flags"].encode() if isinstance(args["flags"], str) else bytes(args["flags"])
+    mi = int(args["max_iter"])
+    N = w * nF + 1
+    keep = [t, xg, yg, frac, bx, by, bm, img, edx, edy, mp, flags]
+    i = RunIn(flags, t.shape[0], t.shape[1], _p(t), _p(xg), _p(yg), hb, w, nF, _p(frac), _p(bx), _p(by), _p(bm),
+              _p(img), _p(edx), _p(edy), _p(mp), int(args["group_size"]), mi, float(args["move_thresh"]),
+              float(args["halt_correlation"]), float(args["correlation_increase_threshold"]),
+              float(args["filter_strength"]), int(args["max_filter_iterations"]),
+              float(args["filter_deactivation_threshold"]), float(args.get("lambda", 0.0)),
+              float(args["linesearch_reduction_multiplier"]), int(args["solver_id"]), int(args["filter_id"]))
+    o = dict(dx=np.zeros((w + 1) * nF), dy=np.zeros((w + 1) * nF), frame_corr=np.zeros(nF), residrms=np.zeros(nF),
+             mask=np.zeros((hb, w * nF), np.uint8), all_params=np.zeros((mi, 2 * N)),
+             iter_errvals=np.zeros((nF, 2 * mi)), iter_corr=np.zeros(mi), frame_corr_hist=np.zeros((mi, nF)))
+    out = RunOut(*[_p(o[k]) for k in ("dx", "dy", "frame_corr", "residrms", "mask", "all_params", "iter_errvals",
+                                      "iter_corr", "frame_corr_hist")], 0, 0, 0)
+    rc = run_lib().ssrun_align(C.byref(i), C.byref(out))
+    del keep
+    if rc != 0:
+        raise RuntimeError(f"reference run failed ({rc})")
+    o["iterations"] = out.iterations
+    o["stop_reason"] = out.stop_reason
+    o["singular_solves"] = out.singular_solves
+    o["mask"] = o["mask"].astype(bool)
+    o["iter_errvals"] = o["iter_errvals"].T.copy()  # (2 max_iter) x nF, as the MEX output
+    return o

@@ -762,7 +762,13 @@ static double global_correlation(St* s) {
             }
         }
     }
-    for (int i = 0; i < npx; i++)
+    /* the swap back is launched with the per-column kernel's grid (task_correlation.cu:86-98): one
+     * block of THREADS_PER_BLOCK per 256 block columns, so only the first 256 ceil(fW / 256)
+     * pixels (row-major) are swapped back; the others keep the warped template until a later
+     * pass writes their difference image again */
+    int swap_back = 256 * ((s->fW + 255) / 256);
+    if (swap_back > npx) swap_back = npx;
+    for (int i = 0; i < swap_back; i++)
         if (s->mask[i]) s->diff[i] = s->in->image[i] - s->diff[i];
     return q / sqrt(assq * bssq);
 }
@@ -981,7 +987,8 @@ int sso_align_group(const sso_in* in, sso_out* out) {
     }
     if (iteration == 1) memcpy(s->p_last, s->p, sizeof(double) * s->P);
     calc_group_errvals(s, 0);
-    frame_correlation(s);
+    /* with flag c the frame correlations of the last iteration are the output (task.cpp:392-395) */
+    if (!s->flag_c) frame_correlation(s);
 
     out->iterations = iteration;
     out->stop_reason = stop;
