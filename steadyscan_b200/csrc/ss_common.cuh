@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <climits>
+
 namespace ss {
 
 // Values the reference leaves in buffers it allocates (task_allocate.cu:226, :244).
@@ -124,6 +126,8 @@ struct GroupDesc {
   uint8_t *params_used, *blocks_present, *grp_active;
   double* errval;           // 2 nF
   double *kmask, *kdiff;    // nF x 2 x (W+1)
+  uint32_t* dparity;        // flag M: fW x ceil(Hb/32) words, bit r of a column's word r/32 set where
+                            // the difference-image buffer holds image - difference; else nullptr
   uint8_t* fstate;          // nF: 2 while the frame's line search runs
   int* ls_trials;           // nF
   double* eig_c;            // N x 4

@@ -889,6 +889,8 @@ static void layout(Batch::Impl* b, char* base) {
     G.errval = cv.take<double>(2 * nF);
     G.kmask = cv.take<double>(nF * 2 * (g.W + 1));
     G.kdiff = cv.take<double>(nF * 2 * (g.W + 1));
+    // written by every correlation pass before a stale frame reads it: no initial value
+    G.dparity = (g.flags & kFlagMaskInactive) ? cv.take<uint32_t>((size_t)g.fW * ((g.Hb + 31) / 32)) : nullptr;
     G.fstate = cv.take<uint8_t>(nF);
     G.ls_trials = cv.take<int>(nF);
     G.ls_done = cv.take<int>(nF);

@@ -79,6 +79,46 @@ __device__ __forceinline__ bool frame_active(const GroupDesc& G, int f, int shif
   return gid < 2 * G.n_rg && G.grp_active[gid];
 }
 
+// The reference's difference-image buffer between its rewrites. hd_globalCorrelation swaps every
+// valid pixel to image - difference and swaps back only the first 256 ceil(fW / 256) pixels in
+// row-major order, the grid of its per-column kernel (task_correlation.cu:86-98); frames rewrite
+// the buffer in d_calcAllGroupErrval and the line search, so with every group active the swapped
+// pixels are rewritten before anything reads them, except hd_frameCorrelation of the same
+// iteration (flag c), which then correlates the difference image itself past that index. With
+// flag M a frame that is inactive in both half-steps keeps its buffer, and each later global
+// correlation swaps its valid pixels past the index once more: the parity bitmap records which
+// buffer pixels hold image - difference.
+//
+// DiffState of one block column: row_s, the first row whose pixel lies past the swap-back (kCorr);
+// par_in, the column's parity words where its frame was not rewritten since the last global
+// correlation (else nullptr: nothing swapped); par_out, the words the correlation pass updates.
+struct DiffState {
+  int row_s;
+  const uint32_t* par_in;
+  uint32_t* par_out;
+};
+
+__device__ __forceinline__ DiffState no_diff_state() { return DiffState{INT_MAX, nullptr, nullptr}; }
+
+template <int MODE>
+__device__ __forceinline__ DiffState diff_state(const GroupDesc& G, int shift, int f, int col) {
+  DiffState d = no_diff_state();
+  if (MODE == kCorr) {
+    const int s = 256 * ((G.fW + 255) / 256);
+    d.row_s = (s - col + G.fW - 1) / G.fW;  // first r with r * fW + col >= s
+  }
+  if (G.dparity) {
+    uint32_t* w = G.dparity + (size_t)col * ((G.Hb + 31) >> 5);
+    bool stale;  // not rewritten since the last global correlation
+    if (MODE == kAssemble) stale = !frame_active(G, f, shift) && !(shift == 1 && frame_active(G, f, 0));
+    else if (MODE == kCorr) stale = !frame_active(G, f, 0) && !frame_active(G, f, 1);
+    else stale = !frame_active(G, f, 0);  // kFinal, after the final hd_calculateGroupErrvals(mem, 0)
+    if (stale) d.par_in = w;
+    if (MODE == kCorr) d.par_out = w;
+  }
+  return d;
+}
+
 template <class Acc>
 struct Limits;
 template <>
@@ -233,10 +273,11 @@ __host__ __device__ constexpr int nsums(int mode) {
 // Evaluates one block column with one warp and returns the warp-reduced sums (all lanes) and the
 // valid-pixel count. coli is the column's offset in the frame data; mask_out (kFinal) receives the
 // reference's mask output.
-template <class Acc, class FrameT, class TplT, int MODE, bool AFFINE = false, bool WIN = false>
+template <class Acc, class FrameT, class TplT, int MODE, bool AFFINE = false, bool WIN = false, bool DS = false>
 __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, const ColGeo<Acc>& geo,
                                             const ColKnots<Acc>& k, double (&out)[kCsStride], int& cnt_out,
-                                            uint8_t* mask_out, int cc = 0, const TWin& win = TWin{nullptr, 0, 0, 0}) {
+                                            uint8_t* mask_out, int cc = 0, const TWin& win = TWin{nullptr, 0, 0, 0},
+                                            const DiffState& ds = no_diff_state()) {
   const int lane = threadIdx.x & 31;
   const int Hb = G.Hb;
   const Acc tw = Limits<Acc>::lim(G.Wt), th = Limits<Acc>::lim(G.Ht);
@@ -280,9 +321,11 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
     Acc x, y;
     const bool mA = warp_pixel<Acc>(k.ax0, k.ax1, k.ay0, k.ay1, f, bxv, byv, bm, tw, th, x, y) && in;
     cnt += mA ? 1 : 0;
+    // the buffer pixel holds image - difference (flag M: swapped by earlier global correlations)
+    const bool par = DS && ds.par_in != nullptr && in && ((ds.par_in[r0 >> 5] >> lane) & 1u);
 
     if (MODE == kAssemble) {
-      Acc img = (mA || (k.dual && in)) ? ld_pixel<Acc, FrameT>(G.image, coli + r) : (Acc)0;
+      Acc img = (mA || ((k.dual || par) && in)) ? ld_pixel<Acc, FrameT>(G.image, coli + r) : (Acc)0;
       Acc wx = 0, wy = 0, d = 0;
       if (mA) {
         Sample<Acc> sa = samp<Acc, TplT, true, WIN>(G, win, x, y);
@@ -295,6 +338,7 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
         bool mB = warp_pixel<Acc>(k.bx0, k.bx1, k.by0, k.by1, f, bxv, byv, bm, tw, th, xb, yb) && in;
         d = mB ? img - samp<Acc, TplT, false, WIN>(G, win, xb, yb).wI : (Acc)0;
       }
+      if (par) d = img - d;
       const Acc fn = split_fn ? (in ? geo.fnext[r] : (Acc)0) : f;
       const Acc fsq = f * f, csq = (one - f) * (one - f), fc = f - fsq, fnsq = fn * fn;
       const Acc gxx = wx * wx, gyy = wy * wy, gxy = wx * wy;
@@ -331,7 +375,12 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
         wB = mB ? samp<Acc, TplT, false, WIN>(G, win, xb, yb).wI : (Acc)0;
       }
       Acc dstate = mB ? img - wB : (Acc)0;  // differenceImage
+      if (par) dstate = img - dstate;       // the buffer as the earlier swaps left it
       Acc dp = mA ? img - dstate : dstate;  // after d_swapWIDiff
+      if (DS && MODE == kCorr && ds.par_out) {
+        const unsigned nb = __ballot_sync(0xffffffffu, par != (mA && r >= ds.row_s));
+        if (lane == 0) ds.par_out[r0 >> 5] = nb;
+      }
       s[kCsSumD] += dp;
       unsigned bal = __ballot_sync(0xffffffffu, mA);
       unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
@@ -345,11 +394,14 @@ __device__ __forceinline__ void eval_column(const GroupDesc& G, size_t coli, con
       }
       run = run && (bal == 0xffffffffu);
       if (mA) {
-        s[kCsFrD] += dp;
+        // hd_frameCorrelation after the global correlation (flag c) swaps back to the buffer the
+        // pixels past the swap-back (kCorr); the final one sees the whole swapped image
+        const Acc da = (DS && MODE == kCorr && r >= ds.row_s) ? dstate : dp;
+        s[kCsFrD] += da;
         s[kCsFrI] += img;
-        s[kCsFrDD] = fma(dp, dp, s[kCsFrDD]);
+        s[kCsFrDD] = fma(da, da, s[kCsFrDD]);
         s[kCsFrII] = fma(img, img, s[kCsFrII]);
-        s[kCsFrDI] = fma(dp, img, s[kCsFrDI]);
+        s[kCsFrDI] = fma(da, img, s[kCsFrDI]);
         if (MODE == kFinal) {
           Acc dA = img - wA;
           s[kCsFinalSsd] = fma(dA, dA, s[kCsFinalSsd]);
@@ -482,6 +534,8 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
           const double* prev = G.asmk + (size_t)(f * W + cc) * 8;
 #pragma unroll
           for (int i = 0; i < 8; i++) changed |= __double_as_longlong(k[i]) != __double_as_longlong(prev[i]);
+          // a swapped buffer changes with every global correlation, the knots staying the same
+          changed |= diff_state<kAssemble>(G, C.shift, f, f * W + cc).par_in != nullptr;
         }
         m |= (unsigned long long)__ballot_sync(0xffffffffu, changed) << (fa - f0);
       }
@@ -580,11 +634,17 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
     double out[kCsStride];
     int cnt;
     uint8_t* mo = G.o_mask ? G.o_mask + coli : nullptr;
-    if constexpr (sizeof(Acc) == 4) {
-      if (MODE == kAssemble && win.p && G.pair_ok && !k.dual) {
+    const DiffState ds = diff_state<MODE>(G, C.shift, f, c);
+    if (ds.par_in || ds.par_out || (MODE == kCorr && (G.flags & kFlagFrameCorr))) {
+      // the buffer state of flags M and c (DiffState), on the table-geometry path
+      eval_column<Acc, FrameT, TplT, MODE, false, false, true>(G, coli, geo, k, out, cnt, mo, cc,
+                                                               TWin{nullptr, 0, 0, 0}, ds);
+    } else if constexpr (sizeof(Acc) == 4) {
+      const bool pairs = win.p && G.pair_ok && !k.dual;
+      if (MODE == kAssemble && pairs) {
         assemble_pairs<FrameT>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt);
         if ((threadIdx.x & 31) == 0) atomicAdd(G.staging + 5, 1ull);
-      } else if (MODE != kAssemble && win.p && G.pair_ok && !k.dual) {
+      } else if (MODE != kAssemble && pairs) {
         corr_pairs<FrameT, MODE>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt, mo);
       } else if (win.p) {
         if (affine) eval_column<Acc, FrameT, TplT, MODE, true, true>(G, coli, geo, k, out, cnt, mo, cc, win);
@@ -900,7 +960,11 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
                 s_kd[1][i + 1]);
       double out[kCsStride];
       int c;
-      if constexpr (sizeof(Acc) == 4) {
+      const DiffState ds = diff_state<kCorr>(G, shift, f, b0 + t);
+      if (ds.par_out || (G.flags & kFlagFrameCorr)) {  // the buffer state of flags M and c (DiffState)
+        eval_column<Acc, FrameT, TplT, kCorr, false, false, true>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k,
+                                                                  out, c, nullptr, t, TWin{nullptr, 0, 0, 0}, ds);
+      } else if constexpr (sizeof(Acc) == 4) {
         const size_t coli = (size_t)(b0 + t) * Hb;
         if (win.p) {
           if (G.geo_k > 0)

@@ -1037,7 +1037,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_final(const GroupDesc* __rest
         G.errval[f] = val;
         atomicAdd(&sh_nact, 1);
       }
-      G.o_frame_corr[f] = pearson(nf, s5[0], s5[1], s5[2], s5[3], s5[4]);
+      // with flag c the last iteration's frame correlations stand (task.cpp:392-395)
+      if (!(G.flags & kFlagFrameCorr)) G.o_frame_corr[f] = pearson(nf, s5[0], s5[1], s5[2], s5[3], s5[4]);
       G.o_residrms[f] = sqrt(G.errval[f]);
     }
   }

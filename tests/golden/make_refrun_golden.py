@@ -35,6 +35,14 @@ CASES = {
     "bidirectional_k1": (dict(nlines=16, linewidth=16, nknots=17, seed=26,
                               settings={"gpu_solver_id": 1, "isbidirectional": True}), "DCce"),
     "mask_inactive": (dict(n_frames=4, seed=9, settings={"gpu_solver_id": 1, "haltcorr": 0.9}), "DCceM"),
+    # frames inactive over consecutive iterations (flag c's frame correlations are low, so a low
+    # haltcorr deactivates them): their difference-image buffers are swapped by several global
+    # correlations without being rewritten
+    "mask_inactive_stale": (dict(n_frames=6, seed=16, settings={"gpu_solver_id": 1, "haltcorr": 0.2}), "DCceM"),
+    "mask_inactive_stale_b": (dict(n_frames=6, seed=10, settings={"gpu_solver_id": 1, "haltcorr": 0.15}), "DCceM"),
+    # 40 frames of 8 blocks: fW = 320 columns, so the global correlation's swap-back (the first
+    # 512 pixels in row-major order) ends inside the second row
+    "swap_back_row1": (dict(n_frames=40, seed=33, settings={"gpu_solver_id": 1}), "DCce"),
     "frames_32_blocks": (dict(nlines=64, linewidth=24, nknots=33, n_frames=4, seed=12,
                               settings={"gpu_solver_id": 1}), "DCce"),
 }

@@ -28,7 +28,7 @@ def _build():
 
 
 def test_fixtures_present():
-    assert len(GOLDEN) >= 9
+    assert len(GOLDEN) >= 11
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[7:-4] for p in GOLDEN])

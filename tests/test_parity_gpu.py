@@ -120,6 +120,40 @@ def test_mask_inactive_flag():
     _compare_d(args)
 
 
+def _compare_history(args):
+    o, g = _compare_d(args, o=oracle.align_group(args, want_history=True), g=api.align_group(args, want_history=True))
+    it = o["iterations"]
+    np.testing.assert_allclose(g["iteration_corr"][:it], o["iter_corr"][:it], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(g["frame_corr_history"][:, :it], o["frame_corr_hist"][:it].T, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(g["all_params"][:, :it], o["all_params"][:it].T, atol=KNOT_TOL_D)
+    return o, g
+
+
+@pytest.mark.parametrize("seed,halt", [(16, 0.2), (10, 0.15)])
+def test_mask_inactive_frames_stale_over_iterations(seed, halt):
+    """Flags M and c with frames inactive over consecutive iterations (the cases of the
+    mask_inactive_stale reference-run fixtures): the difference-image buffer of an inactive frame is
+    swapped by every global correlation past the swap-back index (task_correlation.cu:86-98) and
+    read by the next assembly, correlation and final pass."""
+    args, _, _ = make_args(n_frames=6, seed=seed, settings={"gpu_solver_id": 1, "haltcorr": halt})
+    args["flags"] = "DCceM"
+    o, _ = _compare_history(args)
+    assert o["iterations"] >= 3
+
+
+def test_frame_corr_past_the_swap_back_in_row_one():
+    """Flag c on 40 frames of 8 blocks (fW = 320): the per-iteration frame correlations switch
+    from the swapped image to the difference image at row-major index 512, inside row 1."""
+    args, _, _ = make_args(n_frames=40, seed=33, settings={"gpu_solver_id": 1})
+    args["flags"] = "DCce"
+    _compare_history(args)
+    args["flags"] = "SCce"
+    o = oracle.align_group(dict(args, flags="DCce"), want_history=True)
+    g = api.align_group(args, want_history=True)
+    it = min(o["iterations"], g["iter_used"])
+    np.testing.assert_allclose(g["frame_corr_history"][:, :it], o["frame_corr_hist"][:it].T, atol=2e-3)
+
+
 def test_frames_outside_template():
     """Frames displaced entirely off the template: no block is ever present (steady_scan.m:267-272)."""
     args, _, _ = make_args(seed=9)
