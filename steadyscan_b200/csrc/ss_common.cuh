@@ -66,7 +66,7 @@ struct GroupCtl {
   int ls_state;    // 1 from the half-step solve until the line search is post-processed
   int ls_pending;  // frames of the half-step whose line search still runs (trial rounds)
   int solve_now;          // 1 while the group's half-step solve of this cycle runs (set by k_solve_compact)
-  int pad1;
+  int par_sel;            // flag M: the parity bitmap (0 or 1) of the last global correlation
   double correlation, corr;
   long long n_eval;      // frame evaluations the reference would count: errval passes and trials
   long long passes[4];   // frames read per evaluation kind (EvalMode)
@@ -126,8 +126,10 @@ struct GroupDesc {
   uint8_t *params_used, *blocks_present, *grp_active;
   double* errval;           // 2 nF
   double *kmask, *kdiff;    // nF x 2 x (W+1)
-  uint32_t* dparity;        // flag M: fW x ceil(Hb/32) words, bit r of a column's word r/32 set where
-                            // the difference-image buffer holds image - difference; else nullptr
+  uint32_t* dparity;        // flag M: 2 x fW x ceil(Hb/32) words, bit r of a column's word r/32 set
+                            // where the difference-image buffer holds image - difference: the
+                            // bitmap of the last global correlation (GroupCtl::par_sel) and the one
+                            // the next correlation pass writes; else nullptr
   uint8_t* fstate;          // nF: 2 while the frame's line search runs
   int* ls_trials;           // nF
   double* eig_c;            // N x 4

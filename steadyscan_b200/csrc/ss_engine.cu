@@ -890,7 +890,7 @@ static void layout(Batch::Impl* b, char* base) {
     G.kmask = cv.take<double>(nF * 2 * (g.W + 1));
     G.kdiff = cv.take<double>(nF * 2 * (g.W + 1));
     // written by every correlation pass before a stale frame reads it: no initial value
-    G.dparity = (g.flags & kFlagMaskInactive) ? cv.take<uint32_t>((size_t)g.fW * ((g.Hb + 31) / 32)) : nullptr;
+    G.dparity = (g.flags & kFlagMaskInactive) ? cv.take<uint32_t>(2 * (size_t)g.fW * ((g.Hb + 31) / 32)) : nullptr;
     G.fstate = cv.take<uint8_t>(nF);
     G.ls_trials = cv.take<int>(nF);
     G.ls_done = cv.take<int>(nF);
@@ -925,7 +925,7 @@ static void layout(Batch::Impl* b, char* base) {
 }
 
 int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
-                   const Batch* const* sessions, bool measure_only, void* borrow_stream, bool no_wait) {
+                   const Batch* const* sessions, bool measure_only, void* borrow_stream) {
   Impl* b = d;
   if (n < 1) return fail(SS_ERR_INVALID_ARGUMENT, "no groups");
   b->hg.assign(n, HostGroup{});
@@ -1070,14 +1070,8 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
   SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_chunk_group, chunk_group.data(), chunk_group.size() * 4, cudaMemcpyHostToDevice, s));
   SS_CK(cudaMemcpyAsync(b->d_frame_group, frame_group.data(), frame_group.size() * 4, cudaMemcpyHostToDevice, s));
-  // pageable sources are staged before the copies return; an own stream is also drained unless the
-  // caller runs the batch behind its uploads
-  if (b->own_stream && !no_wait) SS_CK(cudaStreamSynchronize(s));
-  return SS_OK;
-}
-
-int Batch::pin() {
-  if (!d->h_counters) SS_CK(cudaHostAlloc(&d->h_counters, (kCounters + 1) * sizeof(int), cudaHostAllocDefault));
+  // pageable sources are staged before the copies return; an own stream is also drained
+  if (b->own_stream) SS_CK(cudaStreamSynchronize(s));
   return SS_OK;
 }
 
@@ -1913,88 +1907,6 @@ int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out) {
   return SS_OK;
 }
 
-// ss_align_groups for groups whose frames are in host memory: the groups are split into up to
-// kPipelineParts consecutive parts of about equal frame counts, each a batch on its own stream in
-// one device allocation. Every part's uploads are queued first, then every part's run is launched
-// behind its own uploads, so the copies of the later parts overlap the runs of the earlier ones and
-// the runs overlap each other. A group's result does not depend on the other groups of its batch,
-// so it is the one of a single batch.
-constexpr int kPipelineParts = 4;
-
-int align_groups_pipelined(int n, const ss_inputs* in, ss_outputs* out) {
-  long long total = 0;
-  for (int i = 0; i < n; i++) total += in[i].n_frames;
-  const int parts = std::min(n, kPipelineParts);
-  std::vector<int> start(parts + 1, n);
-  {
-    long long acc = 0;
-    int k = 0;
-    start[0] = 0;
-    for (int i = 0; i < n && k + 1 < parts; i++) {
-      acc += in[i].n_frames;
-      if (acc * parts >= total * (k + 1) && i + 1 < n) start[++k] = i + 1;
-    }
-    for (int j = k + 1; j <= parts; j++) start[j] = n;
-  }
-  std::vector<std::unique_ptr<Batch>> bs;
-  std::vector<size_t> bytes;
-  size_t sum = 0;
-  for (int k = 0; k < parts; k++) {
-    const int a = start[k], m = start[k + 1] - start[k];
-    if (m <= 0) continue;
-    Batch meas;
-    int rc = meas.prepare(m, in + a, out ? out + a : nullptr, nullptr, 0, nullptr, true);
-    if (rc) return rc;
-    const size_t nb = (meas.arena_bytes() + 255) & ~size_t(255);
-    bytes.push_back(nb);
-    sum += nb;
-    bs.emplace_back(new Batch);
-  }
-  int dev = in[0].gpu_device_id, ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
-  if (dev < 0 || dev >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
-  SS_CK(cudaSetDevice(dev));
-  char* arena = nullptr;
-  SS_CK(cudaMalloc(&arena, sum));
-  struct Free {
-    std::vector<std::unique_ptr<Batch>>* b;
-    char* p;
-    ~Free() {
-      b->clear();  // batches drain their streams first
-      cudaFree(p);
-    }
-  } guard{&bs, arena};
-  // every part's uploads, then every part's run behind them
-  size_t off = 0;
-  for (size_t k = 0, a = 0; k < bs.size(); k++) {
-    while (start[a + 1] - start[a] <= 0) a++;
-    const int first = start[a], m = start[a + 1] - start[a];
-    a++;
-    int rc = bs[k]->prepare(m, in + first, out ? out + first : nullptr, arena + off, bytes[k], nullptr, false,
-                            nullptr, true);
-    if (!rc) rc = bs[k]->pin();
-    if (rc) return rc;
-    off += bytes[k];
-  }
-  for (auto& b : bs) {
-    int rc = b->start();
-    if (!rc) rc = b->step();
-    if (rc) return rc;
-  }
-  for (auto& b : bs) {
-    for (;;) {
-      SS_CK(cudaStreamSynchronize(static_cast<cudaStream_t>(b->stream())));
-      int rc = b->poll();
-      if (rc < 0) return rc;
-      if (rc == 2) break;
-      if ((rc = b->step())) return rc;  // host-launched cycles (timing on) need the next one
-    }
-    int rc = b->collect();
-    if (rc) return rc;
-  }
-  return SS_OK;
-}
-
 int Batch::cycles() const { return d->cycles; }
 int Batch::rounds() const { return d->rounds; }
 int Batch::n_groups() const { return (int)d->gd.size(); }
@@ -2011,17 +1923,10 @@ extern "C" {
 int ss_align_groups(int32_t n_groups, const ss_inputs* in, ss_outputs* out) {
   auto t0 = std::chrono::steady_clock::now();
   if (!in || n_groups < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "no groups");
-  int rc = SS_OK;
-  bool host_frames = n_groups >= 2;
-  for (int i = 0; i < n_groups && host_frames; i++) host_frames = in[i].bm_data.location == SS_HOST;
-  if (host_frames) {
-    rc = ss::align_groups_pipelined(n_groups, in, out);
-  } else {
-    ss::Batch b;
-    rc = b.prepare(n_groups, in, out, nullptr, 0);
-    if (!rc) rc = b.run();
-    if (!rc) rc = b.collect();
-  }
+  ss::Batch b;
+  int rc = b.prepare(n_groups, in, out, nullptr, 0);
+  if (!rc) rc = b.run();
+  if (!rc) rc = b.collect();
   if (rc) return rc;
   double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (out)

@@ -28,11 +28,8 @@ class Batch {
   // geometry buffers group i uses instead of its own (they must outlive this batch). With
   // measure_only the call stops after computing arena_bytes(): no device work. borrow_stream (a
   // cudaStream_t) runs the batch on the caller's stream without blocking on it.
-  // With no_wait the uploads stay queued on the batch's stream when the call returns (the caller
-  // keeps the host inputs alive until the run has finished).
   int prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
-              const Batch* const* sessions = nullptr, bool measure_only = false, void* borrow_stream = nullptr,
-              bool no_wait = false);
+              const Batch* const* sessions = nullptr, bool measure_only = false, void* borrow_stream = nullptr);
   // Runs every group from its initial knots to its stop criterion.
   int run();
   // The same run one cycle at a time without blocking: start() resets every group to its initial
@@ -41,8 +38,6 @@ class Batch {
   int start();
   int step();
   int poll();
-  // Allocates the pinned host counters of a run ahead of start() (start() does it otherwise).
-  int pin();
   // Resets every group to its initial state (the start of a server slot; waits on an own stream).
   int reset();
   // Copies the results into the ss_outputs given to prepare().
@@ -63,10 +58,6 @@ class Batch {
   friend int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out);
   Impl* d;
 };
-
-// ss_align_groups for host-resident frames: parts of the groups on their own streams, the uploads
-// of later parts overlapping the runs of earlier ones.
-int align_groups_pipelined(int n, const ss_inputs* in, ss_outputs* out);
 
 // The recording-level estimate of ss_estimate_displacements: every set of the recording as one
 // group of one batch, then the caller's post-estimate rules on the device.

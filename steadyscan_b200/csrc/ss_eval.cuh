@@ -91,7 +91,10 @@ __device__ __forceinline__ bool frame_active(const GroupDesc& G, int f, int shif
 //
 // DiffState of one block column: row_s, the first row whose pixel lies past the swap-back (kCorr);
 // par_in, the column's parity words where its frame was not rewritten since the last global
-// correlation (else nullptr: nothing swapped); par_out, the words the correlation pass updates.
+// correlation (else nullptr: nothing swapped); par_out, the words the correlation pass writes. The
+// correlation pass writes the other bitmap of the pair, which becomes current when the group moves
+// to its iteration end (k_after_ls): a pass after which MainIteration retries the iteration without
+// its filter (mainiteration.cpp:62-119) is followed by no global correlation and changes nothing.
 struct DiffState {
   int row_s;
   const uint32_t* par_in;
@@ -101,20 +104,21 @@ struct DiffState {
 __device__ __forceinline__ DiffState no_diff_state() { return DiffState{INT_MAX, nullptr, nullptr}; }
 
 template <int MODE>
-__device__ __forceinline__ DiffState diff_state(const GroupDesc& G, int shift, int f, int col) {
+__device__ __forceinline__ DiffState diff_state(const GroupDesc& G, int par_sel, int shift, int f, int col) {
   DiffState d = no_diff_state();
   if (MODE == kCorr) {
     const int s = 256 * ((G.fW + 255) / 256);
     d.row_s = (s - col + G.fW - 1) / G.fW;  // first r with r * fW + col >= s
   }
   if (G.dparity) {
-    uint32_t* w = G.dparity + (size_t)col * ((G.Hb + 31) >> 5);
+    const size_t nw = (size_t)((G.Hb + 31) >> 5), plane = (size_t)G.fW * nw;
+    uint32_t* w = G.dparity + (size_t)par_sel * plane + (size_t)col * nw;
     bool stale;  // not rewritten since the last global correlation
     if (MODE == kAssemble) stale = !frame_active(G, f, shift) && !(shift == 1 && frame_active(G, f, 0));
     else if (MODE == kCorr) stale = !frame_active(G, f, 0) && !frame_active(G, f, 1);
     else stale = !frame_active(G, f, 0);  // kFinal, after the final hd_calculateGroupErrvals(mem, 0)
     if (stale) d.par_in = w;
-    if (MODE == kCorr) d.par_out = w;
+    if (MODE == kCorr) d.par_out = G.dparity + (size_t)(par_sel ^ 1) * plane + (size_t)col * nw;
   }
   return d;
 }
@@ -535,7 +539,7 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
 #pragma unroll
           for (int i = 0; i < 8; i++) changed |= __double_as_longlong(k[i]) != __double_as_longlong(prev[i]);
           // a swapped buffer changes with every global correlation, the knots staying the same
-          changed |= diff_state<kAssemble>(G, C.shift, f, f * W + cc).par_in != nullptr;
+          changed |= diff_state<kAssemble>(G, C.par_sel, C.shift, f, f * W + cc).par_in != nullptr;
         }
         m |= (unsigned long long)__ballot_sync(0xffffffffu, changed) << (fa - f0);
       }
@@ -619,11 +623,16 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
   for (int f = fb * fpc + warp; f < f_end; f += kEvalWarps) {
     const int c = f * W + cc;
     ColKnots<Acc> k;
-    double ka[8];
     if (MODE == kAssemble) {
       if (!((need >> (f - f0)) & 1ull)) continue;
+      double ka[8];
       assembly_knots(G, f, cc, C.shift, ka);  // (the difference image of an inactive frame is stale)
       set_knots(k, ka[0], ka[1], ka[2], ka[3], ka[4], ka[5], ka[6], ka[7]);
+      // the knots the column's sums belong to (no other tile reads this column's entry meanwhile),
+      // stored before the evaluation so that they hold no registers across it
+      if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int i = 0; i < 8; i++) G.asmk[(size_t)c * 8 + i] = ka[i];
     } else {
       const double* km = G.kmask + (size_t)f * 2 * (W + 1);
       const double* kd = G.kdiff + (size_t)f * 2 * (W + 1);
@@ -634,7 +643,7 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
     double out[kCsStride];
     int cnt;
     uint8_t* mo = G.o_mask ? G.o_mask + coli : nullptr;
-    const DiffState ds = diff_state<MODE>(G, C.shift, f, c);
+    const DiffState ds = diff_state<MODE>(G, C.par_sel, C.shift, f, c);
     if (ds.par_in || ds.par_out || (MODE == kCorr && (G.flags & kFlagFrameCorr))) {
       // the buffer state of flags M and c (DiffState), on the table-geometry path
       eval_column<Acc, FrameT, TplT, MODE, false, false, true>(G, coli, geo, k, out, cnt, mo, cc,
@@ -662,8 +671,6 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
       for (int i = 0; i < nsums(MODE); i++) dst[i] = out[i];
       if (MODE == kAssemble) {
         G.asmcnt[c] = cnt;
-#pragma unroll
-        for (int i = 0; i < 8; i++) G.asmk[(size_t)c * 8 + i] = ka[i];
       } else {
         G.colcnt[c] = cnt;
       }
@@ -960,7 +967,7 @@ __global__ void __launch_bounds__(LsShape<Acc>::threads, LsShape<Acc>::min_block
                 s_kd[1][i + 1]);
       double out[kCsStride];
       int c;
-      const DiffState ds = diff_state<kCorr>(G, shift, f, b0 + t);
+      const DiffState ds = diff_state<kCorr>(G, C.par_sel, shift, f, b0 + t);
       if (ds.par_out || (G.flags & kFlagFrameCorr)) {  // the buffer state of flags M and c (DiffState)
         eval_column<Acc, FrameT, TplT, kCorr, false, false, true>(G, (size_t)(b0 + t) * Hb, global_geo<Acc>(G, t), k,
                                                                   out, c, nullptr, t, TWin{nullptr, 0, 0, 0}, ds);
@@ -1099,9 +1106,9 @@ __device__ __forceinline__ void ls_decide(const GroupDesc& G, GroupCtl& C, int f
   }
 }
 
-// One trial of the line search for the frames of one trial tile: block column cc of the ns <= 8
-// searching frames listed at list[pos..pos+ns) (batch frame indices, ss_sched.cuh); the last column
-// of a frame to arrive decides for the frame (ls_decide).
+// One trial of the line search for the frames of one trial tile: block column cc of the
+// ns <= kTrialTileFrames searching frames listed at list[pos..pos+ns) (batch frame indices,
+// ss_sched.cuh); the last column of a frame to arrive decides for the frame (ls_decide).
 template <class FrameT, class TplT>
 __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int cc, int pos, int ns,
                                            const int* __restrict__ list, unsigned char* smem, uint64_t* bar,

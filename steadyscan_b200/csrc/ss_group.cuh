@@ -845,6 +845,7 @@ __global__ void k_after_ls(const GroupDesc* __restrict__ gds, GroupCtl* __restri
   }
   C.exec_result = C.improved;
   C.phase = kPhIterEnd;
+  C.par_sel ^= G.dparity != nullptr;  // the correlation pass's parity bitmap is the current one
 }
 
 __device__ inline double pearson(double n, double sd, double si, double sdd, double sii, double sdi) {

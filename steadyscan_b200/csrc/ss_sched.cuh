@@ -163,9 +163,15 @@ __device__ __forceinline__ bool fetch_tile(int* __restrict__ sched, int cap, int
 // group. Tiles of fixed frame chunks then leave most warps of a CTA idle, so the trial schedule
 // lists the searching frames themselves: one CTA compacts them (in frame order, hence grouped by
 // group) and cuts each group's run into entries of up to kTrialTileFrames consecutive listed frames,
-// each standing for the group's W tiles (one block column each); a tile's warps take one frame each.
+// each standing for the group's W tiles (one block column each); a tile's warps take its frames in
+// turn. Each tile stages one template window for its frames, so tiles of 32 frames spend a quarter
+// of the staging of tiles of 8 (512x512 frames, 2-line knots, groups of 64: trial rounds 85 ms with
+// 32 frames per tile, 94 ms with 8).
 
-constexpr int kTrialTileFrames = 8;
+#ifndef SS_TRIAL_TILE_FRAMES
+#define SS_TRIAL_TILE_FRAMES 32
+#endif
+constexpr int kTrialTileFrames = SS_TRIAL_TILE_FRAMES;
 
 // Buffer: header, list[nf] (batch frame index of each searching frame), first[ng] and end[ng] (each
 // group's run in the list), then grp[nf], pos[nf], cnt[nf] (entries) and prefix[nf + 1] (tiles).

@@ -71,8 +71,9 @@ def test_lambda_regulariser(solver):
 @pytest.mark.parametrize("flags", ["D", "S"])
 def test_assembly_keeps_columns_with_unchanged_knots(flags):
     """Block columns whose knots did not move since their last assembly keep its sums instead of
-    reading the frame again; the run still matches the oracle (D) or the bound (S)."""
-    args, _, _ = make_args(n_frames=8, seed=23, frame_dtype=np.uint16)
+    reading the frame again; the run still matches the oracle (D) or the bound (S). In this case
+    frames stand still for whole iterations (their knots equal across the oracle's knot history)."""
+    args, _, _ = make_args(n_frames=16, seed=23, frame_dtype=np.uint16)
     o = oracle.align_group(args)
     b = api.Batch([dict(args, flags=flags)], want_mask=True)
     b.run()
