@@ -1159,7 +1159,10 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     window_rows(G, G.col_yrange[2 * cc] + klo, G.col_yrange[2 * cc + 1] + khi, win_cap, r0, rows);
     if (rows > 0) {
       float* wbuf = reinterpret_cast<float*>(smem);
-      if (stage_window(G, wbuf, r0, rows, bar, bar_phase)) win = {wbuf, r0, rows, G.tpitch};
+      // tiles on the 16-byte path (every windowed frame of a quad_ok group takes it) read the
+      // four-plane rows
+      const float* src = (sizeof(FrameT) == 2 && G.quad_ok) ? G.tplain4 : G.tplain;
+      if (stage_window(G, wbuf, r0, rows, bar, bar_phase, src)) win = {wbuf, r0, rows, G.tpitch};
       else win_ok = false;  // a copy may still be in flight: no further windows in this CTA
     }
   }
@@ -1182,7 +1185,7 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     if constexpr (sizeof(FrameT) == 2) quads = win.p && G.quad_ok;
     if (quads) {
       if constexpr (sizeof(FrameT) == 2)
-        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane), pair_win(win), ssd, cnt);
+        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane), pair_win4(win), ssd, cnt);
     } else if (win.p && G.pair_ok) {
       trial_pairs<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(win), ssd, cnt);
     } else {

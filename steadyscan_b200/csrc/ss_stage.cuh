@@ -78,11 +78,13 @@ __device__ __forceinline__ void window_rows(const GroupDesc& G, float ylo, float
 // batch's error word: the copy may then still be in flight, so the phase is left as it is, the
 // caller stages no further window in this CTA (its later tiles and passes sample the global
 // template instead) and calls drain_window before the CTA exits.
+// src: the rows to copy from (G.tplain, or G.tplain4 for the four-plane layout).
 __device__ __forceinline__ bool stage_window(const GroupDesc& G, float* win, int r0, int rows, uint64_t* bar,
-                                           unsigned& phase) {
+                                           unsigned& phase, const float* src = nullptr) {
   __syncthreads();  // the previous window is no longer read
+  if (!src) src = G.tplain;
   if (threadIdx.x == 0)
-    bulk_copy(win, G.tplain + (size_t)r0 * G.tpitch, (unsigned)((size_t)rows * G.tpitch * sizeof(float)), bar);
+    bulk_copy(win, src + (size_t)r0 * G.tpitch, (unsigned)((size_t)rows * G.tpitch * sizeof(float)), bar);
   bool ok = mbar_wait(bar, phase);
   if (!ok) ok = mbar_wait(bar, phase);  // second bounded wait for the copy still in flight
   if (!ok && threadIdx.x == 0) atomicOr(G.err, 1);
