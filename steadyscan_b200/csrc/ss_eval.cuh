@@ -1173,6 +1173,8 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
   }
 
   const bool affine = G.geo_k > 0;
+  // without a staged window the pixel-pair paths read the template rows in global memory (L1)
+  const bool grows = !win.p && G.tplain != nullptr && !G.gquad;
   for (int i = warp; i < ns; i += kEvalWarps) {
     const int f = s_list[i];
     const int c = f * W + cc;
@@ -1182,12 +1184,19 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     double ssd;
     int cnt;
     bool quads = false;
-    if constexpr (sizeof(FrameT) == 2) quads = win.p && G.quad_ok;
-    if (quads) {
+    if constexpr (sizeof(FrameT) == 2) quads = G.quad_ok;
+    if (quads && win.p) {
       if constexpr (sizeof(FrameT) == 2)
         trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane), pair_win4(win), ssd, cnt);
+    } else if (quads && grows) {  // the whole template's rows in global memory as the window
+      if constexpr (sizeof(FrameT) == 2)
+        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane),
+                              pair_win4(TWin{G.tplain4, 0, G.Ht, G.tpitch}), ssd, cnt);
     } else if (win.p && G.pair_ok) {
       trial_pairs<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(win), ssd, cnt);
+    } else if (grows && G.pair_ok) {
+      trial_pairs<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(TWin{G.tplain, 0, G.Ht, G.tpitch}), ssd,
+                          cnt);
     } else {
       ColKnots<float> k;
       set_knots(k, x0, x1, y0, y1, x0, x1, y0, y1);
