@@ -108,12 +108,20 @@ def _outputs(args: dict, want_mask=True, want_history=False):
     nF = int(args["nFrames"])
     N = w * nF + 1
     mi = int(args["max_iter"])
-    a = dict(dx=np.zeros((w + 1) * nF), dy=np.zeros((w + 1) * nF), frame_corr=np.zeros(nF),
-             iter_used=np.zeros(1, np.int32), residrms=np.zeros(nF), device_init_time=np.zeros(1),
-             raw_params=np.zeros(2 * N), frame_params=np.zeros(2 * (w + 1) * nF),
-             blocks_used=np.zeros(w * nF, np.uint8))
+    flags = args["flags"] if isinstance(args["flags"], str) else bytes(args["flags"]).decode()
+    letters = flags[1:]  # after the precision letter
+    # outputs the library writes in full are left uninitialised; flag p's frame-ordered layout leaves
+    # dx/dy unwritten, and the knot layouts of flags P and p exist only with those flags
+    knots = np.zeros if "p" in letters else np.empty
+    a = dict(dx=knots((w + 1) * nF), dy=knots((w + 1) * nF), frame_corr=np.empty(nF),
+             iter_used=np.zeros(1, np.int32), residrms=np.empty(nF), device_init_time=np.zeros(1),
+             blocks_used=np.empty(w * nF, np.uint8))
+    if "P" in letters:
+        a["raw_params"] = np.zeros(2 * N)
+    if "p" in letters:
+        a["frame_params"] = np.zeros(2 * (w + 1) * nF)
     if want_mask:
-        a["mask"] = np.zeros(hb * w * nF, np.uint8)
+        a["mask"] = np.empty(hb * w * nF, np.uint8)
     if want_history:
         a["iteration_corr"] = np.zeros(mi)
         a["frame_corr_history"] = np.zeros(nF * mi)
@@ -132,8 +140,8 @@ def _result(o: SSOutputs, a: dict, dims) -> dict:
              residrms=a["residrms"], device_init_time=float(a["device_init_time"][0]),
              stop_reason=int(o.stop_reason), stop_name=STOP_NAMES[o.stop_reason] if 0 <= o.stop_reason < 5 else "?",
              trial_cap_hit=bool(o.trial_cap_hit), n_frame_passes=int(o.n_frame_passes),
-             elapsed_ms=float(o.elapsed_ms), raw_params=a["raw_params"],
-             frame_params=a["frame_params"].reshape(nF, 2 * (w + 1), order="F"),
+             elapsed_ms=float(o.elapsed_ms), raw_params=a.get("raw_params"),
+             frame_params=a["frame_params"].reshape(nF, 2 * (w + 1), order="F") if "frame_params" in a else None,
              blocks_used=a["blocks_used"].reshape(w, nF, order="F").astype(bool))
     if "mask" in a:
         r["mask"] = a["mask"].reshape(hb, w * nF, order="F").astype(bool)

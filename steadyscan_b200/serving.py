@@ -94,6 +94,7 @@ class Request:
     t_admit: float = 0.0
     t_done: float = 0.0
     result: dict | None = None
+    in_burst: bool = False       # caller's label for latency reports (e.g. arrived during a load burst)
     _c: tuple | None = None      # ctypes inputs/outputs kept alive while the group runs
 
     @property
