@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define SS_ABI_VERSION 3
+#define SS_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define SS_API __attribute__((visibility("default")))
@@ -299,6 +299,39 @@ SS_API int ss_estimate_displacements(const ss_recording* rec, ss_recording_outpu
  * *n_sets and fills at most max_sets entries. */
 SS_API int ss_recording_sets(int32_t n_frames, int32_t frames_per_set, int32_t min_frames_per_set, int32_t* first,
                              int32_t* count, int32_t max_sets, int32_t* n_sets);
+
+/* ---------------------------------------------------------------------------------------------
+ * Caller-side preparation of frames on the GPU: what the reference's MATLAB driver does to the raw
+ * frames of a set before its MEX call (steady_scan.m:229-234): prefilter_foralignment
+ * (:625-643), cropimage (:830-834) and image2blockmatrix (:601-613) of every frame.
+ *
+ * prefilter_foralignment: with pregauss > 0 each frame is blurred by the reference's periodic FFT
+ * convolution with a Gaussian of that standard deviation on the frame padded by
+ * L = ceil(sqrt(2 pregauss^2 log(10000 / (sqrt(2 pi) pregauss)))) zero rows and columns; with
+ * mednorm != 0 each (blurred) frame is then divided by the median of its samples. Both are applied
+ * to the whole frame before cropping, as in the reference. The blur needs pregauss < 3989 (the
+ * reference's L is not real above that).
+ *
+ * gather: the caller's block map (host memory), block_h x n_blocks column-major: for entry (r, b)
+ * the 0-based column-major index of the cropped frame's pixel there, -1 where the block has fewer
+ * pixels (the positions of settings.prevknotind == b + 1 in column-major order, steady_scan.m:609).
+ * out: block_h x (n_blocks * n_frames) in device memory, SS_F64, SS_F32 or SS_U16 (SS_U16 only for
+ * SS_U16 frames without prefilter, whose samples it copies exactly). Synchronous; allocates work
+ * memory for the prefilter. */
+typedef struct ss_prep_frames {
+  ss_matrix frames;      /* H x (W * n_frames) column-major (frame k in columns k W .. k W + W - 1),
+                            host or device, any ss_dtype */
+  int32_t n_frames;
+  double pregauss;       /* settings.pregauss (0: no blur) */
+  int32_t mednorm;       /* settings.mednorm */
+  int32_t cropping[4];   /* settings.cropping: [left right bottom top] pixels removed */
+  const int32_t* gather; /* block_h x n_blocks column-major, host memory */
+  int32_t block_h, n_blocks;
+  ss_matrix out;         /* device memory, block_h x (n_blocks * n_frames) */
+  int32_t gpu_device_id;
+} ss_prep_frames;
+
+SS_API int ss_prepare_frames(const ss_prep_frames* p);
 
 /* Message of the calling thread's last error ("" if none). */
 SS_API const char* ss_last_error(void);

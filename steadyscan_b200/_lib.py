@@ -57,6 +57,12 @@ class SSRecordingOutputs(C.Structure):
                 ("n_sets", C.c_int32)]
 
 
+class SSPrepFrames(C.Structure):
+    _fields_ = [("frames", SSMatrix), ("n_frames", C.c_int32), ("pregauss", C.c_double), ("mednorm", C.c_int32),
+                ("cropping", C.c_int32 * 4), ("gather", C.c_void_p), ("block_h", C.c_int32), ("n_blocks", C.c_int32),
+                ("out", SSMatrix), ("gpu_device_id", C.c_int32)]
+
+
 class SSBatchStats(C.Structure):
     _fields_ = [("n_groups", C.c_int32), ("cycles", C.c_int32), ("linesearch_rounds", C.c_int32),
                 ("kernel_launches", C.c_int32), ("frame_passes", C.c_int64 * 4), ("eval_ms", C.c_double * 4),
@@ -138,6 +144,8 @@ def load(build_if_missing: bool = True):
     lib.ss_recording_sets.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                       C.c_int32, C.POINTER(C.c_int32)]
     lib.ss_recording_sets.restype = C.c_int
+    lib.ss_prepare_frames.argtypes = [C.POINTER(SSPrepFrames)]
+    lib.ss_prepare_frames.restype = C.c_int
     _lib = lib
     return lib
 

@@ -19,10 +19,10 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (SS_DEVICE, SS_F16, SS_F32, SS_F64, SS_HOST, SS_I32, SS_U8, SS_U16, STOP_NAMES, SSInputs,
-                   SSMatrix, SSOutputs, SteadyScanError, check, load)
+                   SSMatrix, SSOutputs, SSPrepFrames, SteadyScanError, check, load)
 
 __all__ = ["align_group_to_template", "align_group", "align_groups", "estimate_displacements", "recording_sets",
-           "DeviceMatrix", "SteadyScanError", "ARG_NAMES", "STOP_NAMES"]
+           "prepare_frames", "DeviceMatrix", "SteadyScanError", "ARG_NAMES", "STOP_NAMES"]
 
 ARG_NAMES = ["flags", "template_image", "xgrad", "ygrad", "tfrac", "basex", "basey", "base_mask", "bmData",
              "est_dx_knots", "est_dy_knots", "group_size", "nFrames", "min_points_per_block", "max_iter",
@@ -212,6 +212,59 @@ def align_group_to_template(*argv, nargout: int = 6, template_storage=None):
         outs += [r["iteration_corr"], None, None, r["frame_corr_history"], r["iteration_errvals"], r["raw_params"],
                  None, r["all_params"]]
     return tuple(outs[:nargout])
+
+
+def prepare_frames(frames, layout, pregauss: float = 0.0, mednorm: bool = False, out_dtype=np.float64,
+                   device: int = 0, n_frames: int | None = None):
+    """The reference driver's preparation of raw frames on the GPU (ss_prepare_frames):
+    prefilter_foralignment (Gaussian blur of std ``pregauss``, then division by each frame's median
+    when ``mednorm``; steady_scan.m:625-643), cropimage and image2blockmatrix (steady_scan.m:229-234)
+    of every frame. ``frames``: H x W x n (numpy in any memory order, or a CUDA tensor whose frames
+    are column-major, i.e. ``t.permute(2, 1, 0)`` contiguous, or a DeviceMatrix of H x (W * n));
+    ``layout``: prep.BlockLayout (block map and cropping); ``n_frames`` is needed for a DeviceMatrix.
+    Returns the block matrix
+    frame_h x (frame_w * n) as a column-major CUDA tensor of ``out_dtype`` (float64, float32, or
+    uint16 for uint16 frames without prefilter)."""
+    import torch
+
+    from . import prep
+    lib = load()
+    keep = []
+    if isinstance(frames, DeviceMatrix):
+        if not n_frames:
+            raise ValueError("n_frames is needed for a DeviceMatrix of frames")
+        fm = SSMatrix(frames.ptr, frames.rows, frames.cols, frames.dtype, SS_DEVICE)
+        n = int(n_frames)
+    elif hasattr(frames, "is_cuda") and frames.is_cuda:
+        t = frames if frames.dim() == 3 else frames[:, :, None]
+        if not t.permute(2, 1, 0).is_contiguous():
+            raise ValueError("CUDA frames must be column-major per frame (t.permute(2, 1, 0) contiguous)")
+        keep.append(t)
+        h, w, n = t.shape
+        fm = SSMatrix(t.data_ptr(), h, w * n, _TORCH_DTYPE[str(t.dtype)], SS_DEVICE)
+    else:
+        a = np.asarray(frames)
+        if a.ndim == 2:
+            a = a[:, :, None]
+        if a.dtype not in _NP_DTYPE or a.dtype in (np.bool_, np.uint8, np.int32):
+            a = a.astype(np.float64)
+        a = np.asfortranarray(a)
+        keep.append(a)
+        h, w, n = a.shape
+        fm = SSMatrix(a.ctypes.data, h, w * n, _NP_DTYPE[a.dtype], SS_HOST)
+    gidx = np.asfortranarray(prep._block_gather_index(layout.prevknotind, layout.frame_w).astype(np.int32))
+    hb, nb = gidx.shape
+    tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32,
+           np.dtype(np.uint16): torch.uint16}[np.dtype(out_dtype)]
+    out = torch.empty((nb * n, hb), dtype=tdt, device=f"cuda:{device}").T  # column-major hb x (nb n)
+    odt = {torch.float64: SS_F64, torch.float32: SS_F32, torch.uint16: SS_U16}[tdt]
+    om = SSMatrix(out.data_ptr(), hb, nb * n, odt, SS_DEVICE)
+    crop = layout.cropping if layout.cropping else [0, 0, 0, 0]
+    p = SSPrepFrames(fm, int(n), float(pregauss), int(bool(mednorm)), (C.c_int32 * 4)(*[int(c) for c in crop]),
+                     gidx.ctypes.data, int(hb), int(nb), om, int(device))
+    check(lib.ss_prepare_frames(C.byref(p)))
+    del keep
+    return out
 
 
 def recording_sets(n_frames: int, frames_per_set: int = 500, min_frames_per_set: int = 100):

@@ -25,6 +25,7 @@
 #include "ss_eval.cuh"
 #include "ss_group.cuh"
 #include "ss_recording.cuh"
+#include "ss_frontend.cuh"
 #include "steadyscan_b200.h"
 
 namespace ss {
@@ -1931,6 +1932,175 @@ void* Batch::stream() const { return d->stream; }
 }  // namespace ss
 
 // ---------------------------------------------------------------------------------------------
+// Caller-side preparation of frames (ss_frontend.cuh)
+
+namespace ss {
+
+// Normalised taps of one axis of the reference's periodic Gaussian (steady_scan.m:628-633): the
+// weights at circular distance 0..R in a period of `period` samples, divided by the axis' sum over
+// the whole period (the 2-D normalisation is the product of the two axes' sums).
+static std::vector<double> blur_taps(double sd, int period, int* r_out) {
+  auto g = [&](int d) {
+    const double c = (double)std::min(d, period - d);
+    return std::exp(-c * c / (2.0 * sd * sd));
+  };
+  double sum = 0.0;
+  for (int d = 0; d < period; d++) sum += g(d);
+  const int R = std::min((int)std::ceil(9.6 * sd), (period - 1) / 2);
+  std::vector<double> t((size_t)R + 1);
+  for (int d = 0; d <= R; d++) t[d] = g(d) / sum;
+  *r_out = R;
+  return t;
+}
+
+template <class T>
+__global__ void k_to_f64(const void* __restrict__ in, double* __restrict__ out, size_t n) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = to_double(reinterpret_cast<const T*>(in)[e]);
+}
+
+template <class InT>
+static void fe_blur(const void* in, double* w1, double* w2, int h, int w, int n, int ph, int pw, const double* ty,
+                    int ry, const double* tx, int rx, cudaStream_t s) {
+  const int nb = 148 * 8;
+  k_blur_pass<InT, 0><<<nb, 256, 0, s>>>(in, w1, h, w, n, ph, ty, ry);
+  k_blur_pass<double, 1><<<nb, 256, 0, s>>>(w1, w2, h, w, n, pw, tx, rx);
+}
+
+template <class InT>
+static void fe_gather(const void* in, int out_dt, void* out, int h, int w, int n, int r0, int c0, int hc,
+                      const int* gather, int hb, int nb, cudaStream_t s) {
+  const int g = 148 * 8;
+  if (out_dt == SS_F64) k_block_gather<InT, double><<<g, 256, 0, s>>>(in, (double*)out, h, w, n, r0, c0, hc, gather, hb, nb);
+  else if (out_dt == SS_F32) k_block_gather<InT, float><<<g, 256, 0, s>>>(in, (float*)out, h, w, n, r0, c0, hc, gather, hb, nb);
+  else k_block_gather<InT, uint16_t><<<g, 256, 0, s>>>(in, (uint16_t*)out, h, w, n, r0, c0, hc, gather, hb, nb);
+}
+
+int prepare_frames(const ss_prep_frames* p) {
+  if (!p) return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: no arguments");
+  const int n = p->n_frames;
+  const int64_t h = p->frames.rows;
+  if (n < 1 || h < 1 || p->frames.cols % n != 0 || !p->frames.data)
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: frames must be H x (W * n_frames)");
+  const int64_t w = p->frames.cols / n;
+  const int* cr = p->cropping;
+  if (cr[0] < 0 || cr[1] < 0 || cr[2] < 0 || cr[3] < 0 || cr[0] + cr[1] >= w || cr[2] + cr[3] >= h)
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: cropping leaves no pixel");
+  const int64_t hc = h - cr[2] - cr[3], wc = w - cr[0] - cr[1];
+  const int hb = p->block_h, nbk = p->n_blocks;
+  if (!p->gather || hb < 1 || nbk < 1) return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: empty block map");
+  for (int64_t i = 0; i < (int64_t)hb * nbk; i++)
+    if (p->gather[i] < -1 || p->gather[i] >= hc * wc)
+      return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: block map index outside the cropped frame");
+  const ss_matrix& o = p->out;
+  if (o.location != SS_DEVICE || !o.data || o.rows != hb || o.cols != (int64_t)nbk * n)
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: out must be block_h x (n_blocks * n_frames) on the device");
+  const bool blur = p->pregauss > 0.0, med = p->mednorm != 0;
+  if (o.dtype != SS_F64 && o.dtype != SS_F32 && o.dtype != SS_U16)
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: out must be SS_F64, SS_F32 or SS_U16");
+  if (o.dtype == SS_U16 && (p->frames.dtype != SS_U16 || blur || med))
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: SS_U16 output only copies SS_U16 frames without prefilter");
+  const int fdt = p->frames.dtype;
+  if (fdt != SS_F64 && fdt != SS_F32 && fdt != SS_U16 && fdt != SS_F16)
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: frames must be SS_F64, SS_F32, SS_U16 or SS_F16");
+  if (blur && !(p->pregauss < 3989.0))
+    return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: pregauss must be below 3989");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
+  if (p->gpu_device_id < 0 || p->gpu_device_id >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
+  SS_CK(cudaSetDevice(p->gpu_device_id));
+
+  // padded periods and taps of the blur (steady_scan.m:627-633)
+  int ry = 0, rx = 0, ph = 0, pw = 0;
+  std::vector<double> ty, tx;
+  if (blur) {
+    const double sd = p->pregauss;
+    const int L = (int)std::ceil(std::sqrt((2.0 * sd * sd) * std::log(10000.0 / (std::sqrt(2.0 * M_PI) * sd))));
+    ph = (int)h + L;
+    pw = (int)w + L;
+    ty = blur_taps(sd, ph, &ry);
+    tx = blur_taps(sd, pw, &rx);
+  }
+  const size_t fsz = dtype_size(fdt), osz = dtype_size(o.dtype), npx = (size_t)h * w;
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, ((size_t)1 << 30) / (16 * npx)));
+  struct Mem {
+    std::vector<void*> ptrs;
+    cudaStream_t s = nullptr;
+    ~Mem() {
+      if (s) cudaStreamSynchronize(s);
+      for (void* q : ptrs) cudaFree(q);
+      if (s) cudaStreamDestroy(s);
+    }
+    void* take(size_t b) {
+      void* q = nullptr;
+      if (cudaMalloc(&q, b) != cudaSuccess) return nullptr;
+      ptrs.push_back(q);
+      return q;
+    }
+  } m;
+  SS_CK(cudaStreamCreateWithFlags(&m.s, cudaStreamNonBlocking));
+  cudaStream_t s = m.s;
+  int* d_gather = (int*)m.take((size_t)hb * nbk * sizeof(int));
+  double* d_taps = blur ? (double*)m.take((ty.size() + tx.size()) * sizeof(double)) : nullptr;
+  void* d_raw = p->frames.location == SS_HOST ? m.take(fsz * npx * chunk) : nullptr;
+  double* w1 = (blur || med) ? (double*)m.take(8 * npx * chunk) : nullptr;
+  double* w2 = blur ? (double*)m.take(8 * npx * chunk) : nullptr;
+  double* d_med = med ? (double*)m.take(sizeof(double) * chunk) : nullptr;
+  if (!d_gather || (blur && !d_taps) || (p->frames.location == SS_HOST && !d_raw) || ((blur || med) && !w1) ||
+      (blur && !w2) || (med && !d_med))
+    return fail(SS_ERR_OUT_OF_MEMORY, "prepare_frames: work memory");
+  SS_CK(cudaMemcpyAsync(d_gather, p->gather, (size_t)hb * nbk * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (blur) {
+    SS_CK(cudaMemcpyAsync(d_taps, ty.data(), ty.size() * 8, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync(d_taps + ty.size(), tx.data(), tx.size() * 8, cudaMemcpyHostToDevice, s));
+  }
+  const int r0 = cr[2], c0 = cr[0];
+  const int g = 148 * 8;
+  for (int f0 = 0; f0 < n; f0 += chunk) {
+    const int c = std::min(chunk, n - f0);
+    const char* src = static_cast<const char*>(p->frames.data) + fsz * npx * f0;
+    if (d_raw) {
+      SS_CK(cudaMemcpyAsync(d_raw, src, fsz * npx * c, cudaMemcpyHostToDevice, s));
+      src = static_cast<const char*>(d_raw);
+    }
+    const void* cur = src;
+    int cur_dt = fdt;
+    if (blur) {  // prefilter_foralignment's blur, then its samples in FP64
+      const double* dty = d_taps;
+      const double* dtx = d_taps + ty.size();
+      if (fdt == SS_F64) fe_blur<double>(src, w1, w2, (int)h, (int)w, c, ph, pw, dty, ry, dtx, rx, s);
+      else if (fdt == SS_F32) fe_blur<float>(src, w1, w2, (int)h, (int)w, c, ph, pw, dty, ry, dtx, rx, s);
+      else if (fdt == SS_U16) fe_blur<uint16_t>(src, w1, w2, (int)h, (int)w, c, ph, pw, dty, ry, dtx, rx, s);
+      else fe_blur<__half>(src, w1, w2, (int)h, (int)w, c, ph, pw, dty, ry, dtx, rx, s);
+      cur = w2;
+      cur_dt = SS_F64;
+    } else if (med) {  // the median division works on FP64 samples
+      if (fdt == SS_F64) k_to_f64<double><<<g, 256, 0, s>>>(src, w1, npx * c);
+      else if (fdt == SS_F32) k_to_f64<float><<<g, 256, 0, s>>>(src, w1, npx * c);
+      else if (fdt == SS_U16) k_to_f64<uint16_t><<<g, 256, 0, s>>>(src, w1, npx * c);
+      else k_to_f64<__half><<<g, 256, 0, s>>>(src, w1, npx * c);
+      cur = w1;
+      cur_dt = SS_F64;
+    }
+    if (med) {
+      double* x = const_cast<double*>(static_cast<const double*>(cur));
+      k_frame_median<double><<<c, 1024, 0, s>>>(x, npx, d_med);
+      k_frame_divide<<<g, 256, 0, s>>>(x, npx, npx * c, d_med);
+    }
+    void* dst = static_cast<char*>(const_cast<void*>(o.data)) + osz * (size_t)hb * nbk * f0;
+    if (cur_dt == SS_F64) fe_gather<double>(cur, o.dtype, dst, (int)h, (int)w, c, r0, c0, (int)hc, d_gather, hb, nbk, s);
+    else if (cur_dt == SS_F32) fe_gather<float>(cur, o.dtype, dst, (int)h, (int)w, c, r0, c0, (int)hc, d_gather, hb, nbk, s);
+    else if (cur_dt == SS_U16) fe_gather<uint16_t>(cur, o.dtype, dst, (int)h, (int)w, c, r0, c0, (int)hc, d_gather, hb, nbk, s);
+    else fe_gather<__half>(cur, o.dtype, dst, (int)h, (int)w, c, r0, c0, (int)hc, d_gather, hb, nbk, s);
+    SS_CK(cudaGetLastError());
+  }
+  SS_CK(cudaStreamSynchronize(s));
+  return SS_OK;
+}
+
+}  // namespace ss
+
+// ---------------------------------------------------------------------------------------------
 // C ABI
 
 extern "C" {
@@ -2222,6 +2392,12 @@ int ss_estimate_displacements(const ss_recording* rec, ss_recording_outputs* out
 int ss_recording_sets(int32_t n_frames, int32_t frames_per_set, int32_t min_frames_per_set, int32_t* first,
                       int32_t* count, int32_t max_sets, int32_t* n_sets) {
   int rc = ss::recording_sets(n_frames, frames_per_set, min_frames_per_set, first, count, max_sets, n_sets);
+  if (!rc) ss::g_err.clear();
+  return rc;
+}
+
+int ss_prepare_frames(const ss_prep_frames* p) {
+  int rc = ss::prepare_frames(p);
   if (!rc) ss::g_err.clear();
   return rc;
 }

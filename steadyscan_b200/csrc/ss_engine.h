@@ -63,6 +63,9 @@ class Batch {
 // group of one batch, then the caller's post-estimate rules on the device.
 int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out);
 // Set split of ss_recording_sets (0-based first frame and frame count per set, overlap included).
+// ss_prepare_frames: prefilter, crop and block-reorder raw frames on the device (ss_frontend.cuh).
+int prepare_frames(const ss_prep_frames* p);
+
 int recording_sets(int n_frames, int frames_per_set, int min_frames_per_set, int* first, int* count, int max_sets,
                    int* n_sets);
 

@@ -36,7 +36,7 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.ss_abi_version() == 3  # ss_outputs gained blocks_used; recording-level entry points
+    assert lib.ss_abi_version() == 4  # ss_prepare_frames (frame preparation on the device)
 
 
 def test_struct_sizes_match_header(lib):
@@ -44,6 +44,12 @@ def test_struct_sizes_match_header(lib):
     assert C.sizeof(_lib.SSOutputs) == 13 * 8 + 4 + 4 + 8 + 8 + 8
     assert _lib.SSRecording.corr_thresh.offset == C.sizeof(_lib.SSInputs) + 8
     assert C.sizeof(_lib.SSRecordingOutputs) == 7 * 8 + 8
+    # ss_prep_frames: ss_matrix (32), n_frames (+pad), pregauss at 40, mednorm 48, cropping 52..68,
+    # gather at 72, block_h/n_blocks, out at 88, gpu_device_id at 120, padded to 128
+    assert _lib.SSPrepFrames.pregauss.offset == 40
+    assert _lib.SSPrepFrames.gather.offset == 72
+    assert _lib.SSPrepFrames.out.offset == 88
+    assert C.sizeof(_lib.SSPrepFrames) == 128
 
 
 def _expect_invalid(args, match):
