@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define SS_ABI_VERSION 4
+#define SS_ABI_VERSION 5
 
 #if defined(__GNUC__)
 #define SS_API __attribute__((visibility("default")))
@@ -332,6 +332,40 @@ typedef struct ss_prep_frames {
 } ss_prep_frames;
 
 SS_API int ss_prepare_frames(const ss_prep_frames* p);
+
+/* ---------------------------------------------------------------------------------------------
+ * Reconstruction on the GPU: invert_bilinear_sampling of the reference's MATLAB driver
+ * (steady_scan.m:290-404) for the frames of one set, i.e. one call of it (steady_scan.m:128-135).
+ * Every frame is reconstructed on the template grid from its knots as the least-squares inverse of
+ * its bilinear sampling with the adjacent-difference regulariser (ibs_regfac; vertical differences
+ * weighted by 1 / ibs_template_pixel_aspect_ratio), by the reference's 4-colour Gauss-Seidel
+ * iteration from its push-grid first guess, stopped when the energy stops decreasing at the
+ * reference's check interval, which is carried from frame to frame within the call. Pixels the
+ * frame does not constrain are NaN in the output and false in the mask. The reference's optional
+ * least-squares gap filling (ibs_inpaint, default off) is not done. Synchronous.
+ *
+ * Extra channels (steady_scan.m:137-154) are the same call with the channel's frames and the same
+ * knots. */
+typedef struct ss_reconstruct {
+  ss_matrix frames;       /* h x (w * n_frames): the set's cropped (and prefiltered) frames, FP32 or
+                             FP64, host or device */
+  int32_t n_frames;
+  ss_matrix basex;        /* h x w: settings.basex (1-based template x of each pixel), FP64 */
+  ss_matrix basey;        /* h x w: settings.basey, FP64 */
+  ss_matrix tfrac;        /* h x w: settings.tfrac, FP64 */
+  ss_matrix prevknotind;  /* h x w: settings.prevknotind (1-based), SS_I32 or FP64 */
+  ss_matrix dx_knots;     /* nknots x n_frames, FP64 (host) */
+  ss_matrix dy_knots;
+  int32_t template_h, template_w;  /* corrected_data_size = size(template_image) */
+  double regfac;          /* settings.ibs_regfac (default 3e-3) */
+  double pixel_aspect_ratio;  /* settings.ibs_template_pixel_aspect_ratio (default 1) */
+  ss_matrix out;          /* template_h x (template_w * n_frames), FP32 or FP64, host or device */
+  uint8_t* mask;          /* template_h x (template_w * n_frames) host, or NULL */
+  int32_t* iterations;    /* n_frames host, or NULL: Gauss-Seidel sweeps of each frame (0: skipped) */
+  int32_t gpu_device_id;
+} ss_reconstruct;
+
+SS_API int ss_reconstruct_frames(const ss_reconstruct* r);
 
 /* Message of the calling thread's last error ("" if none). */
 SS_API const char* ss_last_error(void);

@@ -63,6 +63,14 @@ class SSPrepFrames(C.Structure):
                 ("out", SSMatrix), ("gpu_device_id", C.c_int32)]
 
 
+class SSReconstruct(C.Structure):
+    _fields_ = [("frames", SSMatrix), ("n_frames", C.c_int32), ("basex", SSMatrix), ("basey", SSMatrix),
+                ("tfrac", SSMatrix), ("prevknotind", SSMatrix), ("dx_knots", SSMatrix), ("dy_knots", SSMatrix),
+                ("template_h", C.c_int32), ("template_w", C.c_int32), ("regfac", C.c_double),
+                ("pixel_aspect_ratio", C.c_double), ("out", SSMatrix), ("mask", C.c_void_p),
+                ("iterations", C.c_void_p), ("gpu_device_id", C.c_int32)]
+
+
 class SSBatchStats(C.Structure):
     _fields_ = [("n_groups", C.c_int32), ("cycles", C.c_int32), ("linesearch_rounds", C.c_int32),
                 ("kernel_launches", C.c_int32), ("frame_passes", C.c_int64 * 4), ("eval_ms", C.c_double * 4),
@@ -146,6 +154,8 @@ def load(build_if_missing: bool = True):
     lib.ss_recording_sets.restype = C.c_int
     lib.ss_prepare_frames.argtypes = [C.POINTER(SSPrepFrames)]
     lib.ss_prepare_frames.restype = C.c_int
+    lib.ss_reconstruct_frames.argtypes = [C.POINTER(SSReconstruct)]
+    lib.ss_reconstruct_frames.restype = C.c_int
     _lib = lib
     return lib
 

@@ -19,10 +19,10 @@ import ctypes as C
 import numpy as np
 
 from ._lib import (SS_DEVICE, SS_F16, SS_F32, SS_F64, SS_HOST, SS_I32, SS_U8, SS_U16, STOP_NAMES, SSInputs,
-                   SSMatrix, SSOutputs, SSPrepFrames, SteadyScanError, check, load)
+                   SSMatrix, SSOutputs, SSPrepFrames, SSReconstruct, SteadyScanError, check, load)
 
 __all__ = ["align_group_to_template", "align_group", "align_groups", "estimate_displacements", "recording_sets",
-           "prepare_frames", "DeviceMatrix", "SteadyScanError", "ARG_NAMES", "STOP_NAMES"]
+           "prepare_frames", "reconstruct_frames", "DeviceMatrix", "SteadyScanError", "ARG_NAMES", "STOP_NAMES"]
 
 ARG_NAMES = ["flags", "template_image", "xgrad", "ygrad", "tfrac", "basex", "basey", "base_mask", "bmData",
              "est_dx_knots", "est_dy_knots", "group_size", "nFrames", "min_points_per_block", "max_iter",
@@ -265,6 +265,55 @@ def prepare_frames(frames, layout, pregauss: float = 0.0, mednorm: bool = False,
     check(lib.ss_prepare_frames(C.byref(p)))
     del keep
     return out
+
+
+def reconstruct_frames(frames, dx_knots, dy_knots, settings: dict, template_shape, out_dtype=np.float32,
+                       device: int = 0) -> dict:
+    """invert_bilinear_sampling of the reference's driver for one set of frames
+    (ss_reconstruct_frames, steady_scan.m:290-404): ``frames`` h x w x n (cropped, prefiltered;
+    FP32 or FP64 numpy, or a CUDA tensor column-major per frame), ``dx_knots``/``dy_knots`` nknots x
+    n, ``settings`` from prep.init_settings (basex, basey, tfrac, prevknotind, ibs_regfac,
+    ibs_template_pixel_aspect_ratio), ``template_shape`` (th, tw). Returns the corrected frames
+    (th x tw x n numpy of out_dtype, NaN where unconstrained), the mask and the sweeps per frame."""
+    lib = load()
+    keep = []
+    if hasattr(frames, "is_cuda") and frames.is_cuda:
+        t = frames if frames.dim() == 3 else frames[:, :, None]
+        if not t.permute(2, 1, 0).is_contiguous():
+            raise ValueError("CUDA frames must be column-major per frame (t.permute(2, 1, 0) contiguous)")
+        keep.append(t)
+        h, w, n = t.shape
+        fm = SSMatrix(t.data_ptr(), h, w * n, _TORCH_DTYPE[str(t.dtype)], SS_DEVICE)
+    else:
+        a = np.asarray(frames)
+        if a.ndim == 2:
+            a = a[:, :, None]
+        if a.dtype not in (np.float32, np.float64):
+            a = a.astype(np.float32)
+        a = np.asfortranarray(a)
+        keep.append(a)
+        h, w, n = a.shape
+        fm = SSMatrix(a.ctypes.data, h, w * n, _NP_DTYPE[a.dtype], SS_HOST)
+    th, tw = (int(v) for v in template_shape)
+    out = np.empty((th, tw, n), dtype=out_dtype, order="F")
+    mask = np.empty((th, tw, n), dtype=np.uint8, order="F")
+    iters = np.zeros(n, np.int32)
+
+    def mat(x, dt=np.float64):
+        arr = np.asfortranarray(np.asarray(x, dtype=dt))
+        if arr.ndim == 1:
+            arr = arr.reshape(-1, 1)
+        keep.append(arr)
+        return SSMatrix(arr.ctypes.data, arr.shape[0], arr.shape[1], _NP_DTYPE[arr.dtype], SS_HOST)
+
+    r = SSReconstruct(fm, int(n), mat(settings["basex"]), mat(settings["basey"]), mat(settings["tfrac"]),
+                      mat(settings["prevknotind"], np.int32), mat(dx_knots), mat(dy_knots), th, tw,
+                      float(settings.get("ibs_regfac", 3e-3)), float(settings.get("ibs_template_pixel_aspect_ratio", 1.0)),
+                      SSMatrix(out.ctypes.data, th, tw * n, _NP_DTYPE[out.dtype], SS_HOST), mask.ctypes.data,
+                      iters.ctypes.data, int(device))
+    check(lib.ss_reconstruct_frames(C.byref(r)))
+    del keep
+    return {"data_corrected": out, "mask": mask.astype(bool), "iterations": iters}
 
 
 def recording_sets(n_frames: int, frames_per_set: int = 500, min_frames_per_set: int = 100):

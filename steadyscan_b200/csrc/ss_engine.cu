@@ -26,6 +26,7 @@
 #include "ss_group.cuh"
 #include "ss_recording.cuh"
 #include "ss_frontend.cuh"
+#include "ss_reconstruct.cuh"
 #include "steadyscan_b200.h"
 
 namespace ss {
@@ -1936,6 +1937,28 @@ void* Batch::stream() const { return d->stream; }
 
 namespace ss {
 
+// Device allocations and a stream of one synchronous call, released when it returns (the stream
+// drained first).
+struct CallMem {
+  std::vector<void*> ptrs;
+  cudaStream_t s = nullptr;
+  CallMem() = default;
+  CallMem(const CallMem&) = delete;
+  CallMem& operator=(const CallMem&) = delete;
+  ~CallMem() {
+    if (s) cudaStreamSynchronize(s);
+    for (void* q : ptrs) cudaFree(q);
+    if (s) cudaStreamDestroy(s);
+  }
+  template <class T>
+  T* take(size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(1, count) * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(q);
+    return static_cast<T*>(q);
+  }
+};
+
 // Normalised taps of one axis of the reference's periodic Gaussian (steady_scan.m:628-633): the
 // weights at circular distance 0..R in a period of `period` samples, divided by the axis' sum over
 // the whole period (the 2-D normalisation is the product of the two axes' sums).
@@ -2023,29 +2046,15 @@ int prepare_frames(const ss_prep_frames* p) {
   }
   const size_t fsz = dtype_size(fdt), osz = dtype_size(o.dtype), npx = (size_t)h * w;
   const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, ((size_t)1 << 30) / (16 * npx)));
-  struct Mem {
-    std::vector<void*> ptrs;
-    cudaStream_t s = nullptr;
-    ~Mem() {
-      if (s) cudaStreamSynchronize(s);
-      for (void* q : ptrs) cudaFree(q);
-      if (s) cudaStreamDestroy(s);
-    }
-    void* take(size_t b) {
-      void* q = nullptr;
-      if (cudaMalloc(&q, b) != cudaSuccess) return nullptr;
-      ptrs.push_back(q);
-      return q;
-    }
-  } m;
+  CallMem m;
   SS_CK(cudaStreamCreateWithFlags(&m.s, cudaStreamNonBlocking));
   cudaStream_t s = m.s;
-  int* d_gather = (int*)m.take((size_t)hb * nbk * sizeof(int));
-  double* d_taps = blur ? (double*)m.take((ty.size() + tx.size()) * sizeof(double)) : nullptr;
-  void* d_raw = p->frames.location == SS_HOST ? m.take(fsz * npx * chunk) : nullptr;
-  double* w1 = (blur || med) ? (double*)m.take(8 * npx * chunk) : nullptr;
-  double* w2 = blur ? (double*)m.take(8 * npx * chunk) : nullptr;
-  double* d_med = med ? (double*)m.take(sizeof(double) * chunk) : nullptr;
+  int* d_gather = m.take<int>((size_t)hb * nbk);
+  double* d_taps = blur ? m.take<double>(ty.size() + tx.size()) : nullptr;
+  void* d_raw = p->frames.location == SS_HOST ? m.take<char>(fsz * npx * chunk) : nullptr;
+  double* w1 = (blur || med) ? m.take<double>(npx * chunk) : nullptr;
+  double* w2 = blur ? m.take<double>(npx * chunk) : nullptr;
+  double* d_med = med ? m.take<double>(chunk) : nullptr;
   if (!d_gather || (blur && !d_taps) || (p->frames.location == SS_HOST && !d_raw) || ((blur || med) && !w1) ||
       (blur && !w2) || (med && !d_med))
     return fail(SS_ERR_OUT_OF_MEMORY, "prepare_frames: work memory");
@@ -2095,6 +2104,245 @@ int prepare_frames(const ss_prep_frames* p) {
     SS_CK(cudaGetLastError());
   }
   SS_CK(cudaStreamSynchronize(s));
+  return SS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reconstruction (ss_reconstruct.cuh)
+
+// The error-check interval that follows a frame of `iter` sweeps (steady_scan.m:391):
+// int32(max(1, min(10, sqrt(single(iter))))), int32 rounding halves away from zero.
+static int rc_interval(int iter) {
+  const float v = std::max(1.0f, std::min(10.0f, std::sqrt((float)iter)));
+  return (int)std::floor((double)v + 0.5);
+}
+
+static bool host_f64(const ss_matrix& m, int64_t rows, int64_t cols, std::vector<double>& out) {
+  if (m.location != SS_HOST || !m.data || m.rows != rows || m.cols != cols) return false;
+  const size_t n = (size_t)rows * cols;
+  out.resize(n);
+  if (m.dtype == SS_F64) std::memcpy(out.data(), m.data, n * 8);
+  else if (m.dtype == SS_F32) for (size_t i = 0; i < n; i++) out[i] = static_cast<const float*>(m.data)[i];
+  else if (m.dtype == SS_I32) for (size_t i = 0; i < n; i++) out[i] = static_cast<const int32_t*>(m.data)[i];
+  else return false;
+  return true;
+}
+
+int reconstruct_frames(const ss_reconstruct* r) {
+  if (!r) return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: no arguments");
+  const int n = r->n_frames, th = r->template_h, tw = r->template_w;
+  const int64_t hd = r->basex.rows, wd = r->basex.cols;
+  if (n < 1 || th < 2 || tw < 2 || hd < 1 || wd < 1)
+    return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: empty frames or template");
+  const int64_t np64 = (int64_t)th * tw;
+  if (np64 > (1LL << 30) || hd * wd > (1LL << 30)) return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: too large");
+  const int np = (int)np64;
+  const ss_matrix& fr = r->frames;
+  if (!fr.data || fr.rows != hd || fr.cols != wd * n || (fr.dtype != SS_F32 && fr.dtype != SS_F64))
+    return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: frames must be FP32 or FP64 h x (w * n_frames)");
+  const int nk = (int)r->dx_knots.rows;
+  std::vector<double> bx, by, tf, pkd, dxk, dyk;
+  if (!host_f64(r->basex, hd, wd, bx) || !host_f64(r->basey, hd, wd, by) || !host_f64(r->tfrac, hd, wd, tf) ||
+      !host_f64(r->prevknotind, hd, wd, pkd))
+    return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: basex, basey, tfrac, prevknotind must be h x w in host memory");
+  if (nk < 2 || !host_f64(r->dx_knots, nk, n, dxk) || !host_f64(r->dy_knots, nk, n, dyk))
+    return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: dx_knots, dy_knots must be nknots x n_frames in host memory");
+  std::vector<int> pk(pkd.size());
+  for (size_t i = 0; i < pkd.size(); i++) {
+    pk[i] = (int)pkd[i];
+    if (!(pkd[i] >= 1 && pkd[i] <= nk - 1) || pk[i] != pkd[i])
+      return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: prevknotind must be integers in 1..nknots-1");
+  }
+  const ss_matrix& o = r->out;
+  if (!o.data || o.rows != th || o.cols != (int64_t)tw * n || (o.dtype != SS_F32 && o.dtype != SS_F64))
+    return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: out must be FP32 or FP64 template_h x (template_w * n_frames)");
+  if (!(r->regfac >= 0.0) || !(r->pixel_aspect_ratio > 0.0))
+    return fail(SS_ERR_INVALID_ARGUMENT, "reconstruct: regfac >= 0 and pixel_aspect_ratio > 0 required");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
+  if (r->gpu_device_id < 0 || r->gpu_device_id >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
+  SS_CK(cudaSetDevice(r->gpu_device_id));
+
+  const int chunk = std::min(n, 64);
+  const size_t px = (size_t)hd * wd, fsz = fr.dtype == SS_F64 ? 8 : 4, osz = o.dtype == SS_F64 ? 8 : 4;
+  CallMem m;
+  SS_CK(cudaStreamCreateWithFlags(&m.s, cudaStreamNonBlocking));
+  cudaStream_t s = m.s;
+  double* d_bx = m.take<double>(px);
+  double* d_by = m.take<double>(px);
+  double* d_tf = m.take<double>(px);
+  int* d_pk = m.take<int>(px);
+  double* d_dxk = m.take<double>((size_t)nk * n);
+  double* d_dyk = m.take<double>((size_t)nk * n);
+  const void* d_data = fr.data;
+  if (fr.location == SS_HOST) {
+    void* q = m.take<char>(fsz * px * n);
+    if (q) SS_CK(cudaMemcpyAsync(q, fr.data, fsz * px * n, cudaMemcpyHostToDevice, s));
+    d_data = q;
+  }
+  RcBufs b{};
+  b.th = th;
+  b.tw = tw;
+  b.np = np;
+  b.hd = (int)hd;
+  b.wd = (int)wd;
+  b.nk = nk;
+  const size_t cnp = (size_t)chunk * np;
+  b.wy = m.take<double>(cnp);
+  b.ww = m.take<double>(cnp * kRcStencil);
+  b.z = m.take<float>(cnp);
+  b.cnt = m.take<float>(cnp);
+  b.last_z = m.take<int>(cnp);
+  b.last_n = m.take<int>(cnp);
+  b.mask = m.take<uint8_t>(cnp);
+  b.coef = m.take<float>(cnp * 10);
+  b.le = m.take<float>(cnp);
+  b.x = m.take<float>(cnp);
+  b.xo = m.take<float>(cnp);
+  b.part = m.take<double>((size_t)chunk * kRcParts);
+  b.part_l = m.take<float>((size_t)chunk * kRcParts);
+  int* d_state = m.take<int>(chunk);
+  int* d_due = m.take<int>(chunk);
+  int* d_keep = m.take<int>(chunk);
+  int* d_iters = m.take<int>(chunk);
+  int* d_interval = m.take<int>(chunk);
+  int* d_count = m.take<int>(chunk);
+  int* d_skip = m.take<int>(chunk);
+  float* d_eo = m.take<float>(chunk);
+  void* d_out = o.location == SS_DEVICE ? const_cast<void*>(o.data) : m.take<char>(osz * cnp);
+  uint8_t* d_mk = r->mask ? m.take<uint8_t>(cnp) : nullptr;
+  if (!d_bx || !d_by || !d_tf || !d_pk || !d_dxk || !d_dyk || !d_data || !b.wy || !b.ww || !b.z || !b.cnt ||
+      !b.last_z || !b.last_n || !b.mask || !b.coef || !b.le || !b.x || !b.xo || !b.part || !b.part_l || !d_state ||
+      !d_due || !d_keep || !d_iters || !d_interval || !d_count || !d_skip || !d_eo || !d_out || (r->mask && !d_mk))
+    return fail(SS_ERR_OUT_OF_MEMORY, "reconstruct: work memory");
+  SS_CK(cudaMemcpyAsync(d_bx, bx.data(), px * 8, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(d_by, by.data(), px * 8, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(d_tf, tf.data(), px * 8, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(d_pk, pk.data(), px * 4, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(d_dxk, dxk.data(), (size_t)nk * n * 8, cudaMemcpyHostToDevice, s));
+  SS_CK(cudaMemcpyAsync(d_dyk, dyk.data(), (size_t)nk * n * 8, cudaMemcpyHostToDevice, s));
+  const double regfac = r->regfac, vfac = 1.0 / r->pixel_aspect_ratio, vf2 = vfac * vfac;
+  const int g = 148 * 8;
+
+  // Frames [a, a + nf) of the set with check intervals iv[0..nf): their sweeps to completion, their
+  // outputs into the chunk slots 0..nf; per-frame sweep counts (0: skipped) into it_out.
+  auto run = [&](int a, int nf, const std::vector<int>& iv, std::vector<int>& it_out) -> int {
+    const size_t fnp = (size_t)nf * np;
+    SS_CK(cudaMemsetAsync(b.wy, 0, fnp * 8, s));
+    SS_CK(cudaMemsetAsync(b.ww, 0, fnp * kRcStencil * 8, s));
+    SS_CK(cudaMemsetAsync(b.z, 0, fnp * 4, s));
+    SS_CK(cudaMemsetAsync(b.cnt, 0, fnp * 4, s));
+    SS_CK(cudaMemsetAsync(d_count, 0, nf * 4, s));
+    SS_CK(cudaMemsetAsync(d_iters, 0, nf * 4, s));
+    if (fr.dtype == SS_F64)
+      k_rc_constraints<double><<<g, 256, 0, s>>>(b, d_data, a, nf, d_bx, d_by, d_tf, d_pk, d_dxk, d_dyk);
+    else
+      k_rc_constraints<float><<<g, 256, 0, s>>>(b, d_data, a, nf, d_bx, d_by, d_tf, d_pk, d_dxk, d_dyk);
+    for (int st = 0; st < 4; st++) {
+      k_rc_fill_int<<<g, 256, 0, s>>>(b.last_z, fnp, -1);
+      k_rc_fill_int<<<g, 256, 0, s>>>(b.last_n, fnp, -1);
+      for (int ph = 0; ph < 2; ph++) {
+        if (fr.dtype == SS_F64)
+          k_rc_pushgrid<double><<<g, 256, 0, s>>>(b, d_data, a, nf, st, ph, d_bx, d_by, d_tf, d_pk, d_dxk, d_dyk);
+        else
+          k_rc_pushgrid<float><<<g, 256, 0, s>>>(b, d_data, a, nf, st, ph, d_bx, d_by, d_tf, d_pk, d_dxk, d_dyk);
+      }
+    }
+    k_rc_mask<<<g, 256, 0, s>>>(b, nf);
+    k_rc_coef<<<g, 256, 0, s>>>(b, nf, regfac, vf2);
+    k_rc_count<<<g, 256, 0, s>>>(b, nf, d_count);
+    SS_CK(cudaGetLastError());
+    std::vector<int> count(nf), state(nf), due(nf);
+    SS_CK(cudaMemcpyAsync(count.data(), d_count, nf * 4, cudaMemcpyDeviceToHost, s));
+    SS_CK(cudaStreamSynchronize(s));
+    int running = 0;
+    for (int f = 0; f < nf; f++) {
+      state[f] = count[f] > 0 ? 1 : 3;
+      due[f] = state[f] == 1;
+      running += due[f];
+    }
+    SS_CK(cudaMemcpyAsync(d_state, state.data(), nf * 4, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync(d_due, due.data(), nf * 4, cudaMemcpyHostToDevice, s));
+    SS_CK(cudaMemcpyAsync(d_interval, iv.data(), nf * 4, cudaMemcpyHostToDevice, s));
+    std::vector<int> skip(nf);
+    for (int f = 0; f < nf; f++) skip[f] = state[f] == 3;
+    SS_CK(cudaMemcpyAsync(d_skip, skip.data(), nf * 4, cudaMemcpyHostToDevice, s));
+    const dim3 eg(kRcParts, nf);
+    const int cb = (nf + 127) / 128;
+    k_rc_energy<<<eg, 256, 0, s>>>(b, nf, d_due, regfac, vf2);
+    k_rc_check<<<cb, 128, 0, s>>>(nf, d_due, d_state, d_eo, d_keep, b.part, b.part_l, 1, 0, d_iters);
+    const int kMaxSweeps = 1 << 22;
+    for (int it = 1; running > 0; it++) {
+      if (it > kMaxSweeps) return fail(SS_ERR_CUDA, "reconstruct: the energy kept decreasing over 4M sweeps");
+      for (int colour = 0; colour < 4; colour++) k_rc_sweep<<<g, 256, 0, s>>>(b, nf, colour, d_state);
+      k_rc_due<<<cb, 128, 0, s>>>(nf, d_state, d_interval, it, d_due);
+      k_rc_energy<<<eg, 256, 0, s>>>(b, nf, d_due, regfac, vf2);
+      k_rc_check<<<cb, 128, 0, s>>>(nf, d_due, d_state, d_eo, d_keep, b.part, b.part_l, 0, it, d_iters);
+      k_rc_keep<<<g, 256, 0, s>>>(b, nf, d_keep);
+      if (it % 8 == 0) {
+        SS_CK(cudaMemcpyAsync(state.data(), d_state, nf * 4, cudaMemcpyDeviceToHost, s));
+        SS_CK(cudaStreamSynchronize(s));
+        running = 0;
+        for (int f = 0; f < nf; f++) running += state[f] == 1;
+      }
+    }
+    SS_CK(cudaGetLastError());
+    it_out.resize(nf);
+    SS_CK(cudaMemcpyAsync(it_out.data(), d_iters, nf * 4, cudaMemcpyDeviceToHost, s));
+    char* dst = o.location == SS_DEVICE ? static_cast<char*>(d_out) + osz * (size_t)a * np : static_cast<char*>(d_out);
+    if (o.dtype == SS_F64) k_rc_out<double><<<g, 256, 0, s>>>(b, nf, (double*)dst, d_mk, d_skip);
+    else k_rc_out<float><<<g, 256, 0, s>>>(b, nf, (float*)dst, d_mk, d_skip);
+    SS_CK(cudaStreamSynchronize(s));
+    return SS_OK;
+  };
+
+  int carried = 1;  // the interval entering the next frame; 1 at the start of a call
+  std::vector<int> last_iters;
+  for (int f0 = 0; f0 < n; f0 += chunk) {
+    const int F = std::min(chunk, n - f0);
+    std::vector<int> guess(F, 10), iters(F, 0);
+    guess[0] = carried;
+    int start = 0;
+    while (start < F) {
+      std::vector<int> iv(guess.begin() + start, guess.end()), got;
+      int rc = run(f0 + start, F - start, iv, got);
+      if (rc) return rc;
+      // the chain of intervals from `start`: frames up to the first mismatch ran with their own
+      int cur = guess[start], bad = -1;
+      for (int i = start; i < F; i++) {
+        if (guess[i] != cur) {
+          bad = i;
+          break;
+        }
+        iters[i] = got[i - start];
+        if (iters[i] > 0) cur = rc_interval(iters[i]);  // skipped frames keep the interval
+      }
+      const int good_end = bad < 0 ? F : bad;
+      // outputs of the settled frames [start, good_end) to the host
+      if (o.location == SS_HOST && good_end > start)
+        SS_CK(cudaMemcpy(static_cast<char*>(const_cast<void*>(o.data)) + osz * (size_t)(f0 + start) * np,
+                         d_out, osz * (size_t)(good_end - start) * np, cudaMemcpyDeviceToHost));
+      if (r->mask && good_end > start)
+        SS_CK(cudaMemcpy(r->mask + (size_t)(f0 + start) * np, d_mk, (size_t)(good_end - start) * np,
+                         cudaMemcpyDeviceToHost));
+      if (bad < 0) {
+        carried = cur;
+        break;
+      }
+      // re-run from the first frame that ran with another interval, with the intervals this run's
+      // sweep counts give (its own is now exact)
+      guess[bad] = cur;
+      int g2 = cur;
+      for (int i = bad + 1; i < F; i++) {
+        const int prev = got[i - 1 - start];
+        if (prev > 0) g2 = rc_interval(prev);
+        guess[i] = g2;
+      }
+      start = bad;
+    }
+    if (r->iterations)
+      for (int i = 0; i < F; i++) r->iterations[f0 + i] = iters[i];
+  }
   return SS_OK;
 }
 
@@ -2392,6 +2640,12 @@ int ss_estimate_displacements(const ss_recording* rec, ss_recording_outputs* out
 int ss_recording_sets(int32_t n_frames, int32_t frames_per_set, int32_t min_frames_per_set, int32_t* first,
                       int32_t* count, int32_t max_sets, int32_t* n_sets) {
   int rc = ss::recording_sets(n_frames, frames_per_set, min_frames_per_set, first, count, max_sets, n_sets);
+  if (!rc) ss::g_err.clear();
+  return rc;
+}
+
+int ss_reconstruct_frames(const ss_reconstruct* r) {
+  int rc = ss::reconstruct_frames(r);
   if (!rc) ss::g_err.clear();
   return rc;
 }

@@ -66,6 +66,9 @@ int estimate_displacements(const ss_recording* rec, ss_recording_outputs* out);
 // ss_prepare_frames: prefilter, crop and block-reorder raw frames on the device (ss_frontend.cuh).
 int prepare_frames(const ss_prep_frames* p);
 
+// ss_reconstruct_frames: invert_bilinear_sampling of one set's frames (ss_reconstruct.cuh).
+int reconstruct_frames(const ss_reconstruct* r);
+
 int recording_sets(int n_frames, int frames_per_set, int min_frames_per_set, int* first, int* count, int max_sets,
                    int* n_sets);
 

@@ -36,7 +36,7 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.ss_abi_version() == 4  # ss_prepare_frames (frame preparation on the device)
+    assert lib.ss_abi_version() == 5  # ss_reconstruct_frames (reconstruction on the device)
 
 
 def test_struct_sizes_match_header(lib):
@@ -50,6 +50,13 @@ def test_struct_sizes_match_header(lib):
     assert _lib.SSPrepFrames.gather.offset == 72
     assert _lib.SSPrepFrames.out.offset == 88
     assert C.sizeof(_lib.SSPrepFrames) == 128
+    # ss_reconstruct: frames, n_frames (+pad), six matrices from 40, template_h/w at 232, regfac 240,
+    # aspect 248, out 256, mask 288, iterations 296, gpu_device_id 304, padded to 312
+    assert _lib.SSReconstruct.basex.offset == 40
+    assert _lib.SSReconstruct.template_h.offset == 232
+    assert _lib.SSReconstruct.out.offset == 256
+    assert _lib.SSReconstruct.gpu_device_id.offset == 304
+    assert C.sizeof(_lib.SSReconstruct) == 312
 
 
 def _expect_invalid(args, match):
