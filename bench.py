@@ -46,6 +46,13 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the unbatched per-group comparison")
     ap.add_argument("--no-sweep", action="store_true", help="skip the storage-precision sweep")
+    ap.add_argument("--cpu-single-frames", type=int, default=4,
+                    help="frames of the single-thread CPU baseline (0: skip it)")
+    ap.add_argument("--sweep-frames", type=int, default=4000,
+                    help="frames of the storage sweep on the device (0: skip it)")
+    ap.add_argument("--no-pipeline", action="store_true",
+                    help="skip the frame preparation and reconstruction legs")
+    ap.add_argument("--recon-frames", type=int, default=64, help="frames of the reconstruction leg")
     ap.add_argument("--plain-groups", type=int, default=2)
     ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="seconds of generated serving load (8 sessions, 0 to skip)")
@@ -423,6 +430,60 @@ def traffic_summary():
 
 # ------------------------------------------------------------------------------------------------
 
+def pipeline(groups, dev_frames, results, settings, lay, device, recon_frames: int) -> dict:
+    """The rows either side of the alignment on the same workload: the reference driver's frame
+    preparation (ss_prepare_frames: block reorder of raw frames, and with the prefilter
+    pregauss = 1, mednorm) over all frames, and the reconstruction (ss_reconstruct_frames) of one
+    set of ``recon_frames`` frames of the first group with the knots this run estimated."""
+    import torch
+
+    from steadyscan_b200 import api, prep
+    gidx = torch.from_numpy(np.asfortranarray(prep._block_gather_index(lay.prevknotind, lay.frame_w))
+                            .reshape(-1, order="F")).to(device)
+    valid = gidx >= 0
+    h, w = lay.prevknotind.shape
+    per = lay.frame_h * lay.frame_w
+    # raw frames (h x w column-major each) from the block frames: the inverse of the block map
+    flat = torch.cat(dev_frames)
+    n = flat.numel() // per
+    bm = flat.view(torch.int16).view(n, per)  # same bits; index_put has no uint16 kernel
+    raw16 = torch.zeros((n, h * w), dtype=torch.int16, device=device)
+    raw16[:, gidx[valid]] = bm[:, valid]
+    raw3 = raw16.view(torch.uint16).view(n, w, h).permute(2, 1, 0)  # h x w x n, column-major per frame
+    out = {}
+    for name, kw in (("block_reorder_u16", dict(out_dtype=np.uint16)),
+                     ("prefilter_f64", dict(pregauss=1.0, mednorm=True, out_dtype=np.float64))):
+        for _ in range(3):  # warm-up: work memory and the output's first allocation
+            api.prepare_frames(raw3, lay, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        got = api.prepare_frames(raw3, lay, **kw)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"frames": n, "frames_per_s": n / dt, "ms": dt * 1e3}
+        if name == "block_reorder_u16":
+            out[name]["equals_block_frames"] = bool(torch.equal(got.T.reshape(-1).view(torch.int16),
+                                                                flat.view(torch.int16)))
+    g0, r0 = groups[0], results[0]
+    k = min(recon_frames, int(g0["nFrames"]))
+    nk = lay.frame_w + 1
+    dxk = np.asarray(r0["dx"]).reshape(nk, -1, order="F")[:, :k]
+    dyk = np.asarray(r0["dy"]).reshape(nk, -1, order="F")[:, :k]
+    fr = (raw16[:k].to(torch.int32) & 0xFFFF).to(torch.float32).view(k, w, h).permute(2, 1, 0)
+    th, tw = np.asarray(g0["template_image"]).shape
+    api.reconstruct_frames(fr[:, :, :2], dxk[:, :2], dyk[:, :2], settings, (th, tw))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = api.reconstruct_frames(fr, dxk, dyk, settings, (th, tw))
+    dt = time.perf_counter() - t0
+    out["reconstruct"] = {"frames": k, "frames_per_s": k / dt, "ms": dt * 1e3,
+                          "sweeps_mean": float(np.mean(rc["iterations"])),
+                          "masked_fraction": float(rc["mask"].mean()),
+                          "note": "one set (one invert_bilinear_sampling call) of the first group's frames, "
+                                  "template 512x512, ibs_regfac 3e-3, host output"}
+    return out
+
+
 def max_over_ranks(value: float, dist=None, device=None) -> float:
     """The slowest rank's time (every rank calls this at the same point)."""
     if dist is None:
@@ -459,7 +520,8 @@ def plain_path(groups, precision, n_groups):
         d = dict(g)
         d["flags"] = precision
         gs.append(d)
-    api.align_group(gs[0], want_mask=False)  # warm-up
+    for d in gs[:3]:  # warm-up
+        api.align_group(d, want_mask=False)
     t0 = time.perf_counter()
     frames = 0
     for d in gs:
@@ -505,6 +567,62 @@ def precision_sweep(a, o, template_shape):
                 "rms_px": float(np.sqrt(np.mean(d * d))), "max_px": float(np.max(np.abs(d))),
                 "corrected_rel_l2": correct.relative_l2(c, w, ref_c, ref_w)})
     return {"sample": f"{n} frames of one 512x512 group vs the FP64 oracle", "variants": out}
+
+
+def storage_sweep(args, device) -> dict:
+    """The storage choices on the full 4000-frame workload of 512x512 frames with knots every 2 lines
+    (the headline generator, seed 1004): frames uint16 / FP16 x template and gradients FP32 / FP16 in
+    precision S, each one batch timed on device-resident frames, and each against the precision-D
+    (FP64) run of the same batch: RMS and max knot difference (px) and the fraction of knots within
+    0.05 px. A control runs precision D on the template rounded to FP16."""
+    import torch
+
+    from steadyscan_b200 import api, prep
+    from steadyscan_b200._lib import SS_F16, SS_U16
+    n = args.sweep_frames
+    groups, dev, _, lay = make_workload(n, 512, 64, "S", 1004, device)
+    f16 = [(t.view(torch.int16).to(torch.int32) & 0xFFFF).to(torch.float16) for t in dev]
+    torch.cuda.synchronize()
+
+    def run(frames, dtype, flags, tstore=None, template=None):
+        grads = prep.template_gradients(template) if template is not None else None
+        gs = []
+        for g, t in zip(groups, frames):
+            d = dict(g)
+            d["bmData"] = api.DeviceMatrix(t.data_ptr(), lay.frame_h, lay.frame_w * int(g["nFrames"]), dtype, owner=t)
+            d["flags"] = flags
+            if template is not None:
+                d["template_image"] = template
+                d["xgrad"], d["ygrad"] = grads
+            gs.append(d)
+        b = api.Batch(gs, template_storage=tstore)
+        b.run()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        r = b.collect()
+        b.close()
+        return (np.concatenate([x["dx"] for x in r]), np.concatenate([x["dy"] for x in r])), n / dt
+
+    def err(k, ref):
+        d = np.concatenate([k[0] - ref[0], k[1] - ref[1]])
+        return {"rms_px": float(np.sqrt(np.mean(d * d))), "max_px": float(np.max(np.abs(d))),
+                "within_0p05_px": float(np.mean(np.abs(d) <= 0.05))}
+
+    ref, v_d = run(dev, SS_U16, "D")
+    out = {"workload": f"{n} frames of 512x512, knots every 2 lines, groups of 64, lambda 5e-3; "
+                       "accuracy against the precision-D (FP64) run of the same frames",
+           "D_frames_per_s": v_d, "variants": []}
+    for fname, frames, dt in (("uint16", dev, SS_U16), ("float16", f16, SS_F16)):
+        for tname in ("f32", "f16"):
+            k, v = run(frames, dt, "S", tname)
+            out["variants"].append(dict(frames=fname, template=tname, frames_per_s=v, **err(k, ref)))
+    t16 = np.asarray(groups[0]["template_image"]).astype(np.float16).astype(np.float64)
+    k, v = run(dev, SS_U16, "D", template=t16)
+    out["control_fp64_on_f16_rounded_template"] = dict(frames_per_s=v, **err(k, ref))
+    return out
 
 
 def serve(args, device, seconds, plain_d):
@@ -692,10 +810,8 @@ def main():
         hgroups = []
         h2d = 0
         shared_seen = set()
-        # ss_align_groups splits host-resident groups into up to 4 parts on their own streams (the
-        # uploads of later parts overlap the runs of earlier ones); each part uploads the buffers its
-        # groups share once
-        n_parts = min(len(groups), 4)
+        # ss_align_groups runs host-resident groups as one batch, which uploads each buffer the groups
+        # share once
         for gi, g in enumerate(groups):
             d = dict(g)
             src = np.asarray(g["bmData"])
@@ -706,10 +822,9 @@ def main():
             d["bmData"] = pv
             hgroups.append(d)
             h2d += src.nbytes + 16 * (lay.frame_w + 1) * int(g["nFrames"])  # frames + initial knots
-            part = gi * n_parts // len(groups)
             for k in ("template_image", "xgrad", "ygrad", "tfrac", "basex", "basey", "base_mask"):
-                if (part, id(g[k])) not in shared_seen:  # one upload per distinct buffer and part
-                    shared_seen.add((part, id(g[k])))
+                if id(g[k]) not in shared_seen:  # one upload per distinct buffer
+                    shared_seen.add(id(g[k]))
                     h2d += np.asarray(g[k]).nbytes
         api.align_groups(hgroups, want_mask=False)  # warm-up
         barrier()
@@ -723,23 +838,6 @@ def main():
         e2e = {"value": args.frames * world / dt, "unit": "frames/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "api": "ss_align_groups"}
 
-    cpu = None
-    acc = None
-    if rank == 0 and not args.no_cpu:
-        v, dt, o, a = cpu_sample(groups, args.cpu_sample_frames, threads)
-        cpu = {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_sample_frames} frames of one {args.size}x{args.size} group, FP64 oracle, "
-                         f"{dt:.1f} s"}
-        # accuracy of the timed precision against the FP64 oracle on that sample
-        a2 = dict(a)
-        a2["flags"] = args.precision
-        g = api.align_group(a2, want_mask=False)
-        rms = float(np.sqrt(np.mean(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]) ** 2)))
-        mx = float(np.max(np.abs(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]))))
-        acc = {"rms_px_vs_fp64": rms, "max_px_vs_fp64": mx, "sample": f"{args.cpu_sample_frames} frames"}
-        if not args.no_sweep:
-            acc["precision_sweep"] = precision_sweep(a, o, np.asarray(a["template_image"]).shape)
-
     plain = None
     if rank == 0 and not args.no_plain:
         plain = {}
@@ -752,6 +850,28 @@ def main():
         if e2e:
             plain["e2e_vs_plain_D"] = e2e["value"] / plain["D"]["value"]
 
+    cpu = None
+    acc = None
+    if rank == 0 and not args.no_cpu:
+        v, dt, o, a = cpu_sample(groups, args.cpu_sample_frames, threads)
+        cpu = {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_sample_frames} frames of one {args.size}x{args.size} group, FP64 oracle, "
+                         f"{dt:.1f} s"}
+        if args.cpu_single_frames > 0:
+            v1, dt1, _, _ = cpu_sample(groups, args.cpu_single_frames, 1)
+            cpu["single_thread"] = {"value": v1, "unit": "frames/s", "cores": 1,
+                                    "sample": f"the first {args.cpu_single_frames} frames of the same group, "
+                                              f"{dt1:.1f} s"}
+        # accuracy of the timed precision against the FP64 oracle on that sample
+        a2 = dict(a)
+        a2["flags"] = args.precision
+        g = api.align_group(a2, want_mask=False)
+        rms = float(np.sqrt(np.mean(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]) ** 2)))
+        mx = float(np.max(np.abs(np.concatenate([g["dx"] - o["dx"], g["dy"] - o["dy"]]))))
+        acc = {"rms_px_vs_fp64": rms, "max_px_vs_fp64": mx, "sample": f"{args.cpu_sample_frames} frames"}
+        if not args.no_sweep:
+            acc["precision_sweep"] = precision_sweep(a, o, np.asarray(a["template_image"]).shape)
+
     small_line = None
     if rank == 0 and not args.no_cpu:
         small_line = plain_small(device, threads)
@@ -759,6 +879,14 @@ def main():
     ragged_line = None
     if rank == 0 and not args.no_ragged:
         ragged_line = ragged(args, device)
+
+    sweep_line = None
+    if rank == 0 and args.sweep_frames > 0:
+        sweep_line = storage_sweep(args, device)
+
+    pipeline_line = None
+    if rank == 0 and not args.no_pipeline:
+        pipeline_line = pipeline(groups, dev_frames, results, settings, lay, device, args.recon_frames)
 
     serving_line = None
     if rank == 0 and args.serve_seconds > 0:
@@ -773,6 +901,7 @@ def main():
                 "config": workload_config(args), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clk.summary(), "gpu_launches": launches, "accuracy": acc, "plain_gpu": plain,
                 "plain_method_small": small_line, "ragged": ragged_line, "serving": serving_line,
+                "pipeline": pipeline_line, "storage_sweep": sweep_line,
                 "run": {"cycles": st["cycles"], "linesearch_rounds": st["linesearch_rounds"],
                         "iterations_min": int(min(iters)), "iterations_max": int(max(iters)),
                         "arena_bytes": st["arena_bytes"]}}

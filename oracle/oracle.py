@@ -44,6 +44,7 @@ class _Out(C.Structure):
         ("iter_corr", C.c_void_p), ("frame_corr_hist", C.c_void_p), ("iter_errvals", C.c_void_p),
         ("all_params", C.c_void_p), ("n_eval", C.c_void_p),
         ("iterations", C.c_int), ("stop_reason", C.c_int), ("ls_trial_cap_hit", C.c_int),
+        ("rg_params", C.c_void_p),
     ]
 
 
@@ -119,13 +120,14 @@ def align_group(args: dict, n_threads: int = 1, want_mask: bool = True, want_his
         o["frame_corr_hist"] = np.zeros((mi, nF))
         o["iter_errvals"] = np.zeros((2 * mi, nF))
         o["all_params"] = np.zeros((mi, 2 * N))
+        o["rg_params"] = np.zeros((2 * mi, 2 * N))  # flag t: the chain after every half-step
     out = _Out(_ptr(o["p_last"]), _ptr(o["dx"]), _ptr(o["dy"]), _ptr(o["frame_corr"]), _ptr(o["residrms"]),
                _ptr(o["mask_rm"]) if want_mask else None,
                _ptr(o["iter_corr"]) if want_history else None,
                _ptr(o["frame_corr_hist"]) if want_history else None,
                _ptr(o["iter_errvals"]) if want_history else None,
                _ptr(o["all_params"]) if want_history else None,
-               _ptr(o["n_eval"]), 0, 0, 0)
+               _ptr(o["n_eval"]), 0, 0, 0, _ptr(o["rg_params"]) if want_history else None)
     rc = L.sso_align_group(C.byref(i), C.byref(out))
     del keep
     if rc != 0:

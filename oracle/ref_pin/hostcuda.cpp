@@ -91,7 +91,10 @@ void ss_launch(ss_dim3 g, ss_dim3 b, const std::function<void()>& body) {
 extern "C" {
 
 cudaError_t cudaMalloc(void** p, size_t n) {
-  *p = std::calloc(n ? n : 1, 1);
+  // 256 zero bytes past the end: reads past an array (groupActive for an odd frame count,
+  // task_calcerrval.cu:166, task_linesearch.cu:88) see zeros, as they would in fresh device memory
+  // with its 256-byte allocation granularity, whatever the host heap holds next
+  *p = std::calloc(n + 256, 1);
   return *p ? cudaSuccess : cudaErrorMemoryAllocation;
 }
 cudaError_t cudaFree(void* p) {
@@ -160,10 +163,24 @@ cusparseStatus_t cusparseDestroyMatDescr(cusparseMatDescr_t d) {
 }
 cusparseStatus_t cusparseSetMatType(cusparseMatDescr_t, cusparseMatrixType_t) { return CUSPARSE_STATUS_SUCCESS; }
 cusparseStatus_t cusparseSetMatIndexBase(cusparseMatDescr_t, cusparseIndexBase_t) { return CUSPARSE_STATUS_SUCCESS; }
+// Solves without a defined result: a matrix that was not positive definite (cuSOLVER reports it
+// through `singularity` and leaves x unspecified; the reference ignores the report,
+// cusolversolver.cu:55-57), or a conversion given entries outside the system (nParamsUsed = 0, which
+// TimedMainIteration's cleared paramsUsed allows when every group is inactive). A run that meets
+// one follows no defined trajectory and is not a pin.
+int ss_hostcuda_singular_solves = 0;
+
 cusparseStatus_t cusparseXcoo2csr(cusparseHandle_t, const int* coo_row, int nnz, int m, int* csr_row,
                                   cusparseIndexBase_t base) {
   for (int i = 0; i <= m; i++) csr_row[i] = 0;
-  for (int z = 0; z < nnz; z++) csr_row[coo_row[z] - base + 1]++;
+  for (int z = 0; z < nnz; z++) {
+    const int r = coo_row[z] - base;
+    if (r < 0 || r >= m) {  // an entry outside the system (m = 0: no knot used): no defined result
+      ss_hostcuda_singular_solves++;
+      continue;
+    }
+    csr_row[r + 1]++;
+  }
   for (int i = 0; i < m; i++) csr_row[i + 1] += csr_row[i];
   for (int i = 0; i <= m; i++) csr_row[i] += base;
   return CUSPARSE_STATUS_SUCCESS;
@@ -182,10 +199,6 @@ cusolverStatus_t cusolverSpDestroy(cusolverSpHandle_t h) {
 
 }  // extern "C"
 
-// Solves whose matrix was not positive definite. cuSOLVER reports such a matrix through
-// `singularity` and leaves x unspecified; the reference ignores the report (cusolversolver.cu:55-57),
-// so a run that meets one follows no defined trajectory and is not a pin.
-int ss_hostcuda_singular_solves = 0;
 
 template <class T>
 static cusolverStatus_t dense_chol_solve(int m, int nnz, const T* val, const int* row, const int* col, const T* b,

@@ -155,7 +155,7 @@ class RunOut(C.Structure):
     _fields_ = [("dx", C.c_void_p), ("dy", C.c_void_p), ("frame_corr", C.c_void_p), ("residrms", C.c_void_p),
                 ("mask", C.c_void_p), ("all_params", C.c_void_p), ("iter_errvals", C.c_void_p),
                 ("iter_corr", C.c_void_p), ("frame_corr_hist", C.c_void_p), ("iterations", C.c_int),
-                ("stop_reason", C.c_int), ("singular_solves", C.c_int)]
+                ("stop_reason", C.c_int), ("singular_solves", C.c_int), ("rg_params", C.c_void_p)]
 
 
 def run_available() -> bool:
@@ -177,7 +177,8 @@ def run_align(args: dict) -> dict:
     """The reference's align_group_to_template task (Task::alignFrames with MainIteration, its
     kernels and filters, solver id 1) on the 26 boundary arguments; returns its outputs: knots,
     frame correlations, residrms, mask, the knot chain after every iteration (all_params) and, with
-    flags e / C, the errvals of every half-step and the global correlation of every iteration."""
+    flags e / C, the errvals of every half-step and the global correlation of every iteration, and with
+    flag t the chain after every half-step (rg_params, 2 max_iter x 2N; NaN without flag t)."""
     rm = lambda a, dt=np.float64: np.ascontiguousarray(np.asarray(a, dtype=dt))
     t, xg, yg = rm(args["template_image"]), rm(args["xgrad"]), rm(args["ygrad"])
     frac, bx, by = rm(args["tfrac"]), rm(args["basex"]), rm(args["basey"])
@@ -199,9 +200,10 @@ def run_align(args: dict) -> dict:
               float(args["linesearch_reduction_multiplier"]), int(args["solver_id"]), int(args["filter_id"]))
     o = dict(dx=np.zeros((w + 1) * nF), dy=np.zeros((w + 1) * nF), frame_corr=np.zeros(nF), residrms=np.zeros(nF),
              mask=np.zeros((hb, w * nF), np.uint8), all_params=np.zeros((mi, 2 * N)),
-             iter_errvals=np.zeros((nF, 2 * mi)), iter_corr=np.zeros(mi), frame_corr_hist=np.zeros((mi, nF)))
+             iter_errvals=np.zeros((nF, 2 * mi)), iter_corr=np.zeros(mi), frame_corr_hist=np.zeros((mi, nF)),
+             rg_params=np.full((2 * mi, 2 * N), np.nan))
     out = RunOut(*[_p(o[k]) for k in ("dx", "dy", "frame_corr", "residrms", "mask", "all_params", "iter_errvals",
-                                      "iter_corr", "frame_corr_hist")], 0, 0, 0)
+                                      "iter_corr", "frame_corr_hist")], 0, 0, 0, _p(o["rg_params"]))
     rc = run_lib().ssrun_align(C.byref(i), C.byref(out))
     del keep
     if rc != 0:

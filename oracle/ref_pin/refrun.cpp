@@ -103,6 +103,7 @@ struct ssrun_out {
   double* frame_corr_hist;  // flag c: n_frames x max_iter column-major
   int iterations, stop_reason;
   int singular_solves;  // solves of a matrix that was not positive definite (x unspecified)
+  double* rg_params;    // flag t: the 2N chain after every half-step, 2 max_iter slots (output 14)
 };
 
 extern int ss_hostcuda_singular_solves;
@@ -190,6 +191,8 @@ int ssrun_align(const ssrun_in* in, ssrun_out* out) {
       for (int k = 0; k < 2 * mi; k++) out->iter_errvals[(size_t)f * 2 * mi + k] = o.iterationErrvals(k, f);
   if (out->frame_corr_hist && config.saveFrameCorrelationsEnabled())
     for (int i = 0; i < nF * mi; i++) out->frame_corr_hist[i] = o.frameCorrelations.data()[i];
+  if (out->rg_params && config.subFunctionTimingEnabled())
+    for (size_t i = 0; i < (size_t)2 * N * 2 * mi; i++) out->rg_params[i] = o.rgParams.data()[i];
   if (out->iter_corr && config.saveIterationCorrelationsEnabled())
     for (int it = 0; it < mi; it++) out->iter_corr[it] = o.iterationCorrelations.data()[it];
   delete task;

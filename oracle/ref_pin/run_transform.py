@@ -16,7 +16,10 @@ Rewrites (mechanical; the code itself is the reference's):
   are followed by a reset of the flag without a barrier (``if( sharedResult ) break;`` and
   ``if( !sharedResult ) return;``) read it through ``ss_lockstep_read``: every thread of the block
   reads before any thread goes on, as the threads of one warp do in lock step (the test cases keep
-  a frame's blocks within one warp, frameW <= 32);
+  a frame's blocks within one warp, frameW <= 32), and after a trial with no block present every
+  thread clears the flag before any thread's movement check sets it again (a lock-step point after
+  the clear: without it a later thread's clear erased an earlier thread's report of movement, and
+  the search of a frame whose moving knots run first stopped early);
 * the includes of ``mex.h``, the Eigen headers and the timing/printing helpers are left out by the
   reference's own switches (``_DEBUG``, EIGENINCLUDE unset in the force-included configuration).
 """
@@ -89,7 +92,10 @@ def edit(rel, text):
                  # every thread's trial knot is written before any thread warps its column, which
                  # reads the next thread's knot (lock step within the warp)
                  ("\t\t\td_addDeltaP<T>( mem, idx );\n", "\t\t\td_addDeltaP<T>( mem, idx );\n\t\t\tss_lockstep_point();\n"),
-                 ("if( sharedResult ) break;", "if( ss_lockstep_read( sharedResult ) ) break;"),
+                 # every thread clears the flag before any thread's movement check sets it again
+                 ("\t\t\tif( sharedResult ) break;\n\t\t\tsharedResult = false;\n",
+                  "\t\t\tif( ss_lockstep_read( sharedResult ) ) break;\n\t\t\tsharedResult = false;\n"
+                  "\t\t\tss_lockstep_point();\n"),
                  ("if( !sharedResult ) return;", "if( !ss_lockstep_read( sharedResult ) ) return;"),
                  # thread idx == 0 updates the errval that the block's threads compare with
                  ("if( errvalNew < mem->errval[shift * mem->nFrames + blockIdx.x] ) {",

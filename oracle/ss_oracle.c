@@ -44,6 +44,8 @@ typedef struct {
     const sso_in* in;
     int Hb, W, nF, fW, N, P, Ht, Wt, group_size, n_groups;
     int flag_M, flag_C, flag_c, flag_e, flag_R;
+    int flag_t;                 /* sub-function timing: TimedMainIteration (timedmainiteration.cpp) */
+    double* rg_params;          /* flag t: the chain after every half-step (task.cpp:409) */
     /* device state of the reference (memory.h:85-163) */
     double *p, *p_last, *pnew, *delta_p, *new_delta_p, *x, *y, *diff, *wx, *wy, *jtr, *errval;
     double *p_ls;               /* Q3 snapshot */
@@ -825,10 +827,20 @@ static void mask_inactive(St* s) {
 
 static void disable_filter(St* s) { s->filter_active = 0; }
 
-/* MainIteration::execute (mainiteration.cpp:62-119). */
+/* MainIteration::execute (mainiteration.cpp:62-119), or with flag t TimedMainIteration::execute
+ * (timedmainiteration.cpp:45-143), which differs in four ways: it clears paramsUsed before every
+ * half-step (:50), so the knots of frames whose group is inactive are unused instead of keeping
+ * their last use; at the filter's iteration limit it disables the filter without zeroing filterID
+ * (:97-105), and on the retry without filter it zeroes filterID (:136), the reverse of
+ * MainIteration (mainiteration.cpp:83-89, 96-106), which changes when alignFrames's
+ * filter-deactivation branch (task.cpp:313-325) fires; it copies the chain after every half-step
+ * into slot shift + 2 (iteration - 1) of rgParams (:124); and its retry runs as iteration + 1
+ * (:141), which moves those slots. The timers and its clearing of the mask (every mask entry is
+ * rewritten by applyParameters) leave the results alone. */
 static int main_iteration(St* s, int iteration) {
     int improved = 1;
     for (int shift = 0; shift < 2; shift++) {
+        if (s->flag_t) memset(s->params_used, 0, s->N);
         apply_all(s);
         calc_group_errvals(s, shift);
         update_gradients(s);
@@ -837,7 +849,7 @@ static int main_iteration(St* s, int iteration) {
         fill_jtr(s);
         if (s->n_filter_iter != 0 && iteration > s->n_filter_iter) {
             disable_filter(s);
-            s->filter_id = 0;
+            if (!s->flag_t) s->filter_id = 0;
             s->n_filter_iter = 0;
         }
         solve(s);
@@ -857,12 +869,18 @@ static int main_iteration(St* s, int iteration) {
         }
         expand_results(s, shift);
         improved &= linesearch(s, shift);
+        /* slots past 2 max_iter (a retry in the last iteration) are not written: the reference's
+         * host buffer has 2 max_iter slots (task_allocate.cu:122) */
+        const int slot = shift + 2 * (iteration - 1);
+        if (s->flag_t && s->rg_params && slot < 2 * s->in->max_iter)
+            memcpy(s->rg_params + (size_t)slot * s->P, s->p, sizeof(double) * s->P);
     }
     if (!improved) {
         if (s->n_filter_iter != 0) {
             disable_filter(s);
+            if (s->flag_t) s->filter_id = 0;
             s->n_filter_iter = 0;
-            return main_iteration(s, iteration);
+            return main_iteration(s, s->flag_t ? iteration + 1 : iteration);
         }
         return 0;
     }
@@ -886,6 +904,7 @@ static int state_init(St* s, const sso_in* in, long long* n_eval) {
     s->flag_c = has_flag(in->flags, 'c');
     s->flag_e = has_flag(in->flags, 'e');
     s->flag_R = has_flag(in->flags, 'R');
+    s->flag_t = has_flag(in->flags, 't');
     /* Task::initialize filter factory (task.cpp:54-70) */
     s->filter_id = in->filter_id;
     s->n_filter_iter = in->max_filter_iter;
@@ -946,6 +965,7 @@ int sso_align_group(const sso_in* in, sso_out* out) {
     if (!out) return -1;
     int rc = state_init(s, in, out->n_eval);
     if (rc) return rc;
+    s->rg_params = out->rg_params;
 
     /* Task::alignFrames (task.cpp:259-412) */
     double correlation = 0, corr = 0;

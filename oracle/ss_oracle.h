@@ -60,6 +60,7 @@ typedef struct {
     int iterations;
     int stop_reason;         /* StopCriterion (stopcriterion.h:4-10) */
     int ls_trial_cap_hit;    /* a line search ran into the trial cap */
+    double* rg_params;       /* flag t: 2N chain after every half-step, 2*max_iter slots row-major, may be NULL */
 } sso_out;
 
 /* Runs one align_group_to_template call. Returns 0 on success, <0 on invalid arguments. */

@@ -6,7 +6,8 @@ ParameterOrganizer and SolverCuSolver), host-compiled from the reference tree by
 Run in a container that has the reference sources:  python tests/golden/make_refrun_golden.py
 Each fixture holds the 26 inputs and the run's outputs: iterations, stop reason, per-frame knots,
 frame correlations, residrms, the mask, the knot chain after every iteration and (flags C and e)
-every iteration's global correlation and every half-step's errvals. The cases keep frames of at
+every iteration's global correlation and every half-step's errvals, and (flag t) the chain after
+every half-step. The cases keep frames of at
 most 32 blocks, so that a frame's line-search block is one warp, whose lock-step execution the
 host emulation reproduces; the solver is id 1 (exact Cholesky: Eigen, the default id 2, is not
 part of the reference tree). Flag R is left out: its median kernel (d_medianfilter.cu:3-20) reads
@@ -45,6 +46,17 @@ CASES = {
     "swap_back_row1": (dict(n_frames=40, seed=33, settings={"gpu_solver_id": 1}), "DCce"),
     "frames_32_blocks": (dict(nlines=64, linewidth=24, nknots=33, n_frames=4, seed=12,
                               settings={"gpu_solver_id": 1}), "DCce"),
+    # huge first steps: a trial with no block present whose moving knots belong to the frame's first
+    # threads (the block-wide movement flag after such a trial)
+    "absent_trial_movement": (dict(seed=45, n_frames=4, clip_px=6.0, jumps=2, jump_px=4.0,
+                                   settings={"gpu_solver_id": 1, "gpu_filter_max_iterations": 2}), "DCce"),
+    # flag t (TimedMainIteration): the retry without filter as iteration + 1, paramsUsed cleared
+    # before every half-step (with the odd frame count's inactive last group), the filterID rules
+    # that move the filter-deactivation branch, and rgParams
+    "timed_retry_odd": (dict(n_frames=3, seed=6, settings={"gpu_solver_id": 1}), "DCcet"),
+    "timed_filter_limit": (dict(seed=41, n_frames=4, clip_px=6.0, jumps=2, jump_px=4.0,
+                                settings={"gpu_solver_id": 1, "gpu_filter_max_iterations": 2}), "DCcet"),
+    "timed_mask_inactive": (dict(n_frames=6, seed=10, settings={"gpu_solver_id": 1, "haltcorr": 0.15}), "DCceMt"),
 }
 
 
@@ -69,6 +81,8 @@ def main():
         store["iter_corr"] = r["iter_corr"][:it]
         store["iter_errvals"] = r["iter_errvals"][:2 * it]
         store["frame_corr_hist"] = r["frame_corr_hist"][:it]
+        if "t" in flags:  # the slots a run writes: two per iteration, two more for a last retry
+            store["rg_params"] = r["rg_params"][:2 * it + 2]
         np.savez_compressed(os.path.join(out_dir, f"refrun_{name}.npz"), **store)
         print("wrote", name, "iterations", it, "stop", r["stop_reason"])
 

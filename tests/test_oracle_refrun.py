@@ -28,7 +28,8 @@ def _build():
 
 
 def test_fixtures_present():
-    assert len(GOLDEN) >= 11
+    assert len(GOLDEN) >= 16
+    assert sum("t" in str(np.load(p)["in_flags"]) for p in GOLDEN) >= 3  # TimedMainIteration runs
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[7:-4] for p in GOLDEN])
@@ -53,3 +54,7 @@ def test_trajectory_matches_reference_run(path):
     np.testing.assert_allclose(o["frame_corr_hist"][:it], z["frame_corr_hist"], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(o["frame_corr"], z["frame_corr"], rtol=1e-10, atol=1e-12, equal_nan=True)
     np.testing.assert_allclose(o["residrms"], z["residrms"], rtol=1e-10, atol=1e-12, equal_nan=True)
+    if "rg_params" in z.files:  # flag t: the chain after every half-step; later slots stay zero
+        k = z["rg_params"].shape[0]
+        np.testing.assert_allclose(o["rg_params"][:k], z["rg_params"], rtol=0, atol=1e-9)
+        assert not np.any(o["rg_params"][k:])
