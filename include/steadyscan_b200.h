@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define SS_ABI_VERSION 5
+#define SS_ABI_VERSION 6
 
 #if defined(__GNUC__)
 #define SS_API __attribute__((visibility("default")))
@@ -122,6 +122,20 @@ typedef struct ss_outputs {
   double elapsed_ms;          /* wall time of the call */
   uint8_t* blocks_used;       /* W x n_frames column-major: the block has a valid pixel in the final
                                  mask (output 5), the caller's blocksused (steady_scan.m:264-265) */
+  /* Timing and half-step outputs (mexgateway.cpp:266-300; filled with zeros where the flags do not
+   * produce them). Flag t also switches the iteration to the reference's TimedMainIteration
+   * (task.cpp:99-103), whose bookkeeping differs (timedmainiteration.cpp:45-143): paramsUsed is
+   * cleared before every half-step, filterID follows other rules, a retry counts as the next
+   * iteration for output 14. */
+  double* iteration_times;    /* 9: max_iter seconds per iteration (flags T and t; device clock) */
+  double* function_times;     /* 10: 14 seconds per sub-function (flag t; CUDA events over the batch,
+                                 whose stages the run's groups share; flag t runs host-launched
+                                 cycles): 1 applyParameters with the errval, gradient and system sums
+                                 of the same pass, 2 group errvals and parameter mask, 4 compaction,
+                                 5 system blocks, 7 solve and filter, 8 expansion, 9 line search,
+                                 10 correlation, 11 iteration end; 0, 3, 6, 12 and 13 stay zero */
+  double* rg_params;          /* 14: 2N x (2 max_iter) column-major: the chain after every half-step
+                                 (flag t; slot shift + 2 (iteration - 1)) */
 } ss_outputs;
 
 /* align_group_to_template: one group of frames (replaces mexFunction,

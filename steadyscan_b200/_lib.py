@@ -43,6 +43,7 @@ class SSOutputs(C.Structure):
         ("raw_params", C.c_void_p), ("all_params", C.c_void_p), ("frame_params", C.c_void_p),
         ("stop_reason", C.c_int32), ("trial_cap_hit", C.c_int32), ("n_frame_passes", C.c_int64),
         ("elapsed_ms", C.c_double), ("blocks_used", C.c_void_p),
+        ("iteration_times", C.c_void_p), ("function_times", C.c_void_p), ("rg_params", C.c_void_p),
     ]
 
 

@@ -122,6 +122,13 @@ def _outputs(args: dict, want_mask=True, want_history=False):
         a["frame_params"] = np.zeros(2 * (w + 1) * nF)
     if want_mask:
         a["mask"] = np.empty(hb * w * nF, np.uint8)
+    # outputs 9, 10 and 14 exist with the timing flags (mexgateway.cpp:266-300, task.cpp:242-248)
+    if "t" in letters:
+        a["rg_params"] = np.empty(2 * N * 2 * mi)
+    if "t" in letters or "T" in letters:
+        a["function_times"] = np.empty(14)
+    if "t" in letters and "T" in letters:
+        a["iteration_times"] = np.empty(mi)
     if want_history:
         a["iteration_corr"] = np.zeros(mi)
         a["frame_corr_history"] = np.zeros(nF * mi)
@@ -130,7 +137,8 @@ def _outputs(args: dict, want_mask=True, want_history=False):
     p = lambda k: a[k].ctypes.data if k in a else None
     o = SSOutputs(p("dx"), p("dy"), p("frame_corr"), p("iter_used"), p("mask"), p("residrms"),
                   p("device_init_time"), p("iteration_corr"), p("frame_corr_history"), p("iteration_errvals"),
-                  p("raw_params"), p("all_params"), p("frame_params"), 0, 0, 0, 0.0, p("blocks_used"))
+                  p("raw_params"), p("all_params"), p("frame_params"), 0, 0, 0, 0.0, p("blocks_used"),
+                  p("iteration_times"), p("function_times"), p("rg_params"))
     return o, a, (hb, w, nF, N, mi)
 
 
@@ -145,6 +153,9 @@ def _result(o: SSOutputs, a: dict, dims) -> dict:
              blocks_used=a["blocks_used"].reshape(w, nF, order="F").astype(bool))
     if "mask" in a:
         r["mask"] = a["mask"].reshape(hb, w * nF, order="F").astype(bool)
+    r["rg_params"] = a["rg_params"].reshape(2 * N, 2 * mi, order="F") if "rg_params" in a else None
+    r["function_times"] = a.get("function_times")
+    r["iteration_times"] = a.get("iteration_times")
     if "iteration_corr" in a:
         r["iteration_corr"] = a["iteration_corr"]
         r["frame_corr_history"] = a["frame_corr_history"].reshape(nF, mi, order="F")

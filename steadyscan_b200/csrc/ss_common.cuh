@@ -33,7 +33,16 @@ enum FlagBits : int {
   kFlagMedianBefore = 1 << 4,   // R
   kFlagRawParams = 1 << 5,      // P
   kFlagFrameOrdered = 1 << 6,   // p
+  kFlagTimeExec = 1 << 7,       // T: execution timing (outputs 9 and 10)
+  kFlagTimeSub = 1 << 8,        // t: sub-function timing, TimedMainIteration (outputs 9, 10, 14)
 };
+
+// The device's global clock in nanoseconds (the iteration times of flags T and t).
+__device__ __forceinline__ unsigned long long device_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Per-column sums written by k_eval. Assembly uses all slots; other modes a prefix.
 enum ColSum : int {
@@ -67,9 +76,12 @@ struct GroupCtl {
   int ls_pending;  // frames of the half-step whose line search still runs (trial rounds)
   int solve_now;          // 1 while the group's half-step solve of this cycle runs (set by k_solve_compact)
   int par_sel;            // flag M: the parity bitmap (0 or 1) of the last global correlation
+  int retry;              // the iteration is being retried without the filter
+  int rg_slot;            // flag t: rgParams slot of the half-step that just ended, -1 if none
   double correlation, corr;
   long long n_eval;      // frame evaluations the reference would count: errval passes and trials
   long long passes[4];   // frames read per evaluation kind (EvalMode)
+  unsigned long long t_mark;  // flags T and t: device clock (ns) at the start of the iteration
 };
 
 struct GroupDesc {
@@ -143,6 +155,8 @@ struct GroupDesc {
   // outputs on the device
   double *o_frame_corr, *o_residrms, *o_iter_corr, *o_frame_corr_hist, *o_iter_errvals, *o_all_params;
   double *o_dx, *o_dy, *o_frame_params, *o_raw;
+  double* o_rg_params;      // flag t: 2N x 2 max_iter, the chain after every half-step
+  double* o_iter_times;     // flags T and t: max_iter seconds
   uint8_t* o_mask;          // Hb x fW column-major, may be null
   uint8_t* o_blocks_used;   // fW: block column has a valid pixel in the final mask, may be null
 };

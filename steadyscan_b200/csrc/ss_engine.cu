@@ -105,6 +105,9 @@ __global__ void k_build_gquad(const double* __restrict__ xg, const double* __res
 // Sum of all frame samples of a group in two deterministic passes: kSumBlocks CTA partials over
 // fixed contiguous ranges, then one CTA adds the partials in a fixed order.
 constexpr int kSumBlocks = 296;
+// Entries of output 10: TimedMainIteration's ten sub-functions, then the correlation and the
+// iteration end's remainder, and two that the reference never writes (task.cpp:244).
+constexpr int kFunctionTimes = 14;
 
 __device__ __forceinline__ double block_sum(double s) {
   __shared__ double sh[32];
@@ -431,7 +434,9 @@ static int parse_flags(const char* flags, int& compute, int& bits) {
       case 'R': bits |= kFlagMedianBefore; break;
       case 'P': bits |= kFlagRawParams; break;
       case 'p': bits |= kFlagFrameOrdered; break;
-      default: break;  // T t I F W w G E r f V: timing, printing and debug switches
+      case 'T': bits |= kFlagTimeExec; break;
+      case 't': bits |= kFlagTimeSub; break;
+      default: break;  // I F W w G E r f V: printing and debug switches
     }
   }
   if (compute < 0)
@@ -730,6 +735,14 @@ struct Batch::Impl {
   std::vector<int> event_mode;
   size_t event_used = 0;
   double eval_ms[4] = {0, 0, 0, 0};
+  // flag t: CUDA-event timing of the stages, summed into the reference's sub-function slots
+  // (output 10, timedmainiteration.cpp:45-143 and task.cpp:293-356); the interval from a mark to the
+  // next one counts for the first mark's slot (-1: not counted)
+  bool ftime = false;
+  std::vector<cudaEvent_t> fevents;
+  std::vector<int> fslot;
+  size_t fused = 0;
+  double ftimes[kFunctionTimes] = {};
   // non-blocking cycle state: 0 prepared, 1 ready to launch a cycle, 2 cycle in flight, 3 finished
   int state = 0;
   int cur_rounds = 0;
@@ -741,6 +754,20 @@ struct Batch::Impl {
   bool graph_run = false;  // the run in flight was launched as the graph
   cudaGraphExec_t run_exec = nullptr;
   cudaStream_t cap_stream = nullptr;
+
+  void fmark(int slot) {
+    if (!ftime) return;
+    if (fused == fevents.size()) {
+      for (int k = 0; k < 64; k++) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        fevents.push_back(e);
+        fslot.push_back(-1);
+      }
+    }
+    cudaEventRecord(fevents[fused], stream);
+    fslot[fused++] = slot;
+  }
 
   void eval_timed(int mode) {
     if (mode == kTrial && ks.round)
@@ -774,6 +801,7 @@ Batch::Batch() : d(new Impl) {}
 Batch::~Batch() {
   if (d->stream && d->own_stream) cudaStreamSynchronize(d->stream);
   for (cudaEvent_t e : d->events) cudaEventDestroy(e);
+  for (cudaEvent_t e : d->fevents) cudaEventDestroy(e);
   if (d->ev_cycle) cudaEventDestroy(d->ev_cycle);
   if (d->run_exec) cudaGraphExecDestroy(d->run_exec);
   if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
@@ -930,6 +958,10 @@ static void layout(Batch::Impl* b, char* base) {
     G.o_raw = (o && o->raw_params) ? cv.take<double>(2 * N) : nullptr;
     G.o_mask = (o && o->mask) ? cv.take<uint8_t>(npx) : nullptr;
     G.o_blocks_used = (o && o->blocks_used) ? cv.take<uint8_t>(g.fW) : nullptr;
+    const bool timed = g.flags & kFlagTimeSub, exec_timed = g.flags & kFlagTimeExec;
+    G.o_rg_params = (o && o->rg_params && timed) ? cv.take<double>((size_t)2 * N * 2 * mi) : nullptr;
+    G.o_iter_times = (o && o->iteration_times && timed && exec_timed) ? cv.take<double>(mi) : nullptr;
+    if (timed && o && o->function_times) b->ftime = true;
   }
   b->d_gd = cv.take<GroupDesc>(gd.size());
   b->d_ctl = cv.take<GroupCtl>(gd.size());
@@ -1110,6 +1142,8 @@ static int reset_state(Batch::Impl* b) {
     SS_CK(cudaMemsetAsync(G.o_frame_corr, 0, nF * 8, s));
     SS_CK(cudaMemsetAsync(G.eig_valid, 0, N, s));
     SS_CK(cudaMemsetAsync(G.ls_done, 0, nF * sizeof(int), s));
+    if (G.o_rg_params) SS_CK(cudaMemsetAsync(G.o_rg_params, 0, (size_t)2 * N * 2 * g.in->max_iter * 8, s));
+    if (G.o_iter_times) SS_CK(cudaMemsetAsync(G.o_iter_times, 0, (size_t)g.in->max_iter * 8, s));
     k_fill<<<64, 256, 0, s>>>(G.errval, 2 * nF, kErrvalFill);
     // the reference's x/y/mask/difference buffers start zero-filled: NaN knots give an all-invalid
     // mask and a zero difference image
@@ -1172,23 +1206,48 @@ constexpr int kFirstRounds = 8, kMinRounds = 3, kMaxRounds = 16;
 static int enqueue_cycle(Batch::Impl* b) {
   cudaStream_t s = b->stream;
   const int nG = (int)b->gd.size();
+  // flag t's sub-function slots (output 10): 1 applyParameters, here with the errval, gradient and
+  // JᵀJ / Jᵀr sums of the same pass; 2 the group errvals and parameter mask; 4 the compaction;
+  // 5 the system's blocks (fillDiagonals, fillJtr); 7 the solve and its filter; 8 the expansion;
+  // 9 the line search; 10 the correlation; 11 the rest of the iteration end
+  b->fmark(1);
   b->eval_timed(kAssemble);
-  solve_launch(s, b->d_gd, b->d_ctl, nG);
+  if (b->ftime) {
+    const dim3 split(kSolveSplit, nG);
+    b->fmark(2);
+    k_solve_prep<<<split, kSolvePrepThreads, 0, s>>>(b->d_gd, b->d_ctl);
+    b->fmark(4);
+    k_solve_compact<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+    b->fmark(5);
+    k_solve_planes<<<split, kSolvePrepThreads, 0, s>>>(b->d_gd, b->d_ctl);
+    b->fmark(7);
+    k_solve_system<<<nG, kSolveThreads, kSolveSmem, s>>>(b->d_gd, b->d_ctl);
+    b->fmark(8);
+    k_solve_expand<<<split, kSolvePrepThreads, 0, s>>>(b->d_gd, b->d_ctl);
+  } else {
+    solve_launch(s, b->d_gd, b->d_ctl, nG);
+  }
   SS_CK(cudaGetLastError());
+  b->fmark(9);
   if (b->ks.round) {
     // trial rounds without a host round trip: as many as the longest search of the previous
     // cycle took; a search that needs more continues in the next cycle (its group skips
     // assembly and solve until it has finished)
     SS_CK(cudaMemsetAsync(b->d_counters, 0, sizeof(int), s));
     for (int r = 0; r < b->cur_rounds; r++) b->eval_timed(kTrial);
+    b->fmark(10);
     b->eval_timed(kCorr);  // correlation sums after the second half-step
+    b->fmark(9);
   } else {
     b->eval_timed(kTrial);  // line search (and, after shift 1, the correlation sums)
   }
   SS_CK(cudaGetLastError());
-  k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+  k_after_ls<<<nG, kAfterLsThreads, 0, s>>>(b->d_gd, b->d_ctl);
+  b->fmark(10);
   k_iter_sums<<<dim3(kIterSplit, nG), 256, 0, s>>>(b->d_gd, b->d_ctl);
+  b->fmark(11);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
+  b->fmark(-1);
   b->eval_timed(kFinal);
   k_final<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl, b->d_counters + 1);
   SS_CK(cudaGetLastError());
@@ -1329,7 +1388,7 @@ static int build_run_graph(Batch::Impl* b) {
   } else {
     b->ks.ls(b->n_frames_total, s, b->d_gd, b->d_frame_group, b->d_ctl, b->ls_win_bytes);
   }
-  k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(b->d_gd, b->d_ctl, nG);
+  k_after_ls<<<nG, kAfterLsThreads, 0, s>>>(b->d_gd, b->d_ctl);
   k_iter_sums<<<dim3(kIterSplit, nG), 256, 0, s>>>(b->d_gd, b->d_ctl);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(b->d_gd, b->d_ctl);
   sched_launch(kFinal, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
@@ -1378,6 +1437,7 @@ int Batch::start() {
   b->rounds = 0;
   b->launches = 0;
   b->event_used = 0;
+  b->fused = 0;
   b->cur_rounds = kFirstRounds;
   b->cycle_no = 0;
   b->graph_run = false;
@@ -1393,7 +1453,7 @@ int Batch::step() {
   Impl* b = d;
   if (b->state != 1) return fail(SS_ERR_INVALID_ARGUMENT, "batch: step() needs start() and a finished cycle");
   SS_CK(cudaSetDevice(b->device));
-  int rc = b->use_graph && !b->timing ? launch_run_graph(b) : launch_cycle(b);
+  int rc = b->use_graph && !b->timing && !b->ftime ? launch_run_graph(b) : launch_cycle(b);
   if (rc) return rc;
   b->state = 2;
   return SS_OK;
@@ -1407,6 +1467,13 @@ static int finish_run(Batch::Impl* b) {
   SS_CK(cudaMemcpyAsync(b->h_staging, b->d_staging, sizeof(b->h_staging), cudaMemcpyDeviceToHost, b->stream));
   SS_CK(cudaStreamSynchronize(b->stream));
   if (b->h_counters[kCounters] & 1) return fail(SS_ERR_CUDA, "a shared-memory staging copy did not complete in time");
+  for (int k = 0; k < kFunctionTimes; k++) b->ftimes[k] = 0;
+  for (size_t k = 0; k + 1 < b->fused; k++) {
+    if (b->fslot[k] < 0) continue;
+    float ms = 0;
+    SS_CK(cudaEventElapsedTime(&ms, b->fevents[k], b->fevents[k + 1]));
+    b->ftimes[b->fslot[k]] += ms * 1e-3;
+  }
   for (int m = 0; m < 4; m++) b->eval_ms[m] = 0;
   for (size_t k = 0; k < b->event_used; k += 2) {
     float ms = 0;
@@ -1518,6 +1585,20 @@ int Batch::collect() {
       SS_CK(cudaMemcpyAsync(o->frame_params, G.o_frame_params, 2 * nk * 8, cudaMemcpyDeviceToHost, s));
     if (o->raw_params && (g.flags & kFlagRawParams))
       SS_CK(cudaMemcpyAsync(o->raw_params, G.o_raw, 2 * (size_t)g.N * 8, cudaMemcpyDeviceToHost, s));
+    // outputs 9, 10, 14: zeros where the flags do not produce them
+    if (o->rg_params) {
+      if (G.o_rg_params)
+        SS_CK(cudaMemcpyAsync(o->rg_params, G.o_rg_params, (size_t)2 * g.N * 2 * mi * 8, cudaMemcpyDeviceToHost, s));
+      else
+        std::memset(o->rg_params, 0, (size_t)2 * g.N * 2 * mi * 8);
+    }
+    if (o->iteration_times) {
+      if (G.o_iter_times) SS_CK(cudaMemcpyAsync(o->iteration_times, G.o_iter_times, mi * 8, cudaMemcpyDeviceToHost, s));
+      else std::memset(o->iteration_times, 0, mi * 8);
+    }
+    if (o->function_times)
+      for (int k = 0; k < kFunctionTimes; k++)
+        o->function_times[k] = (g.flags & kFlagTimeSub) ? b->ftimes[k] : 0.0;
   }
   SS_CK(cudaStreamSynchronize(s));
   for (size_t i = 0; i < b->gd.size(); i++) {
@@ -1775,7 +1856,7 @@ int Server::step() {
   } else {
     v->ks.ls(v->n_frames, s, v->d_gd, v->d_frame_group, v->d_ctl, v->ls_win_bytes);
   }
-  k_after_ls<<<(nG + 127) / 128, 128, 0, s>>>(v->d_gd, v->d_ctl, nG);
+  k_after_ls<<<nG, kAfterLsThreads, 0, s>>>(v->d_gd, v->d_ctl);
   k_iter_sums<<<dim3(kIterSplit, nG), 256, 0, s>>>(v->d_gd, v->d_ctl);
   k_iter_end<<<nG, kSolveThreads, 0, s>>>(v->d_gd, v->d_ctl);
   sched_launch(kFinal, s, v->d_gd, v->d_ctl, v->d_chunk_group, nc, sc);

@@ -437,7 +437,12 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_prep(const GroupDes
     const bool present = G.asmcnt[c] >= G.min_points[c % W];
     G.blocks_present[c] = present;
     const int f = c / W;
-    if (!frame_active(G, f, shift)) continue;
+    if (!frame_active(G, f, shift)) {
+      // TimedMainIteration clears paramsUsed before every half-step (timedmainiteration.cpp:50), so
+      // the knots of inactive frames are unused; MainIteration leaves their last use
+      if (G.flags & kFlagTimeSub) G.params_used[c] = 0;
+      continue;
+    }
     const bool before = c > 0 && G.asmcnt[c - 1] >= G.min_points[(c - 1) % W];
     G.params_used[c] = present || before;
   }
@@ -495,6 +500,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_compact(const GroupDesc
   const bool starts = solve_starts(C);
   __syncthreads();  // every thread has read the phase before thread 0 changes the state below
   if (threadIdx.x == 0) C.solve_now = starts ? 1 : 0;
+  // the first iteration's clock starts at its first solve (flags T and t)
+  if (threadIdx.x == 0 && starts && G.o_iter_times && C.t_mark == 0) C.t_mark = device_clock_ns();
   if (!starts) return;
   const int t = threadIdx.x, nt = blockDim.x;
   const int N = G.N, nF = G.nF, shift = C.shift;
@@ -504,7 +511,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve_compact(const GroupDesc
   if (t == 0) {
     if (C.n_filter_iter != 0 && C.iteration > C.n_filter_iter) {
       C.filter_active = 0;
-      C.filter_id = 0;
+      // TimedMainIteration keeps filterID here (timedmainiteration.cpp:97-105)
+      if (!(G.flags & kFlagTimeSub)) C.filter_id = 0;
       C.n_filter_iter = 0;
     }
     sh_nact = 0;
@@ -817,35 +825,57 @@ __global__ void __launch_bounds__(kSolvePrepThreads) k_solve_expand(const GroupD
   }
 }
 
-// After the line search of a half-step (task_linesearch.cu:158-169, mainiteration.cpp:266-284).
-__global__ void k_after_ls(const GroupDesc* __restrict__ gds, GroupCtl* __restrict__ ctl, int n_groups) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_groups) return;
-  const GroupDesc& G = gds[g];
-  GroupCtl& C = ctl[g];
-  if (C.phase != kPhHalf || C.ls_state != 1 || C.ls_pending != 0) return;
-  C.ls_state = 0;
-  double e0 = 0, e1 = 0;
-  for (int i = 0; i < G.nF; i++) {
-    e0 += G.errval[i];
-    e1 += G.errval[i + G.nF];
+// After the line search of a half-step (task_linesearch.cu:158-169, mainiteration.cpp:266-284), a
+// CTA per group: thread 0 runs the control; with flag t the CTA then copies the chain into the
+// half-step's rgParams slot (timedmainiteration.cpp:124).
+constexpr int kAfterLsThreads = 128;
+__global__ void __launch_bounds__(kAfterLsThreads) k_after_ls(const GroupDesc* __restrict__ gds,
+                                                              GroupCtl* __restrict__ ctl) {
+  const GroupDesc& G = gds[blockIdx.x];
+  GroupCtl& C = ctl[blockIdx.x];
+  __shared__ int sh_slot;
+  if (threadIdx.x == 0) {
+    sh_slot = -1;
+    if (C.phase == kPhHalf && C.ls_state == 1 && C.ls_pending == 0) {
+      C.ls_state = 0;
+      double e0 = 0, e1 = 0;
+      for (int i = 0; i < G.nF; i++) {
+        e0 += G.errval[i];
+        e1 += G.errval[i + G.nF];
+      }
+      bool imp = C.shift ? (e0 > e1) : (e0 < e1);
+      C.improved = C.improved && imp;
+      // TimedMainIteration runs its retry as iteration + 1 (timedmainiteration.cpp:141); slots past
+      // its 2 max_iter are not written (the reference's buffer has 2 max_iter slots)
+      const int slot = C.shift + 2 * (C.iteration - 1 + C.retry);
+      if ((G.flags & kFlagTimeSub) && G.o_rg_params && slot < 2 * G.max_iter) sh_slot = slot;
+      if (C.shift == 0) {
+        C.shift = 1;
+      } else {
+        C.shift = 0;
+        if (!C.improved && C.n_filter_iter != 0) {  // retry this iteration without the filter
+          C.filter_active = 0;
+          C.n_filter_iter = 0;
+          C.improved = 1;
+          C.retry = 1;
+          // TimedMainIteration zeroes filterID here (timedmainiteration.cpp:136); MainIteration
+          // does not (mainiteration.cpp:96-106)
+          if (G.flags & kFlagTimeSub) C.filter_id = 0;
+        } else {
+          C.exec_result = C.improved;
+          C.phase = kPhIterEnd;
+          C.retry = 0;
+          C.par_sel ^= G.dparity != nullptr;  // the correlation pass's parity bitmap is the current one
+        }
+      }
+    }
   }
-  bool imp = C.shift ? (e0 > e1) : (e0 < e1);
-  C.improved = C.improved && imp;
-  if (C.shift == 0) {
-    C.shift = 1;
-    return;
-  }
-  C.shift = 0;
-  if (!C.improved && C.n_filter_iter != 0) {  // retry this iteration without the filter
-    C.filter_active = 0;
-    C.n_filter_iter = 0;
-    C.improved = 1;
-    return;
-  }
-  C.exec_result = C.improved;
-  C.phase = kPhIterEnd;
-  C.par_sel ^= G.dparity != nullptr;  // the correlation pass's parity bitmap is the current one
+  __syncthreads();
+  const int slot = sh_slot;
+  if (slot < 0) return;
+  const int P = 2 * G.N;
+  double* dst = G.o_rg_params + (size_t)slot * P;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) dst[i] = G.p[i];
 }
 
 __device__ inline double pearson(double n, double sd, double si, double sdd, double sii, double sdi) {
@@ -960,6 +990,13 @@ __global__ void __launch_bounds__(kSolveThreads) k_iter_end(const GroupDesc* __r
       action = 0;
     }
     sh_action = action;
+    // iteration times (flags T and t): not saved for an iteration that ends in the filter's
+    // switch-off (task.cpp:323 continues before :358-360); every iteration restarts the clock
+    if (G.o_iter_times) {
+      const unsigned long long now = device_clock_ns();
+      if (action != 1 && it <= G.max_iter) G.o_iter_times[it - 1] = (double)(now - C.t_mark) * 1e-9;
+      C.t_mark = now;
+    }
   }
   __syncthreads();
   const int action = sh_action;

@@ -36,12 +36,13 @@ def test_exports_every_declared_symbol(lib):
 
 
 def test_abi_version(lib):
-    assert lib.ss_abi_version() == 5  # ss_reconstruct_frames (reconstruction on the device)
+    assert lib.ss_abi_version() == 6  # outputs 9, 10 and 14 (flags T and t) at the end of ss_outputs
 
 
 def test_struct_sizes_match_header(lib):
     """The ctypes mirrors have the C structs' layout: the last field sits where the header puts it."""
-    assert C.sizeof(_lib.SSOutputs) == 13 * 8 + 4 + 4 + 8 + 8 + 8
+    assert C.sizeof(_lib.SSOutputs) == 13 * 8 + 4 + 4 + 8 + 8 + 8 + 3 * 8
+    assert _lib.SSOutputs.rg_params.offset == 13 * 8 + 4 + 4 + 8 + 8 + 8 + 2 * 8
     assert _lib.SSRecording.corr_thresh.offset == C.sizeof(_lib.SSInputs) + 8
     assert C.sizeof(_lib.SSRecordingOutputs) == 7 * 8 + 8
     # ss_prep_frames: ss_matrix (32), n_frames (+pad), pregauss at 40, mednorm 48, cropping 52..68,

@@ -50,6 +50,9 @@ CASES = {
     "uint16_frames": dict(frame_dtype=np.uint16, seed=8),
     # a knot chain longer than the solve's 1024 partitions: partitions with interior nodes
     "long_chain": dict(n_frames=72, nknots=17, seed=61),
+    # huge first steps: trials with no block present whose moving knots are the frame's first
+    "absent_trial_movement": dict(seed=45, n_frames=4, clip_px=6.0, jumps=2, jump_px=4.0,
+                                  settings={"gpu_filter_max_iterations": 2}),
 }
 
 
@@ -128,6 +131,51 @@ def _compare_history(args):
     np.testing.assert_allclose(g["frame_corr_history"][:, :it], o["frame_corr_hist"][:it].T, rtol=1e-9, atol=1e-12)
     np.testing.assert_allclose(g["all_params"][:, :it], o["all_params"][:it].T, atol=KNOT_TOL_D)
     return o, g
+
+
+# Flag t (TimedMainIteration): the cases of the timed reference-run fixtures
+TIMED = {
+    "retry_odd": dict(n_frames=3, seed=6, settings={"gpu_solver_id": 1}),
+    "filter_limit": dict(seed=41, n_frames=4, clip_px=6.0, jumps=2, jump_px=4.0,
+                         settings={"gpu_solver_id": 1, "gpu_filter_max_iterations": 2}),
+    "mask_inactive": dict(n_frames=6, seed=10, settings={"gpu_solver_id": 1, "haltcorr": 0.15}),
+}
+
+
+@pytest.mark.parametrize("name", list(TIMED))
+def test_flag_t_timed_iteration_and_rg_params(name):
+    """Flag t switches to TimedMainIteration's bookkeeping (paramsUsed cleared every half-step,
+    its filterID rules, the retry as the next iteration) and fills output 14 with the chain after
+    every half-step."""
+    args, _, _ = make_args(**TIMED[name])
+    args["flags"] = "DCcet" + ("M" if name == "mask_inactive" else "")
+    o, g = _compare_history(args)
+    k = 2 * o["iterations"] + 2
+    rg = g["rg_params"]
+    assert rg.shape == (2 * (args["tfrac"].shape[1] * int(args["nFrames"]) + 1), 2 * int(args["max_iter"]))
+    np.testing.assert_allclose(rg[:, :k], o["rg_params"][:k].T, atol=KNOT_TOL_D)
+    assert not np.any(rg[:, k:])
+    assert not np.any(g["function_times"][[0, 3, 6, 12, 13]])
+    assert g["iteration_times"] is None  # output 9 needs flag T as well
+
+
+def test_timing_outputs_flags_T_and_t():
+    args, _, _ = make_args(seed=4, n_frames=6)
+    g = api.align_group(dict(args, flags="STt"), want_history=True)
+    it = g["iter_used"]
+    ft, itt = g["function_times"], g["iteration_times"]
+    assert ft.shape == (14,) and itt.shape == (int(args["max_iter"]),)
+    assert np.all(ft[[1, 2, 4, 5, 7, 8, 9, 10, 11]] > 0) and not np.any(ft[[0, 3, 6, 12, 13]])
+    assert ft.sum() <= g["elapsed_ms"] / 1000.0
+    assert np.all(itt[:it] >= 0) and np.count_nonzero(itt[:it]) >= it - 1 and not np.any(itt[it:])
+    assert itt.sum() <= g["elapsed_ms"] / 1000.0
+    # the chain after the second half-step of every iteration is the iteration's chain (output 15),
+    # one slot pair later when the iteration was retried without the filter
+    rg, ap = g["rg_params"], g["all_params"]
+    for j in range(it):
+        assert any(np.array_equal(rg[:, s], ap[:, j]) for s in (2 * j + 1, 2 * j + 3) if s < rg.shape[1])
+    g2 = api.align_group(dict(args, flags="ST"))
+    assert not np.any(g2["function_times"]) and g2["iteration_times"] is None and g2["rg_params"] is None
 
 
 @pytest.mark.parametrize("seed,halt", [(16, 0.2), (10, 0.15)])
