@@ -263,7 +263,13 @@ def prepare_frames(frames, layout, pregauss: float = 0.0, mednorm: bool = False,
         keep.append(a)
         h, w, n = a.shape
         fm = SSMatrix(a.ctypes.data, h, w * n, _NP_DTYPE[a.dtype], SS_HOST)
-    gidx = np.asfortranarray(prep._block_gather_index(layout.prevknotind, layout.frame_w).astype(np.int32))
+    gidx = getattr(layout, "_gather_i32", None)  # the layout's gather map, built once per layout
+    if gidx is None:
+        gidx = np.asfortranarray(prep._block_gather_index(layout.prevknotind, layout.frame_w).astype(np.int32))
+        try:
+            layout._gather_i32 = gidx
+        except AttributeError:
+            pass
     hb, nb = gidx.shape
     tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32,
            np.dtype(np.uint16): torch.uint16}[np.dtype(out_dtype)]

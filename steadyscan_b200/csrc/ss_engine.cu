@@ -2018,23 +2018,52 @@ void* Batch::stream() const { return d->stream; }
 
 namespace ss {
 
-// Device allocations and a stream of one synchronous call, released when it returns (the stream
-// drained first).
+// The library's memory pool of a device for the work memory of synchronous calls: stream-ordered
+// allocations whose freed memory the pool keeps for the next call (no cudaMalloc / cudaFree, and no
+// device-wide synchronisation, per call once a call of that size has run).
+static cudaMemPool_t work_pool(int device) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(device);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[device] = pool;
+  return pool;
+}
+
+// Device allocations and a stream of one synchronous call, released into the device's work pool
+// when it returns (the stream drained first). The stream must exist before the first take().
 struct CallMem {
   std::vector<void*> ptrs;
   cudaStream_t s = nullptr;
+  cudaMemPool_t pool = nullptr;
   CallMem() = default;
   CallMem(const CallMem&) = delete;
   CallMem& operator=(const CallMem&) = delete;
   ~CallMem() {
-    if (s) cudaStreamSynchronize(s);
-    for (void* q : ptrs) cudaFree(q);
-    if (s) cudaStreamDestroy(s);
+    for (void* q : ptrs) cudaFreeAsync(q, s);
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
   }
   template <class T>
   T* take(size_t count) {
+    if (!s) return nullptr;
+    if (!pool) {
+      int dev = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess || !(pool = work_pool(dev))) return nullptr;
+    }
     void* q = nullptr;
-    if (cudaMalloc(&q, std::max<size_t>(1, count) * sizeof(T)) != cudaSuccess) return nullptr;
+    if (cudaMallocFromPoolAsync(&q, std::max<size_t>(1, count) * sizeof(T), pool, s) != cudaSuccess) return nullptr;
     ptrs.push_back(q);
     return static_cast<T*>(q);
   }
@@ -2066,9 +2095,9 @@ __global__ void k_to_f64(const void* __restrict__ in, double* __restrict__ out, 
 template <class InT>
 static void fe_blur(const void* in, double* w1, double* w2, int h, int w, int n, int ph, int pw, const double* ty,
                     int ry, const double* tx, int rx, cudaStream_t s) {
-  const int nb = 148 * 8;
-  k_blur_pass<InT, 0><<<nb, 256, 0, s>>>(in, w1, h, w, n, ph, ty, ry);
-  k_blur_pass<double, 1><<<nb, 256, 0, s>>>(w1, w2, h, w, n, pw, tx, rx);
+  const dim3 grid((h + 255) / 256, w, n);
+  k_blur_pass<InT, 0><<<grid, 256, 0, s>>>(in, w1, h, w, ph, ty, ry);
+  k_blur_pass<double, 1><<<grid, 256, 0, s>>>(w1, w2, h, w, pw, tx, rx);
 }
 
 template <class InT>
@@ -2109,6 +2138,7 @@ int prepare_frames(const ss_prep_frames* p) {
     return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: frames must be SS_F64, SS_F32, SS_U16 or SS_F16");
   if (blur && !(p->pregauss < 3989.0))
     return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: pregauss must be below 3989");
+  if (blur && w > 65535) return fail(SS_ERR_INVALID_ARGUMENT, "prepare_frames: the blur takes frames of at most 65535 columns");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
   if (p->gpu_device_id < 0 || p->gpu_device_id >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
@@ -2126,7 +2156,8 @@ int prepare_frames(const ss_prep_frames* p) {
     tx = blur_taps(sd, pw, &rx);
   }
   const size_t fsz = dtype_size(fdt), osz = dtype_size(o.dtype), npx = (size_t)h * w;
-  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, ((size_t)1 << 30) / (16 * npx)));
+  // frames per pass: about 1 GB of FP64 work memory, and the blur grid's z extent
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>({(size_t)n, ((size_t)1 << 30) / (16 * npx), (size_t)65535}));
   CallMem m;
   SS_CK(cudaStreamCreateWithFlags(&m.s, cudaStreamNonBlocking));
   cudaStream_t s = m.s;
@@ -2331,7 +2362,8 @@ int reconstruct_frames(const ss_reconstruct* r) {
     }
     k_rc_mask<<<g, 256, 0, s>>>(b, nf);
     k_rc_coef<<<g, 256, 0, s>>>(b, nf, regfac, vf2);
-    k_rc_count<<<g, 256, 0, s>>>(b, nf, d_count);
+    const dim3 fg(std::max(1, g / nf), nf);  // per-frame grids: at most g CTAs (one wave) over the frames
+    k_rc_count<<<fg, 256, 0, s>>>(b, d_count);
     SS_CK(cudaGetLastError());
     std::vector<int> count(nf), state(nf), due(nf);
     SS_CK(cudaMemcpyAsync(count.data(), d_count, nf * 4, cudaMemcpyDeviceToHost, s));
@@ -2355,11 +2387,11 @@ int reconstruct_frames(const ss_reconstruct* r) {
     const int kMaxSweeps = 1 << 22;
     for (int it = 1; running > 0; it++) {
       if (it > kMaxSweeps) return fail(SS_ERR_CUDA, "reconstruct: the energy kept decreasing over 4M sweeps");
-      for (int colour = 0; colour < 4; colour++) k_rc_sweep<<<g, 256, 0, s>>>(b, nf, colour, d_state);
+      for (int colour = 0; colour < 4; colour++) k_rc_sweep<<<fg, 256, 0, s>>>(b, colour, d_state);
       k_rc_due<<<cb, 128, 0, s>>>(nf, d_state, d_interval, it, d_due);
       k_rc_energy<<<eg, 256, 0, s>>>(b, nf, d_due, regfac, vf2);
       k_rc_check<<<cb, 128, 0, s>>>(nf, d_due, d_state, d_eo, d_keep, b.part, b.part_l, 0, it, d_iters);
-      k_rc_keep<<<g, 256, 0, s>>>(b, nf, d_keep);
+      k_rc_keep<<<fg, 256, 0, s>>>(b, d_keep);
       if (it % 8 == 0) {
         SS_CK(cudaMemcpyAsync(state.data(), d_state, nf * 4, cudaMemcpyDeviceToHost, s));
         SS_CK(cudaStreamSynchronize(s));

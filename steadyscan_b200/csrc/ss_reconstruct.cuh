@@ -217,18 +217,18 @@ __global__ void __launch_bounds__(256) k_rc_coef(RcBufs b, int nf, double regfac
 }
 
 // One colour sweep of the frames still running (state[f] == 1).
-__global__ void __launch_bounds__(256) k_rc_sweep(RcBufs b, int nf, int colour, const int* __restrict__ state) {
+__global__ void __launch_bounds__(256) k_rc_sweep(RcBufs b, int colour, const int* __restrict__ state) {
+  const int f = blockIdx.y;
+  if (state[f] != 1) return;
   const int th = b.th, tw = b.tw;
   const int rh = (th + 1 - (colour >> 1)) >> 1, cw = (tw + 1 - (colour & 1)) >> 1;  // rows / columns of the colour
-  const size_t per = (size_t)rh * cw, total = per * nf;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const int f = (int)(e / per);
-    if (state[f] != 1) continue;
-    const int k = (int)(e - (size_t)f * per);
+  const int per = rh * cw;
+  float* x = b.x + (size_t)f * b.np;
+  const float* cf0 = b.coef + (size_t)f * b.np * 10;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < per; k += gridDim.x * blockDim.x) {
     const int r = 2 * (k % rh) + (colour >> 1), c = 2 * (k / rh) + (colour & 1);
     const int p = r + th * c;
-    float* x = b.x + (size_t)f * b.np;
-    const float* cf = b.coef + ((size_t)f * b.np + p) * 10;
+    const float* cf = cf0 + (size_t)p * 10;
     const int q[8] = {p - 1, p + th - 1, p + th, p + th + 1, p + 1, p - th + 1, p - th, p - th - 1};
     float s = 0.0f;
 #pragma unroll
@@ -321,17 +321,30 @@ __global__ void k_rc_due(int nf, const int* __restrict__ state, const int* __res
   if (f < nf) due[f] = state[f] == 1 && it % interval[f] == 0;
 }
 
-// Masked pixels of every frame (a frame with none is skipped, as the reference's `continue`).
-__global__ void __launch_bounds__(256) k_rc_count(RcBufs b, int nf, int* __restrict__ count) {
-  const size_t total = (size_t)b.np * nf;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
-    if (b.mask[e]) atomicAdd(count + e / b.np, 1);
+// Masked pixels of every frame (a frame with none is skipped, as the reference's `continue`); grid
+// (blocks, frames), one atomic per CTA.
+__global__ void __launch_bounds__(256) k_rc_count(RcBufs b, int* __restrict__ count) {
+  const int f = blockIdx.y;
+  const uint8_t* mk = b.mask + (size_t)f * b.np;
+  int c = 0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < b.np; p += gridDim.x * blockDim.x) c += mk[p] ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  __shared__ int sc[8];
+  if ((threadIdx.x & 31) == 0) sc[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sc[w];
+    if (t) atomicAdd(count + f, t);
+  }
 }
 
-__global__ void __launch_bounds__(256) k_rc_keep(RcBufs b, int nf, const int* __restrict__ keep) {
-  const size_t total = (size_t)b.np * nf;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
-    if (keep[e / b.np]) b.xo[e] = b.x[e];
+// The candidate iterate of the frames whose check kept the sweep: xo = x; grid (blocks, frames).
+__global__ void __launch_bounds__(256) k_rc_keep(RcBufs b, const int* __restrict__ keep) {
+  const int f = blockIdx.y;
+  if (!keep[f]) return;
+  const size_t o = (size_t)f * b.np;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < b.np; p += gridDim.x * blockDim.x) b.xo[o + p] = b.x[o + p];
 }
 
 // Output of a finished frame: its candidate iterate, NaN outside the mask.
