@@ -61,6 +61,8 @@ def parse():
                     help="groups of the ragged batch also run one batch per group")
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged batch with the autotuner")
     ap.add_argument("--only-ragged", action="store_true", help="run and print only the ragged batch")
+    ap.add_argument("--only-pipeline", action="store_true",
+                    help="run and print only the frame preparation and reconstruction legs")
     ap.add_argument("--ragged-lean", action="store_true",
                     help="ragged batch at the default schedule only (no tuner, no comparison runs)")
     ap.add_argument("--serve-warm", action="store_true",
@@ -430,7 +432,7 @@ def traffic_summary():
 
 # ------------------------------------------------------------------------------------------------
 
-def pipeline(groups, dev_frames, results, settings, lay, device, recon_frames: int) -> dict:
+def pipeline(groups, dev_frames, results, settings, lay, device, recon_frames: int, cpu: bool = True) -> dict:
     """The rows either side of the alignment on the same workload: the reference driver's frame
     preparation (ss_prepare_frames: block reorder of raw frames, and with the prefilter
     pregauss = 1, mednorm) over all frames, and the reconstruction (ss_reconstruct_frames) of one
@@ -460,7 +462,15 @@ def pipeline(groups, dev_frames, results, settings, lay, device, recon_frames: i
         got = api.prepare_frames(raw3, lay, **kw)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        out[name] = {"frames": n, "frames_per_s": n / dt, "ms": dt * 1e3}
+        # algorithmic bytes: the raw frames read once and the block matrices written once
+        ob = 2 if name == "block_reorder_u16" else 8
+        algo = n * (h * w * 2 + lay.frame_h * lay.frame_w * ob)
+        pk, pk_kind = peaks()
+        out[name] = {"frames": n, "frames_per_s": n / dt, "ms": dt * 1e3,
+                     "roofline": {"bound": "hbm", "algorithmic_bytes": algo, "achieved_gbs": algo / dt / 1e9,
+                                  "frac": algo / dt / 1e9 / pk, "peak": pk, "peak_source": pk_kind,
+                                  "note": "whole call timed on the host (work memory, launches and the "
+                                          "blur's and median's extra passes included)"}}
         if name == "block_reorder_u16":
             out[name]["equals_block_frames"] = bool(torch.equal(got.T.reshape(-1).view(torch.int16),
                                                                 flat.view(torch.int16)))
@@ -481,6 +491,26 @@ def pipeline(groups, dev_frames, results, settings, lay, device, recon_frames: i
                           "masked_fraction": float(rc["mask"].mean()),
                           "note": "one set (one invert_bilinear_sampling call) of the first group's frames, "
                                   "template 512x512, ibs_regfac 3e-3, host output"}
+    if cpu:
+        # CPU baselines: the numpy restatements of the reference's MATLAB code on a bounded sample
+        # (one host thread: numpy's FFT and scipy's sparse products are single-threaded)
+        from oracle import frontend as ofe
+        from oracle import reconstruct as orc
+        nfc, nrc = 16, 4
+        host = raw16[:nfc].cpu().numpy().view(np.uint16).reshape(nfc, w, h).transpose(2, 1, 0)
+        for name, gsd, med in (("block_reorder_u16", 0.0, False), ("prefilter_f64", 1.0, True)):
+            t0 = time.perf_counter()
+            ofe.set_bmdata(host, lay.prevknotind, lay.frame_w, lay.cropping, gsd, med)
+            dtc = time.perf_counter() - t0
+            out[name]["cpu_baseline"] = {"frames_per_s": nfc / dtc, "cores": 1, "kind": "port",
+                                         "sample": f"{nfc} frames, numpy restatement (FFT blur)"}
+        t0 = time.perf_counter()
+        orc.invert_bilinear_sampling(host[:, :, :nrc].astype(np.float32), dxk[:, :nrc], dyk[:, :nrc],
+                                     settings["basex"], settings["basey"], settings["tfrac"],
+                                     settings["prevknotind"], th, tw)
+        dtc = time.perf_counter() - t0
+        out["reconstruct"]["cpu_baseline"] = {"frames_per_s": nrc / dtc, "cores": 1, "kind": "port",
+                                              "sample": f"the set's first {nrc} frames, numpy/scipy restatement"}
     return out
 
 
@@ -604,12 +634,19 @@ def storage_sweep(args, device) -> dict:
         dt = time.perf_counter() - t0
         r = b.collect()
         b.close()
-        return (np.concatenate([x["dx"] for x in r]), np.concatenate([x["dy"] for x in r])), n / dt
+        # frames the reference's caller marks failed (steady_scan.m:246-284): correlation below
+        # corr_thresh 0.75, or fewer than minblockfrac 0.25 of the blocks with a valid pixel
+        ok = np.concatenate([(x["frame_corr"] >= 0.75) & (x["blocks_used"].mean(axis=0) >= 0.25) for x in r])
+        return (np.concatenate([x["dx"] for x in r]), np.concatenate([x["dy"] for x in r]), ok), n / dt
 
     def err(k, ref):
         d = np.concatenate([k[0] - ref[0], k[1] - ref[1]])
+        keep = np.repeat(ref[2], lay.frame_w + 1)  # the knots of the frames the caller keeps (D run)
+        da = np.concatenate([(k[0] - ref[0])[keep], (k[1] - ref[1])[keep]])
         return {"rms_px": float(np.sqrt(np.mean(d * d))), "max_px": float(np.max(np.abs(d))),
-                "within_0p05_px": float(np.mean(np.abs(d) <= 0.05))}
+                "within_0p05_px": float(np.mean(np.abs(d) <= 0.05)),
+                "accepted_frames": int(ref[2].sum()), "rms_px_accepted": float(np.sqrt(np.mean(da * da))),
+                "max_px_accepted": float(np.max(np.abs(da)))}
 
     ref, v_d = run(dev, SS_U16, "D")
     out = {"workload": f"{n} frames of 512x512, knots every 2 lines, groups of 64, lambda 5e-3; "
@@ -743,6 +780,15 @@ def main():
         dgroups.append(d)
     batch = api.Batch(dgroups)
     stream = torch.cuda.ExternalStream(batch.stream_ptr, device=device)
+
+    if args.only_pipeline:  # the rows either side of the alignment, on this workload's frames and knots
+        batch.run()
+        results = batch.collect()
+        batch.close()
+        if rank == 0:
+            print(json.dumps({"pipeline": pipeline(groups, dev_frames, results, settings, lay, device,
+                                                   args.recon_frames, cpu=not args.no_cpu)}))
+        return
 
     def barrier():
         if dist:
@@ -886,7 +932,8 @@ def main():
 
     pipeline_line = None
     if rank == 0 and not args.no_pipeline:
-        pipeline_line = pipeline(groups, dev_frames, results, settings, lay, device, args.recon_frames)
+        pipeline_line = pipeline(groups, dev_frames, results, settings, lay, device, args.recon_frames,
+                                 cpu=not args.no_cpu)
 
     serving_line = None
     if rank == 0 and args.serve_seconds > 0:
