@@ -19,7 +19,8 @@ constexpr int kTrialCap = 2048;
 enum EvalMode : int { kAssemble = 0, kTrial = 1, kCorr = 2, kFinal = 3 };
 
 // Group phases of the device-side control state machine.
-enum Phase : int { kPhHalf = 0, kPhIterEnd = 1, kPhFinal = 2, kPhDone = 3 };
+// kPhWait: the group's frames are still on their way to the device (streamed uploads).
+enum Phase : int { kPhHalf = 0, kPhIterEnd = 1, kPhFinal = 2, kPhDone = 3, kPhWait = 4 };
 
 // StopCriterion (interface/stopcriterion.h:4-10).
 enum Stop : int { kStopCorrInc = 0, kStopHaltCorr = 1, kStopMovement = 2, kStopIterLimit = 3, kStopError = 4 };

@@ -109,6 +109,9 @@ constexpr int kSumBlocks = 296;
 // iteration end's remainder, and two that the reference never writes (task.cpp:244).
 constexpr int kFunctionTimes = 14;
 
+// The library's stream-ordered memory pool of a device (defined with the per-call work memory).
+static cudaMemPool_t work_pool(int device);
+
 __device__ __forceinline__ double block_sum(double s) {
   __shared__ double sh[32];
   s = warp_sum(s);
@@ -458,6 +461,7 @@ enum RunCounter {
   kCtrRound = 3,      // trial rounds of the graph's current cycle
   kCtrRounds = 4,     // trial rounds run by the graph
   kCtrBound = 5,      // bit 0: the graph stopped at the cycle bound; bit 1: a cycle hit its round bound
+  kCtrWaiting = 6,    // groups whose streamed frames have not arrived (k_join)
   kCounters = 8
 };
 
@@ -735,6 +739,13 @@ struct Batch::Impl {
   std::vector<int> event_mode;
   size_t event_used = 0;
   double eval_ms[4] = {0, 0, 0, 0};
+  // streamed frame uploads (set_stream_frames): the upload stream, its start event, and a ready
+  // flag per group written after the group's frames and image sum
+  bool stream_req = false;
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t ev_up = nullptr;
+  int* d_ready = nullptr;
+  bool pool_arena = false;  // the arena comes from the library's memory pool
   // flag t: CUDA-event timing of the stages, summed into the reference's sub-function slots
   // (output 10, timedmainiteration.cpp:45-143 and task.cpp:293-356); the interval from a mark to the
   // next one counts for the first mark's slot (-1: not counted)
@@ -805,13 +816,26 @@ Batch::~Batch() {
   if (d->ev_cycle) cudaEventDestroy(d->ev_cycle);
   if (d->run_exec) cudaGraphExecDestroy(d->run_exec);
   if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
-  if (d->arena && !d->external_arena) cudaFree(d->arena);
+  if (d->up_stream) {
+    cudaStreamSynchronize(d->up_stream);
+    cudaStreamDestroy(d->up_stream);
+  }
+  if (d->ev_up) cudaEventDestroy(d->ev_up);
+  if (d->arena && !d->external_arena) {
+    if (d->pool_arena) {
+      cudaFreeAsync(d->arena, d->stream);
+      cudaStreamSynchronize(d->stream);
+    } else {
+      cudaFree(d->arena);
+    }
+  }
   if (d->h_counters) cudaFreeHost(d->h_counters);
   if (d->stream && d->own_stream) cudaStreamDestroy(d->stream);
   delete d;
 }
 
 size_t Batch::arena_bytes() const { return d->arena_bytes; }
+void Batch::set_stream_frames(bool on) { d->stream_req = on; }
 
 // Lays out all device buffers of the batch; with base == nullptr only measures.
 static void layout(Batch::Impl* b, char* base) {
@@ -828,6 +852,7 @@ static void layout(Batch::Impl* b, char* base) {
   b->d_counters = cv.take<int>(kCounters);
   b->d_staging = cv.take<unsigned long long>(kStagingCounters);
   b->d_sum_parts = cv.take<double>(kSumBlocks);
+  b->d_ready = b->stream_req ? cv.take<int>(std::max<size_t>(1, b->hg.size())) : nullptr;
   b->win_bytes = 0;
   b->ls_win_bytes = 0;
   for (size_t i = 0; i < b->hg.size(); i++) {
@@ -1038,7 +1063,11 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     b->arena = external;
     b->external_arena = true;
   } else {
-    SS_CK(cudaMalloc(&b->arena, b->arena_bytes));
+    cudaMemPool_t pool = work_pool(b->device);
+    if (!pool) return fail(SS_ERR_OUT_OF_MEMORY, "no device memory pool");
+    if (cudaMallocFromPoolAsync(&b->arena, b->arena_bytes, pool, b->stream) != cudaSuccess)
+      return fail(SS_ERR_OUT_OF_MEMORY, "device arena");
+    b->pool_arena = true;
   }
   char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(b->arena) + 255) & ~uintptr_t(255));
   layout(b, base);
@@ -1081,7 +1110,8 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
         SS_CK(cudaMemcpyAsync((void*)G.col_yrange, g.yrange.data(), g.yrange.size() * 4, cudaMemcpyHostToDevice, s));
       }
     }
-    if (!g.frames_dev)
+    const bool streamed = b->stream_req && !g.frames_dev;  // uploaded by start() on the upload stream
+    if (!g.frames_dev && !streamed)
       SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
     SS_CK(cudaMemcpyAsync(g.d_p0, g.p0.data(), g.p0.size() * 8, cudaMemcpyHostToDevice, s));
     if (g.tpl_src == -1) {
@@ -1110,7 +1140,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
         k_build_gquad<__half><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (__half*)G.gquad);
     }
     SS_CK(cudaGetLastError());
-    b->sum(G.image, (size_t)g.Hb * g.fW, b->d_sum_parts, g.d_sum, s);
+    if (!streamed) b->sum(G.image, (size_t)g.Hb * g.fW, b->d_sum_parts, g.d_sum, s);
     SS_CK(cudaGetLastError());
     const int nchunks = (g.nF + g.frames_per_cta - 1) / g.frames_per_cta;
     for (int t = 0; t < nchunks; t++) chunk_group[G.chunk_base + t] = (int)i;
@@ -1153,7 +1183,7 @@ static int reset_state(Batch::Impl* b) {
     SS_CK(cudaGetLastError());
     GroupCtl& C = b->h_ctl[i];
     std::memset(&C, 0, sizeof(C));
-    C.phase = kPhHalf;
+    C.phase = b->stream_req && !g.frames_dev ? kPhWait : kPhHalf;
     C.iteration = 1;
     C.improved = 1;
     C.stop_reason = kStopError;
@@ -1200,6 +1230,30 @@ static cudaError_t block_tridiag_attr() { return smem_attr(k_block_tridiag, (int
 // later ones (set from the longest search that ended in the cycle before).
 constexpr int kFirstRounds = 8, kMinRounds = 3, kMaxRounds = 16;
 
+// Groups whose streamed frames have arrived (ready flag, written on the upload stream after the
+// frames and their image sum) join the run at the start of the cycle; ctr[kCtrWaiting] counts those
+// still waiting. One CTA.
+__global__ void __launch_bounds__(1024) k_join(GroupCtl* __restrict__ ctl, const int* __restrict__ ready, int n_groups,
+                                               int* __restrict__ ctr) {
+  int waiting = 0;
+  for (int g = threadIdx.x; g < n_groups; g += blockDim.x) {
+    if (ctl[g].phase != kPhWait) continue;
+    if (ld_acquire(ready + g)) ctl[g].phase = kPhHalf;
+    else waiting++;
+  }
+  for (int o = 16; o > 0; o >>= 1) waiting += __shfl_xor_sync(0xffffffffu, waiting, o);
+  __shared__ int sw[32];
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = waiting;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sw[w];
+    ctr[kCtrWaiting] = t;
+  }
+}
+
+__global__ void k_set_flag(int* __restrict__ flag) { *flag = 1; }
+
 // Enqueues one cycle of every group's state machine on the batch stream (assembly, solve, trial
 // rounds or the cluster line search, correlation, iteration end, final pass) and the copy of the
 // cycle's counters to pinned memory.
@@ -1210,6 +1264,7 @@ static int enqueue_cycle(Batch::Impl* b) {
   // JᵀJ / Jᵀr sums of the same pass; 2 the group errvals and parameter mask; 4 the compaction;
   // 5 the system's blocks (fillDiagonals, fillJtr); 7 the solve and its filter; 8 the expansion;
   // 9 the line search; 10 the correlation; 11 the rest of the iteration end
+  if (b->d_ready) k_join<<<1, 1024, 0, s>>>(b->d_ctl, b->d_ready, nG, b->d_counters);
   b->fmark(1);
   b->eval_timed(kAssemble);
   if (b->ftime) {
@@ -1300,10 +1355,12 @@ __global__ void __launch_bounds__(kSchedThreads) k_sched_rounds(const GroupDesc*
   }
 }
 
-// Condition of the cycle loop: another cycle while a group is running, up to `max_cycles`.
+// Condition of the cycle loop: another cycle while a group is running, up to `max_cycles`. A cycle
+// in which every running group still waits for its frames does not count toward the bound.
 __global__ void k_cycle_ctl(int* __restrict__ ctr, int n_groups, int max_cycles, cudaGraphConditionalHandle h) {
   if (threadIdx.x != 0) return;
-  const int c = ++ctr[kCtrCycles];
+  const bool idle = ctr[kCtrWaiting] > 0 && ctr[kCtrWaiting] + ctr[kCtrDone] >= n_groups;
+  const int c = idle ? ctr[kCtrCycles] : ++ctr[kCtrCycles];
   const bool running = ctr[kCtrDone] < n_groups;
   if (running && c >= max_cycles) ctr[kCtrBound] |= 1;
   cudaGraphSetConditional(h, running && c < max_cycles ? 1u : 0u);
@@ -1362,7 +1419,7 @@ static int build_run_graph(Batch::Impl* b) {
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
   // top: counters, the cycle loop, the counters to the host
   SS_CK(cudaStreamBeginCaptureToGraph(s, top, nullptr, nullptr, 0, mode));
-  cudaMemsetAsync(b->d_counters + kCtrCycles, 0, (kCtrBound - kCtrCycles + 1) * sizeof(int), s);
+  cudaMemsetAsync(b->d_counters + kCtrCycles, 0, (kCtrWaiting - kCtrCycles + 1) * sizeof(int), s);
   rc = capture_while(s, h_cycle, &body);
   cudaMemcpyAsync(b->h_counters, b->d_counters, kCounters * sizeof(int), cudaMemcpyDeviceToHost, s);
   cudaGraph_t out = nullptr;
@@ -1374,6 +1431,7 @@ static int build_run_graph(Batch::Impl* b) {
   SS_CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, mode));
   int* sc = b->d_sched;
   const int nc = b->n_chunks;
+  if (b->d_ready) k_join<<<1, 1024, 0, s>>>(b->d_ctl, b->d_ready, nG, b->d_counters);
   sched_launch(kAssemble, s, b->d_gd, b->d_ctl, b->d_chunk_group, nc, sc);
   b->ks.eval(kAssemble, b->n_tiles, s, b->d_gd, sc, nc, b->d_ctl, b->max_hb, b->win_bytes);
   solve_launch(s, b->d_gd, b->d_ctl, nG);
@@ -1433,6 +1491,25 @@ int Batch::start() {
   SS_CK(smem_attr(k_solve_system, (int)kSolveSmem));
   int rc = reset_state(b);
   if (rc) return rc;
+  if (b->d_ready) {  // streamed frames: upload, image sum and ready flag per group, in group order
+    cudaStream_t s = b->stream;
+    if (!b->up_stream) SS_CK(cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking));
+    if (!b->ev_up) SS_CK(cudaEventCreateWithFlags(&b->ev_up, cudaEventDisableTiming));
+    SS_CK(cudaMemsetAsync(b->d_ready, 0, b->hg.size() * sizeof(int), s));
+    SS_CK(cudaEventRecord(b->ev_up, s));
+    SS_CK(cudaStreamWaitEvent(b->up_stream, b->ev_up, 0));
+    for (size_t i = 0; i < b->hg.size(); i++) {
+      const HostGroup& g = b->hg[i];
+      if (g.frames_dev) {
+        k_set_flag<<<1, 1, 0, b->up_stream>>>(b->d_ready + i);
+        continue;
+      }
+      SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, b->up_stream));
+      b->sum(b->gd[i].image, (size_t)g.Hb * g.fW, b->d_sum_parts, g.d_sum, b->up_stream);
+      k_set_flag<<<1, 1, 0, b->up_stream>>>(b->d_ready + i);
+    }
+    SS_CK(cudaGetLastError());
+  }
   b->cycles = 0;
   b->rounds = 0;
   b->launches = 0;
@@ -1461,6 +1538,7 @@ int Batch::step() {
 
 // Completion of the batch: final state, error word and staging counters on the host.
 static int finish_run(Batch::Impl* b) {
+  if (b->up_stream) SS_CK(cudaStreamSynchronize(b->up_stream));
   SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost,
                         b->stream));
   SS_CK(cudaMemcpyAsync(b->h_counters + kCounters, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
@@ -2470,6 +2548,7 @@ int ss_align_groups(int32_t n_groups, const ss_inputs* in, ss_outputs* out) {
   auto t0 = std::chrono::steady_clock::now();
   if (!in || n_groups < 1) return ss::fail(SS_ERR_INVALID_ARGUMENT, "no groups");
   ss::Batch b;
+  b.set_stream_frames(true);  // frames of later groups upload while earlier groups run
   int rc = b.prepare(n_groups, in, out, nullptr, 0);
   if (!rc) rc = b.run();
   if (!rc) rc = b.collect();

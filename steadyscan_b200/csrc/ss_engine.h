@@ -30,6 +30,10 @@ class Batch {
   // cudaStream_t) runs the batch on the caller's stream without blocking on it.
   int prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
               const Batch* const* sessions = nullptr, bool measure_only = false, void* borrow_stream = nullptr);
+  // Before prepare(): upload the frames of host-resident groups on a second stream while earlier
+  // groups already run (each group joins the run when its frames have arrived). For batches run
+  // once, such as ss_align_groups; results are those of an unstreamed run.
+  void set_stream_frames(bool on);
   // Runs every group from its initial knots to its stop criterion.
   int run();
   // The same run one cycle at a time without blocking: start() resets every group to its initial

@@ -288,6 +288,24 @@ def test_batched_equals_single():
         np.testing.assert_array_equal(single["residrms"], b["residrms"])
 
 
+@pytest.mark.parametrize("prec", ["D", "S"])
+def test_streamed_uploads_equal_the_resident_batch(prec):
+    """ss_align_groups uploads host frames on a second stream while earlier groups run (each group
+    joins when its frames have arrived): the results are those of a batch whose frames were all
+    uploaded before the run."""
+    specs = [dict(seed=41 + k, n_frames=2 + k % 3, frame_dtype=np.uint16) for k in range(6)]
+    groups = [dict(make_args(**sp)[0], flags=prec) for sp in specs]
+    streamed = api.align_groups(groups, want_mask=False)
+    b = api.Batch(groups)
+    b.run()
+    resident = b.collect()
+    b.close()
+    for a, r in zip(streamed, resident):
+        assert a["iter_used"] == r["iter_used"] and a["stop_reason"] == r["stop_reason"]
+        for k in ("dx", "dy", "frame_corr", "residrms"):
+            np.testing.assert_array_equal(a[k], r[k])
+
+
 def test_persistent_grid_many_tiles_precision_s():
     """A batch with more tiles (block column x frame chunk) than the persistent grid has CTAs, so
     every CTA takes several tiles, and searches spread over several cycles: each group still gets
