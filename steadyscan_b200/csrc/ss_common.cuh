@@ -110,9 +110,6 @@ struct GroupDesc {
   // Precision 'S': the template as FP32 rows of tpitch floats (16-byte aligned rows) for staging
   // row windows in shared memory, and per block column the [min, max] of basey over valid rows.
   const float* tplain;
-  // The same rows in four planes (column x at (x mod 4) tpitch / 4 + x / 4): the windows of trial
-  // tiles on the 16-byte path (quad_ok), whose lanes read columns 4 apart in one plane.
-  const float* tplain4;
   int tpitch;
   const float* col_yrange;  // W x 2
   int* err;                 // device error word of the batch (bit 0: a staging copy timed out)

@@ -75,18 +75,6 @@ __global__ void k_build_tplain(const double* __restrict__ T, int Ht, int Wt, int
   }
 }
 
-// The rows of k_build_tplain in four planes of pitch / 4 floats: column x of row iy at
-// iy pitch + (x mod 4) pitch / 4 + x / 4 (zero padding).
-__global__ void k_build_tplain4(const double* __restrict__ T, int Ht, int Wt, int pitch, float* __restrict__ out) {
-  const size_t n = (size_t)Ht * pitch;
-  const int q = pitch / 4;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int iy = (int)(i / pitch), pos = (int)(i % pitch);
-    const int ix = 4 * (pos % q) + pos / q;
-    out[i] = ix < Wt ? (float)T[(size_t)ix * Ht + iy] : 0.0f;
-  }
-}
-
 // Gradient quads (xg[iy][ix], xg[iy+1][ix], yg[iy][ix], yg[iy][ix+1]) for caller gradients that
 // are not the template's forward differences.
 template <class TplT>
@@ -920,7 +908,6 @@ static void layout(Batch::Impl* b, char* base) {
       G.tquad = S.tquad;
       G.gquad = S.gquad;
       G.tplain = S.tplain;
-      G.tplain4 = S.tplain4;
       G.tpitch = S.tpitch;
     } else {
       G.tquad = cv.take<char>(nq * 4 * tsz);
@@ -931,7 +918,6 @@ static void layout(Batch::Impl* b, char* base) {
       // (the layout's measuring pass takes no memory: decide by the condition, not by the pointer)
       const bool rows = b->compute == 1 && b->tpl_dt == SS_F32 && g.grad_derived && 2 * G.tpitch * 4 <= kWinBytes;
       G.tplain = rows ? cv.take<float>((size_t)g.Ht * G.tpitch) : nullptr;
-      G.tplain4 = rows ? cv.take<float>((size_t)g.Ht * G.tpitch) : nullptr;
       g.d_templ_stage = cv.take<double>((size_t)g.Ht * g.Wt);
       if (!g.grad_derived) {
         g.d_xg_stage = cv.take<double>((size_t)g.Ht * g.Wt);
@@ -1131,7 +1117,6 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     } else if (b->tpl_dt == SS_F32) {
       k_build_tquad<float><<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, (float*)G.tquad);
       if (G.tplain) k_build_tplain<<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, G.tpitch, (float*)G.tplain);
-      if (G.tplain4) k_build_tplain4<<<nb, 256, 0, s>>>(g.d_templ_stage, g.Ht, g.Wt, G.tpitch, (float*)G.tplain4);
       if (!g.grad_derived)
         k_build_gquad<float><<<nb, 256, 0, s>>>(g.d_xg_stage, g.d_yg_stage, g.Ht, g.Wt, (float*)G.gquad);
     } else {

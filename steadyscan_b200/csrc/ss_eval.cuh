@@ -1159,10 +1159,7 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     window_rows(G, G.col_yrange[2 * cc] + klo, G.col_yrange[2 * cc + 1] + khi, win_cap, r0, rows);
     if (rows > 0) {
       float* wbuf = reinterpret_cast<float*>(smem);
-      // tiles on the 16-byte path (every windowed frame of a quad_ok group takes it) read the
-      // four-plane rows
-      const float* src = (sizeof(FrameT) == 2 && G.quad_ok) ? G.tplain4 : G.tplain;
-      if (stage_window(G, wbuf, r0, rows, bar, bar_phase, src)) win = {wbuf, r0, rows, G.tpitch};
+      if (stage_window(G, wbuf, r0, rows, bar, bar_phase, G.tplain)) win = {wbuf, r0, rows, G.tpitch};
       else win_ok = false;  // a copy may still be in flight: no further windows in this CTA
     }
   }
@@ -1185,13 +1182,15 @@ __device__ __forceinline__ void trial_tile(const GroupDesc& G, GroupCtl& C, int 
     int cnt;
     bool quads = false;
     if constexpr (sizeof(FrameT) == 2) quads = G.quad_ok;
+    // separate call sites for the staged window and the global rows keep the window's loads in
+    // shared memory
     if (quads && win.p) {
       if constexpr (sizeof(FrameT) == 2)
-        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane), pair_win4(win), ssd, cnt);
+        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(win), ssd, cnt);
     } else if (quads && grows) {  // the whole template's rows in global memory as the window
       if constexpr (sizeof(FrameT) == 2)
-        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1, 8 * lane),
-                              pair_win4(TWin{G.tplain4, 0, G.Ht, G.tpitch}), ssd, cnt);
+        trial_pairs16<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(TWin{G.tplain, 0, G.Ht, G.tpitch}),
+                              ssd, cnt);
     } else if (win.p && G.pair_ok) {
       trial_pairs<FrameT>(G, coli, pair_col(G, cc, x0, x1, y0, y1), pair_win(win), ssd, cnt);
     } else if (grows && G.pair_ok) {

@@ -258,55 +258,18 @@ __device__ __forceinline__ void trial_pairs(const GroupDesc& G, size_t coli, con
   ssd_out = (double)warp_sumf(ssd.x + ssd.y);
 }
 
-// Window addressing of the four-plane rows (GroupDesc::tplain4): column ix of window row ry sits at
-// ry pitch + (ix mod 4) q + ix / 4 with q = pitch / 4, its right neighbour q further, or for
-// ix mod 4 == 3 at the next position of plane 0. Lanes that read columns 4 apart (trial_pairs16)
-// then read consecutive floats of one plane: 32 banks instead of 8. From v = 2^23 + floor(c), whose
-// bits are 0x4B000000 + ix with 0x4B000000 a multiple of 4, the index is
-// vy pitch + (vx mod 4) q + vx / 4 - kbias in wrapping 32-bit arithmetic; both corners are clamped
-// so masked pixels stay in bounds.
-struct PairWin4 {
-  const float* p;
-  unsigned pitch, q, kbias, emax;
-};
-__device__ __forceinline__ PairWin4 pair_win4(const TWin& w) {
-  PairWin4 v;
-  v.p = w.p;
-  v.pitch = (unsigned)w.pitch;
-  v.q = (unsigned)w.pitch >> 2;
-  v.kbias = 0x4B000000u * (unsigned)w.pitch + (0x4B000000u >> 2) + (unsigned)w.r0 * (unsigned)w.pitch;
-  v.emax = (unsigned)((w.rows - 1) * w.pitch - 1);
-  return v;
-}
-__device__ __forceinline__ void pair_sample4(const PairWin4& w, float2 x, float2 y, float2& xf, float2& yf,
-                                             float2& t00, float2& t01, float2& t10, float2& t11) {
-  const float2 big = f2(8388608.0f);
-  const float2 vx = __fadd2_rd(x, big), vy = __fadd2_rd(y, big);
-  xf = sub2(x, sub2(vx, big));
-  yf = sub2(y, sub2(vy, big));
-  const unsigned uA = __float_as_uint(vx.x), uB = __float_as_uint(vx.y);
-  const unsigned eA = __float_as_uint(vy.x) * w.pitch + (uA & 3u) * w.q + (uA >> 2) - w.kbias;
-  const unsigned eB = __float_as_uint(vy.y) * w.pitch + (uB & 3u) * w.q + (uB >> 2) - w.kbias;
-  const unsigned nA = min(eA + ((uA & 3u) == 3u ? 1u - 3u * w.q : w.q), w.emax);
-  const unsigned nB = min(eB + ((uB & 3u) == 3u ? 1u - 3u * w.q : w.q), w.emax);
-  const float* qA = w.p + min(eA, w.emax);
-  const float* qB = w.p + min(eB, w.emax);
-  const float* rA = w.p + nA;
-  const float* rB = w.p + nB;
-  t00 = f2(qA[0], qB[0]);
-  t01 = f2(rA[0], rB[0]);
-  t10 = f2(qA[w.pitch], qB[w.pitch]);
-  t11 = f2(rA[w.pitch], rB[w.pitch]);
-}
-
 // trial_pairs for 16-bit frame samples with knots every 1 or 2 lines, Hb a multiple of 256 and a
-// 16-byte aligned column: each lane loads rows 8 lane .. 8 lane + 7 of every 256-row step as one
-// 16-byte load (four pixel pairs), two steps ahead (the trial kernel's 64 registers hold no more). The lane's pairs keep the line offsets of rows 8 lane and 8 lane + 1 (k <= 2),
-// so pc is pair_col's with its first row at 8 lane; pair m of step t sits at j0 + m (2 >> ks) +
-// t (256 >> ks). Same arithmetic per pixel as trial_pairs.
+// 16-byte aligned column, on the plain window rows: each lane loads rows 8 lane .. 8 lane + 7 of
+// every 256-row step as one 16-byte load (four pixel pairs), and four shuffles hand the pairs round
+// so that in round rho lane L = 4 a + b takes pair L + 32 m of the step, m = (b - rho) mod 4, from
+// lane 8 m + a, which sends its word b (each lane first rotates its words by lane / 8, so the word
+// it sends in round rho is its rotated word rho). The lanes of a round then take pairs 32 apart on
+// consecutive template columns: no bank conflicts on the plain rows, whose index needs no plane
+// arithmetic. pc is pair_col's with row0 = 2 lane; pair L + 32 m + 128 t sits at
+// j0 + (64 m + 256 t) / k. One step in flight keeps the kernel within its registers.
 template <class FrameT>
-__device__ __forceinline__ void trial_pairs16(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin4& w,
-                                              double& ssd_out, int& cnt_out) {
+__device__ __forceinline__ void trial_pairs16(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
+                                               double& ssd_out, int& cnt_out) {
   static_assert(sizeof(FrameT) == 2, "16-bit frame samples");
   using PL = PairLoad<FrameT>;
   const int lane = threadIdx.x & 31;
@@ -314,38 +277,35 @@ __device__ __forceinline__ void trial_pairs16(const GroupDesc& G, size_t coli, c
   const uint4* col = reinterpret_cast<const uint4*>(reinterpret_cast<const FrameT*>(G.image) + coli);
   const int steps = G.Hb >> 8;
   const int ks = __ffs(G.geo_k) - 1;
-  const float dm = (float)(2 >> ks), dt = (float)(256 >> ks);
+  const float d64 = (float)(64 >> ks), dt = (float)(256 >> ks);
+  const int b = lane & 3, a = lane >> 2, rot = lane >> 3;
   float2 ssd = f2(0.f);
   int cnt = 0;
-  constexpr int kPf = 2;
-  uint4 ring[kPf];
-#pragma unroll
-  for (int d = 0; d < kPf; d++) ring[d] = d < steps ? __ldg(col + d * 32 + lane) : make_uint4(0u, 0u, 0u, 0u);
+  uint4 next = __ldg(col + lane);
 #pragma unroll 1
-  for (int t0 = 0; t0 < steps; t0 += kPf) {
+  for (int t = 0; t < steps; t++) {
+    uint4 cur = next;
+    if (t + 1 < steps) next = __ldg(col + (t + 1) * 32 + lane);
+    if (rot & 1) cur = make_uint4(cur.y, cur.z, cur.w, cur.x);
+    if (rot & 2) cur = make_uint4(cur.z, cur.w, cur.x, cur.y);
+    const float2 jb = add2(pc.j0, f2(dt * (float)t));
+    const uint32_t wv[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
-    for (int d = 0; d < kPf; d++) {
-      const int t = t0 + d;
-      if (t >= steps) break;
-      const uint4 cur = ring[d];
-      if (t + kPf < steps) ring[d] = __ldg(col + (t + kPf) * 32 + lane);
-      const float2 jb = add2(pc.j0, f2(dt * (float)t));
-      const uint32_t wv[4] = {cur.x, cur.y, cur.z, cur.w};
-#pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const float2 j = add2(jb, f2(dm * (float)m));
-        const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
-        const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
-        const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
-        cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
-        float2 xf, yf, t00, t01, t10, t11;
-        pair_sample4(w, x, y, xf, yf, t00, t01, t10, t11);
-        const float2 a = fma2(yf, sub2(t10, t00), t00), b = fma2(yf, sub2(t11, t01), t01);
-        const float2 wI = fma2(xf, sub2(b, a), a);
-        float2 d2 = sub2(PL::cvt(wv[m]), wI);
-        d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
-        ssd = fma2(d2, d2, ssd);
-      }
+    for (int rho = 0; rho < 4; rho++) {
+      const int m = (b - rho) & 3;
+      const uint32_t v = __shfl_sync(0xffffffffu, wv[rho], (m << 3) | a);
+      const float2 j = add2(jb, f2(d64 * (float)m));
+      const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
+      const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+      const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+      cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+      float2 xf, yf, t00, t01, t10, t11;
+      pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+      const float2 a2 = fma2(yf, sub2(t10, t00), t00), b2 = fma2(yf, sub2(t11, t01), t01);
+      const float2 wI = fma2(xf, sub2(b2, a2), a2);
+      float2 d2 = sub2(PL::cvt(v), wI);
+      d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
+      ssd = fma2(d2, d2, ssd);
     }
   }
   cnt_out = warp_sum(cnt);

@@ -78,7 +78,7 @@ __device__ __forceinline__ void window_rows(const GroupDesc& G, float ylo, float
 // batch's error word: the copy may then still be in flight, so the phase is left as it is, the
 // caller stages no further window in this CTA (its later tiles and passes sample the global
 // template instead) and calls drain_window before the CTA exits.
-// src: the rows to copy from (G.tplain, or G.tplain4 for the four-plane layout).
+// src: the rows to copy from (G.tplain when null).
 __device__ __forceinline__ bool stage_window(const GroupDesc& G, float* win, int r0, int rows, uint64_t* bar,
                                            unsigned& phase, const float* src = nullptr) {
   __syncthreads();  // the previous window is no longer read
