@@ -116,7 +116,8 @@ def make_workload(n_frames, size, group, precision, seed, device):
     from steadyscan_b200 import prep, synth
     rng = np.random.default_rng(seed)
     nk = size // 2 + 1
-    tmpl = synth.make_template(size, size, 400 * (size * size) // (512 * 512), (2.0, 6.0), rng)
+    # column-major, as the C ABI reads it: no conversion per call
+    tmpl = np.asfortranarray(synth.make_template(size, size, 400 * (size * size) // (512 * 512), (2.0, 6.0), rng))
     walk = synth.make_walk(size * (n_frames + 1), 0.1, 10.0, (0, 3), size, 4.0, rng)
     s = prep.init_settings({"nknots": nk, "gpu_forced_precision": precision, "lambda": 5e-3}, tmpl, size, size)
     lay = prep.block_layout(s)

@@ -248,7 +248,7 @@ def template_gradients(template: np.ndarray):
     t = np.asarray(template, dtype=np.float64)
     xg = np.concatenate([np.diff(t, axis=1), np.full((t.shape[0], 1), np.nan)], axis=1)
     yg = np.concatenate([np.diff(t, axis=0), np.full((1, t.shape[1]), np.nan)], axis=0)
-    return xg, yg
+    return np.asfortranarray(xg), np.asfortranarray(yg)  # column-major, as the C ABI reads them
 
 
 def min_points_per_block(prevknotind: np.ndarray, nknots: int, ratio: float) -> np.ndarray:
@@ -282,7 +282,8 @@ def block_layout(settings: dict) -> BlockLayout:
     bx, _ = image2blockmatrix(np.asarray(settings["basex"], dtype=np.float64) - 1, pk, nk - 1)
     by, _ = image2blockmatrix(np.asarray(settings["basey"], dtype=np.float64) - 1, pk, nk - 1)
     mp = min_points_per_block(pk, nk, float(settings["min_blockpoints_ratio"]))
-    return BlockLayout(nk, nk - 1, tfrac.shape[0], pk, tfrac, bx, by, bmask, mp,
+    f = np.asfortranarray  # column-major, as the C ABI reads them (no conversion per call)
+    return BlockLayout(nk, nk - 1, tfrac.shape[0], pk, f(tfrac), f(bx), f(by), f(bmask), mp,
                        list(settings["cropping"]))
 
 
@@ -329,8 +330,9 @@ def boundary_arguments(settings: dict, template: np.ndarray, bm_data: np.ndarray
         "basey": lay.basey,
         "base_mask": lay.base_mask,
         "bmData": bm_data,
-        "est_dx_knots": np.asarray(est_dx_knots, dtype=np.float64),
-        "est_dy_knots": np.asarray(est_dy_knots, dtype=np.float64),
+        # column-major like every matrix of the C ABI (no conversion per call)
+        "est_dx_knots": np.asfortranarray(est_dx_knots, dtype=np.float64),
+        "est_dy_knots": np.asfortranarray(est_dy_knots, dtype=np.float64),
         "group_size": lay.frame_w * int(settings["gpu_frame_groupsize"]),
         "nFrames": int(n_frames),
         "min_points_per_block": lay.min_points,
