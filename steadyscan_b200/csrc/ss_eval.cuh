@@ -651,7 +651,14 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
     } else if constexpr (sizeof(Acc) == 4) {
       const bool pairs = win.p && G.pair_ok && !k.dual;
       if (MODE == kAssemble && pairs) {
-        assemble_pairs<FrameT>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt);
+        bool quads = false;
+        if constexpr (sizeof(FrameT) == 2) quads = G.quad_ok;  // 16-byte loads handed round by shuffles
+        if (quads) {
+          if constexpr (sizeof(FrameT) == 2)
+            assemble_pairs16<FrameT>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt);
+        } else {
+          assemble_pairs<FrameT>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt);
+        }
         if ((threadIdx.x & 31) == 0) atomicAdd(G.staging + 5, 1ull);
       } else if (MODE != kAssemble && pairs) {
         corr_pairs<FrameT, MODE>(G, coli, pair_col(G, cc, k.ax0, k.ax1, k.ay0, k.ay1), pair_win(win), out, cnt, mo);

@@ -143,6 +143,61 @@ __device__ __forceinline__ void pair_sample(const PairWin& w, float2 x, float2 y
 // values and NaN have larger patterns).
 __device__ __forceinline__ bool in_range(float c, unsigned lim_bits) { return __float_as_uint(c) < lim_bits; }
 
+// The assembly sums of one lane's pixel pairs (kCsSsd .. kCsJ2y, in that order) and its valid count.
+struct AsmAcc {
+  float2 v[kCsAssemble];
+  int cnt;
+  __device__ __forceinline__ AsmAcc() : cnt(0) {
+#pragma unroll
+    for (int i = 0; i < kCsAssemble; i++) v[i] = f2(0.f);
+  }
+  // the pixel pair at j (both halves) with frame samples img: warp, mask, bilinear sample and
+  // gradients, residual, and the sums of JᵀJ blocks ((1-f)², f², f(1-f)), Jᵀr and SSD
+  __device__ __forceinline__ void add(const PairCol& pc, const PairWin& w, float2 j, float2 img, unsigned twb,
+                                      unsigned thb) {
+    const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy), f = fma2(pc.fsj, j, pc.f0);
+    const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
+    const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
+    cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
+    float2 xf, yf, t00, t01, t10, t11;
+    pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
+    const float2 gy0 = sub2(t10, t00), gy1 = sub2(t11, t01);
+    const float2 gx0 = sub2(t01, t00), gx1 = sub2(t11, t10);
+    const float2 a = fma2(yf, gy0, t00), b = fma2(yf, gy1, t01);
+    const float2 wI = fma2(xf, sub2(b, a), a);
+    float2 wx = fma2(yf, sub2(gx1, gx0), gx0);
+    float2 wy = fma2(xf, sub2(gy1, gy0), gy0);
+    float2 d2 = sub2(img, wI);
+    d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
+    wx = f2(mA ? wx.x : 0.f, mB ? wx.y : 0.f);
+    wy = f2(mA ? wy.x : 0.f, mB ? wy.y : 0.f);
+    const float2 c = sub2(f2(1.0f), f);
+    const float2 csq = mul2(c, c), fsq = mul2(f, f), fc = mul2(f, c);
+    const float2 gxx = mul2(wx, wx), gyy = mul2(wy, wy), gxy = mul2(wx, wy);
+    v[0] = fma2(d2, d2, v[0]);
+    v[1] = fma2(gxx, csq, v[1]);
+    v[2] = fma2(gyy, csq, v[2]);
+    v[3] = fma2(gxy, csq, v[3]);
+    v[4] = fma2(gxx, fsq, v[4]);
+    v[5] = fma2(gyy, fsq, v[5]);
+    v[6] = fma2(gxy, fsq, v[6]);
+    v[7] = fma2(gxx, fc, v[7]);
+    v[8] = fma2(gyy, fc, v[8]);
+    v[9] = fma2(gxy, fc, v[9]);
+    const float2 d1 = mul2(d2, c), dd2 = mul2(d2, f);
+    v[10] = fma2(d1, wx, v[10]);
+    v[11] = fma2(d1, wy, v[11]);
+    v[12] = fma2(dd2, wx, v[12]);
+    v[13] = fma2(dd2, wy, v[13]);
+  }
+  // the block's partials reduced in FP32 over the warp, combined in FP64 by the solve
+  __device__ __forceinline__ void reduce(double (&out)[kCsStride], int& cnt_out) const {
+    cnt_out = warp_sum(cnt);
+#pragma unroll
+    for (int i = 0; i < kCsAssemble; i++) out[i] = (double)warp_sumf(v[i].x + v[i].y);
+  }
+};
+
 // Assembly sums (kCsSsd .. kCsJ2y) and valid count of one block column at knots that are both the
 // mask and the difference-image knots. out/cnt are warp-reduced (all lanes).
 template <class FrameT>
@@ -153,11 +208,9 @@ __device__ __forceinline__ void assemble_pairs(const GroupDesc& G, size_t coli, 
   const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
   const FrameT* col = reinterpret_cast<const FrameT*>(G.image) + coli;
   const int steps = G.Hb >> 6;
-  float2 ssd = f2(0.f), axx = f2(0.f), ayy = f2(0.f), axy = f2(0.f), bxx = f2(0.f), byy = f2(0.f), bxy = f2(0.f),
-         oxx = f2(0.f), oyy = f2(0.f), oxy = f2(0.f), j1x = f2(0.f), j1y = f2(0.f), j2x = f2(0.f), j2y = f2(0.f);
-  int cnt = 0;
+  AsmAcc acc;
   float2 j = pc.j0;
-  const float2 dj = f2(pc.dj), one = f2(1.0f);
+  const float2 dj = f2(pc.dj);
   // kPrefetchAsm steps of frame samples in flight (a register ring)
   typename PL::W ring[kPrefetchAsm];
 #pragma unroll
@@ -170,48 +223,48 @@ __device__ __forceinline__ void assemble_pairs(const GroupDesc& G, size_t coli, 
       if (t >= steps) break;
       const typename PL::W cur = ring[d];
       if (t + kPrefetchAsm < steps) ring[d] = PL::load(col, (t + kPrefetchAsm) * 32 + lane);
-      const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy), f = fma2(pc.fsj, j, pc.f0);
+      acc.add(pc, w, j, PL::cvt(cur), twb, thb);
       j = add2(j, dj);
-      const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
-      const bool mB = in_range(x.y, twb) && in_range(y.y, thb);
-      cnt += (mA ? 1 : 0) + (mB ? 1 : 0);
-      float2 xf, yf, t00, t01, t10, t11;
-      pair_sample(w, x, y, xf, yf, t00, t01, t10, t11);
-      const float2 gy0 = sub2(t10, t00), gy1 = sub2(t11, t01);
-      const float2 gx0 = sub2(t01, t00), gx1 = sub2(t11, t10);
-      const float2 a = fma2(yf, gy0, t00), b = fma2(yf, gy1, t01);
-      const float2 wI = fma2(xf, sub2(b, a), a);
-      float2 wx = fma2(yf, sub2(gx1, gx0), gx0);
-      float2 wy = fma2(xf, sub2(gy1, gy0), gy0);
-      float2 d2 = sub2(PL::cvt(cur), wI);
-      d2 = f2(mA ? d2.x : 0.f, mB ? d2.y : 0.f);
-      wx = f2(mA ? wx.x : 0.f, mB ? wx.y : 0.f);
-      wy = f2(mA ? wy.x : 0.f, mB ? wy.y : 0.f);
-      const float2 c = sub2(one, f);
-      const float2 csq = mul2(c, c), fsq = mul2(f, f), fc = mul2(f, c);
-      const float2 gxx = mul2(wx, wx), gyy = mul2(wy, wy), gxy = mul2(wx, wy);
-      ssd = fma2(d2, d2, ssd);
-      axx = fma2(gxx, csq, axx);
-      ayy = fma2(gyy, csq, ayy);
-      axy = fma2(gxy, csq, axy);
-      bxx = fma2(gxx, fsq, bxx);
-      byy = fma2(gyy, fsq, byy);
-      bxy = fma2(gxy, fsq, bxy);
-      oxx = fma2(gxx, fc, oxx);
-      oyy = fma2(gyy, fc, oyy);
-      oxy = fma2(gxy, fc, oxy);
-      const float2 d1 = mul2(d2, c), dd2 = mul2(d2, f);
-      j1x = fma2(d1, wx, j1x);
-      j1y = fma2(d1, wy, j1y);
-      j2x = fma2(dd2, wx, j2x);
-      j2y = fma2(dd2, wy, j2y);
     }
   }
-  // the block's partials reduced in FP32, combined in FP64 by the solve
-  cnt_out = warp_sum(cnt);
-  const float2 v[kCsAssemble] = {ssd, axx, ayy, axy, bxx, byy, bxy, oxx, oyy, oxy, j1x, j1y, j2x, j2y};
+  acc.reduce(out, cnt_out);
+}
+
+// assemble_pairs for 16-bit frame samples with knots every 1 or 2 lines, Hb a multiple of 256 and a
+// 16-byte aligned column: the frame samples of a 256-row step arrive as one 16-byte load per lane
+// and are handed round by four shuffles as in trial_pairs16 (lane L = 4 a + b takes pair L + 32 m,
+// m = (b - rho) mod 4, in round rho), so the lanes of a round read consecutive template columns.
+// One load per lane covers four pairs of work: twice the bytes in flight of assemble_pairs' ring.
+template <class FrameT>
+__device__ __forceinline__ void assemble_pairs16(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
+                                                 double (&out)[kCsStride], int& cnt_out) {
+  static_assert(sizeof(FrameT) == 2, "16-bit frame samples");
+  using PL = PairLoad<FrameT>;
+  const int lane = threadIdx.x & 31;
+  const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
+  const uint4* col = reinterpret_cast<const uint4*>(reinterpret_cast<const FrameT*>(G.image) + coli);
+  const int steps = G.Hb >> 8;
+  const int ks = __ffs(G.geo_k) - 1;
+  const float d64 = (float)(64 >> ks), dt = (float)(256 >> ks);
+  const int b = lane & 3, a = lane >> 2, rot = lane >> 3;
+  AsmAcc acc;
+  uint4 next = __ldg(col + lane);
+#pragma unroll 1
+  for (int t = 0; t < steps; t++) {
+    uint4 cur = next;
+    if (t + 1 < steps) next = __ldg(col + (t + 1) * 32 + lane);
+    if (rot & 1) cur = make_uint4(cur.y, cur.z, cur.w, cur.x);
+    if (rot & 2) cur = make_uint4(cur.z, cur.w, cur.x, cur.y);
+    const float2 jb = add2(pc.j0, f2(dt * (float)t));
+    const uint32_t wv[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
-  for (int i = 0; i < kCsAssemble; i++) out[i] = (double)warp_sumf(v[i].x + v[i].y);
+    for (int rho = 0; rho < 4; rho++) {
+      const int m = (b - rho) & 3;
+      const uint32_t v = __shfl_sync(0xffffffffu, wv[rho], (m << 3) | a);
+      acc.add(pc, w, add2(jb, f2(d64 * (float)m)), PL::cvt(v), twb, thb);
+    }
+  }
+  acc.reduce(out, cnt_out);
 }
 
 // Trial SSD and valid count of one block column (task_linesearch.cu:50-74 with the SSD of
