@@ -35,19 +35,24 @@ constexpr int kLsMaxKnots = 256;    // knots per cluster CTA: frame_w <= kLsClus
 constexpr int kMaxFrameW = kLsCluster * kLsMaxKnots;
 constexpr int kMinWinFrames = 4;    // frames of a tile worth staging a template window for
 
-// Resident 256-thread CTAs per SM requested from the register allocator: the FP32 path is
-// latency-bound on frame loads and template gathers and needs the warps; the FP64 path keeps its
-// registers.
-template <class Acc>
+// Resident 256-thread CTAs per SM requested from the register allocator: the FP32 correlation and
+// final passes are latency-bound on frame loads and template gathers and need the warps (three
+// CTAs, 80 registers); the FP32 assembly, whose 14 packed sums spill at 80 registers, runs two CTAs
+// of up to 128 registers (assembly -5%, the correlation pass +41% when it ran two); the FP64 path
+// keeps its registers.
+template <class Acc, int MODE>
 struct MinBlocks {
   static constexpr int value = 2;
 };
 #ifndef SS_EVAL_MIN_BLOCKS
 #define SS_EVAL_MIN_BLOCKS 3
 #endif
-template <>
-struct MinBlocks<float> {
-  static constexpr int value = SS_EVAL_MIN_BLOCKS;
+#ifndef SS_ASM_MIN_BLOCKS
+#define SS_ASM_MIN_BLOCKS 2
+#endif
+template <int MODE>
+struct MinBlocks<float, MODE> {
+  static constexpr int value = MODE == 0 ? SS_ASM_MIN_BLOCKS : SS_EVAL_MIN_BLOCKS;
 };
 
 // Trial-round CTAs per SM (register bound) and the bytes of their template window; both must fit
@@ -688,7 +693,7 @@ __device__ __forceinline__ void eval_tile(const GroupDesc& G, const GroupCtl& C,
 // The evaluation passes over the tiles of the launch's schedule (ss_sched.cuh), one tile at a time
 // per CTA. Dynamic shared memory: the window's mbarrier (16 bytes), the column geometry, the window.
 template <class Acc, class FrameT, class TplT, int MODE>
-__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc>::value)
+__global__ void __launch_bounds__(32 * kEvalWarps, MinBlocks<Acc, MODE>::value)
     k_eval(const GroupDesc* __restrict__ gds, int* __restrict__ sched, int cap, const GroupCtl* __restrict__ ctl,
            int stage_rows, int win_bytes) {
   extern __shared__ __align__(16) unsigned char smem[];
