@@ -330,8 +330,19 @@ def ragged(args, device):
         ok64 = inner & (np.abs(ox - tx) <= 0.5) & (np.abs(oy - ty) <= 0.5)
         okS = inner & (np.abs(sx - tx) <= 0.5) & (np.abs(sy - ty) <= 0.5)
         ec = np.concatenate([(sx - ox)[ok64], (sy - oy)[ok64]])
+        # the frames the reference's caller keeps (steady_scan.m:246-284), from the FP64 run:
+        # correlation >= corr_thresh 0.75 and >= minblockfrac 0.25 of the blocks with a valid pixel
+        keep = (np.asarray(o["frame_corr"]) >= 0.75) & (np.asarray(o["blocks_used"]).mean(axis=0) >= 0.25)
+        ea = np.concatenate([(sx - ox)[:, keep].ravel(), (sy - oy)[:, keep].ravel()])
+        ea = ea[np.isfinite(ea)]
         cur = acc.setdefault(f"{h}x{w}", {"se": 0.0, "n": 0, "max": 0.0, "se_c": 0.0, "n_c": 0, "max_c": 0.0,
-                                          "knots": 0, "ok64": 0, "okS": 0})
+                                          "knots": 0, "ok64": 0, "okS": 0, "se_a": 0.0, "n_a": 0, "max_a": 0.0,
+                                          "frames": 0, "kept": 0})
+        cur["se_a"] += float(np.sum(ea * ea))
+        cur["n_a"] += ea.size
+        cur["max_a"] = max(cur["max_a"], float(np.max(np.abs(ea))) if ea.size else 0.0)
+        cur["frames"] += nf
+        cur["kept"] += int(keep.sum())
         cur["se"] += float(np.sum(e * e))
         cur["n"] += e.size
         cur["max"] = max(cur["max"], float(np.max(np.abs(e))))
@@ -344,7 +355,10 @@ def ragged(args, device):
     err = {k: {"rms_px": float(np.sqrt(v["se"] / v["n"])), "max_px": v["max"],
                "rms_px_where_fp64_within_0.5px_of_truth": float(np.sqrt(v["se_c"] / max(1, v["n_c"]))),
                "max_px_where_fp64_within_0.5px_of_truth": v["max_c"],
-               "knots_within_0.5px_of_truth": {"fp64": v["ok64"] / v["knots"], "S": v["okS"] / v["knots"]}}
+               "knots_within_0.5px_of_truth": {"fp64": v["ok64"] / v["knots"], "S": v["okS"] / v["knots"]},
+               "frames_kept_by_the_caller": f"{v['kept']} of {v['frames']}",
+               "rms_px_kept_frames": float(np.sqrt(v["se_a"] / max(1, v["n_a"]))),
+               "max_px_kept_frames": v["max_a"]}
            for k, v in acc.items()}
     iters = np.array([r["iter_used"] for r in res_t])
     choices = {k: v for k, v in tuner.choices.items()}

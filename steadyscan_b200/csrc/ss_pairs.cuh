@@ -72,6 +72,9 @@ struct PairLoad<double> {
 // fewer for wider frame types), assembly (whose 14 accumulators leave fewer registers).
 constexpr int kPrefetch = 8;
 constexpr int kPrefetchAsm = 2;
+// correlation and final passes: six 64-row steps in flight (17.2 -> 16.6 ms over two; four gained
+// nothing)
+constexpr int kPrefetchCorr = 6;
 
 // Per-warp constants of one block column for the pair loop.
 struct PairCol {
@@ -384,17 +387,17 @@ __device__ __forceinline__ void corr_pairs(const GroupDesc& G, size_t coli, cons
   bool run = true;
   float2 j = pc.j0;
   const float2 dj = f2(pc.dj);
-  typename PL::W ring[kPrefetchAsm];
+  typename PL::W ring[kPrefetchCorr];
 #pragma unroll
-  for (int d = 0; d < kPrefetchAsm; d++) ring[d] = d < steps ? PL::load(col, d * 32 + lane) : typename PL::W{};
+  for (int d = 0; d < kPrefetchCorr; d++) ring[d] = d < steps ? PL::load(col, d * 32 + lane) : typename PL::W{};
 #pragma unroll 1
-  for (int t0 = 0; t0 < steps; t0 += kPrefetchAsm) {
+  for (int t0 = 0; t0 < steps; t0 += kPrefetchCorr) {
 #pragma unroll
-    for (int d = 0; d < kPrefetchAsm; d++) {
+    for (int d = 0; d < kPrefetchCorr; d++) {
       const int t = t0 + d;
       if (t >= steps) break;
       const typename PL::W cur = ring[d];
-      if (t + kPrefetchAsm < steps) ring[d] = PL::load(col, (t + kPrefetchAsm) * 32 + lane);
+      if (t + kPrefetchCorr < steps) ring[d] = PL::load(col, (t + kPrefetchCorr) * 32 + lane);
       const float2 x = fma2(pc.bxj, j, pc.cx), y = fma2(pc.byj, j, pc.cy);
       j = add2(j, dj);
       const bool mA = in_range(x.x, twb) && in_range(y.x, thb);
