@@ -406,7 +406,14 @@ static int host_doubles(const ss_matrix& m, const char* name, std::vector<double
   if (dtype_size(m.dtype) == 0) return fail(SS_ERR_INVALID_ARGUMENT, std::string(name) + ": unknown dtype");
   size_t n = (size_t)(m.rows * m.cols);
   out.resize(n);
-  for (size_t i = 0; i < n; i++) out[i] = elem_as_double(m, i);
+  if (m.dtype == SS_F64) {  // one type test per matrix, not per element
+    if (n) std::memcpy(out.data(), m.data, n * sizeof(double));
+  } else if (m.dtype == SS_F32) {
+    const float* p = static_cast<const float*>(m.data);
+    for (size_t i = 0; i < n; i++) out[i] = (double)p[i];
+  } else {
+    for (size_t i = 0; i < n; i++) out[i] = elem_as_double(m, i);
+  }
   return SS_OK;
 }
 
@@ -480,6 +487,10 @@ struct HostGroup {
   double* d_sum = nullptr;
   double* d_p0 = nullptr;
   void* d_image = nullptr;
+  // streamed frames (Batch::set_stream_frames): the frames and their image sum in the batch's early
+  // buffer, uploaded while the host prepares the rest
+  void* early_image = nullptr;
+  double* early_sum = nullptr;
 };
 
 static void detect_affine_geometry(HostGroup& g);
@@ -521,6 +532,9 @@ static int validate_group(const ss_inputs* in, HostGroup& g) {
   if (!(g.frame_dt == SS_F64 || g.frame_dt == SS_F32 || g.frame_dt == SS_U16 || g.frame_dt == SS_F16))
     return fail(SS_ERR_INVALID_ARGUMENT, "bm_data dtype must be f64, f32, u16 or f16");
   if (!in->bm_data.data) return fail(SS_ERR_INVALID_ARGUMENT, "bm_data is NULL");
+  // known here, before the host inputs load: streamed uploads start right after validation
+  g.frame_bytes = (size_t)g.Hb * g.fW * dtype_size(g.frame_dt);
+  g.frames_dev = in->bm_data.location == SS_DEVICE ? in->bm_data.data : nullptr;
   if (in->est_dx_knots.rows * in->est_dx_knots.cols != (int64_t)(g.W + 1) * g.nF ||
       in->est_dy_knots.rows * in->est_dy_knots.cols != (int64_t)(g.W + 1) * g.nF)
     return fail(SS_ERR_INVALID_ARGUMENT, "est_dx_knots and est_dy_knots must hold (frameW + 1) x n_frames values");
@@ -633,8 +647,6 @@ static int load_host_inputs(std::vector<HostGroup>& all, size_t gi) {
     g.geo_k = s.geo_k; g.geo_L = s.geo_L;
     g.geo_ax = s.geo_ax; g.geo_bx = s.geo_bx; g.geo_ay = s.geo_ay; g.geo_by = s.geo_by; g.geo_fs = s.geo_fs;
   }
-  g.frame_bytes = (size_t)g.Hb * g.fW * dtype_size(g.frame_dt);
-  if (in->bm_data.location == SS_DEVICE) g.frames_dev = in->bm_data.data;
   return SS_OK;
 }
 
@@ -733,6 +745,7 @@ struct Batch::Impl {
   cudaStream_t up_stream = nullptr;
   cudaEvent_t ev_up = nullptr;
   int* d_ready = nullptr;
+  void* early = nullptr;  // streamed frames, their image sums, sum scratch and ready flags (pool)
   bool pool_arena = false;  // the arena comes from the library's memory pool
   // flag t: CUDA-event timing of the stages, summed into the reference's sub-function slots
   // (output 10, timedmainiteration.cpp:45-143 and task.cpp:293-356); the interval from a mark to the
@@ -806,6 +819,10 @@ Batch::~Batch() {
   if (d->cap_stream) cudaStreamDestroy(d->cap_stream);
   if (d->up_stream) {
     cudaStreamSynchronize(d->up_stream);
+    if (d->early) {
+      cudaFreeAsync(d->early, d->up_stream);
+      cudaStreamSynchronize(d->up_stream);
+    }
     cudaStreamDestroy(d->up_stream);
   }
   if (d->ev_up) cudaEventDestroy(d->ev_up);
@@ -840,7 +857,7 @@ static void layout(Batch::Impl* b, char* base) {
   b->d_counters = cv.take<int>(kCounters);
   b->d_staging = cv.take<unsigned long long>(kStagingCounters);
   b->d_sum_parts = cv.take<double>(kSumBlocks);
-  b->d_ready = b->stream_req ? cv.take<int>(std::max<size_t>(1, b->hg.size())) : nullptr;
+  if (!b->early) b->d_ready = b->stream_req ? cv.take<int>(std::max<size_t>(1, b->hg.size())) : nullptr;
   b->win_bytes = 0;
   b->ls_win_bytes = 0;
   for (size_t i = 0; i < b->hg.size(); i++) {
@@ -894,8 +911,8 @@ static void layout(Batch::Impl* b, char* base) {
     G.ls_rounds = b->compute == 1 ? 1 : 0;
     G.ls_max_trials = b->d_counters;
     G.staging = b->d_staging;
-    g.d_image = g.frames_dev ? nullptr : cv.take<char>(g.frame_bytes);
-    G.image = g.frames_dev ? g.frames_dev : g.d_image;
+    g.d_image = (g.frames_dev || g.early_image) ? nullptr : cv.take<char>(g.frame_bytes);
+    G.image = g.frames_dev ? g.frames_dev : (g.early_image ? g.early_image : g.d_image);
     {
       const size_t fsz = dtype_size(g.frame_dt);
       G.pair_ok = (b->compute == 1 && g.geo_k > 0 && g.Hb % 64 == 0 &&
@@ -925,7 +942,7 @@ static void layout(Batch::Impl* b, char* base) {
       }
     }
     if (G.tplain) b->win_bytes = kWinBytes;  // the line search runs from the global template
-    g.d_sum = cv.take<double>(1);
+    g.d_sum = g.early_sum ? g.early_sum : cv.take<double>(1);
     G.sum_image = g.d_sum;
     g.d_p0 = cv.take<double>(2 * N);
     G.p = cv.take<double>(2 * N);
@@ -983,6 +1000,59 @@ static void layout(Batch::Impl* b, char* base) {
   b->arena_bytes = cv.off + 256;
 }
 
+__global__ void k_set_flag(int* __restrict__ flag) { *flag = 1; }
+
+// Streamed frames: as soon as the groups are validated, one pool allocation on the upload stream
+// holds every host-resident group's frames (256-byte aligned), their image sums, the sums' scratch
+// and the ready flags; the upload stream then copies each group's frames, sums them and sets its
+// flag, in group order, while the host prepares the rest of the batch. Groups whose frames are on
+// the device only get their flag. ev_up, recorded right after the allocation, orders the buffer
+// before the batch stream's work.
+static int start_frame_uploads(Batch::Impl* b, int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SS_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(SS_ERR_INVALID_ARGUMENT, "gpu_device_id out of range");
+  SS_CK(cudaSetDevice(device));
+  SumFn sum = pick_sum(b->hg[0].frame_dt);
+  if (!sum) return fail(SS_ERR_INVALID_ARGUMENT, "unsupported frame dtype");
+  const size_t n = b->hg.size();
+  auto up = [](size_t v) { return (v + 255) & ~size_t(255); };
+  size_t bytes = up(n * sizeof(int)) + up(kSumBlocks * sizeof(double)) + up(n * sizeof(double));
+  for (const HostGroup& g : b->hg) {
+    if (g.frame_bytes == 0 || g.frame_bytes != (size_t)g.Hb * g.fW * dtype_size(g.frame_dt))
+      return fail(SS_ERR_INVALID_ARGUMENT, "streamed frames: group not validated");
+    if (!g.frames_dev) bytes += up(g.frame_bytes);
+  }
+  SS_CK(cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking));
+  SS_CK(cudaEventCreateWithFlags(&b->ev_up, cudaEventDisableTiming));
+  cudaMemPool_t pool = work_pool(device);
+  if (!pool) return fail(SS_ERR_OUT_OF_MEMORY, "no device memory pool");
+  if (cudaMallocFromPoolAsync(&b->early, bytes, pool, b->up_stream) != cudaSuccess)
+    return fail(SS_ERR_OUT_OF_MEMORY, "device memory for the streamed frames");
+  SS_CK(cudaEventRecord(b->ev_up, b->up_stream));
+  char* p = static_cast<char*>(b->early);
+  b->d_ready = reinterpret_cast<int*>(p);
+  p += up(n * sizeof(int));
+  double* parts = reinterpret_cast<double*>(p);
+  p += up(kSumBlocks * sizeof(double));
+  double* sums = reinterpret_cast<double*>(p);
+  p += up(n * sizeof(double));
+  SS_CK(cudaMemsetAsync(b->d_ready, 0, n * sizeof(int), b->up_stream));
+  for (size_t i = 0; i < n; i++) {
+    HostGroup& g = b->hg[i];
+    if (!g.frames_dev) {
+      g.early_image = p;
+      g.early_sum = sums + i;
+      p += up(g.frame_bytes);
+      SS_CK(cudaMemcpyAsync(g.early_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, b->up_stream));
+      sum(g.early_image, (size_t)g.Hb * g.fW, parts, g.early_sum, b->up_stream);
+    }
+    k_set_flag<<<1, 1, 0, b->up_stream>>>(b->d_ready + i);
+  }
+  SS_CK(cudaGetLastError());
+  return SS_OK;
+}
+
 int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
                    const Batch* const* sessions, bool measure_only, void* borrow_stream) {
   Impl* b = d;
@@ -1014,6 +1084,10 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
         return fail(SS_ERR_INVALID_ARGUMENT, "all groups of a batch need the same precision, frame dtype and device");
     }
   }
+  if (b->stream_req && !measure_only) {  // the frames travel while the host prepares the rest
+    int rc = start_frame_uploads(b, in[0].gpu_device_id);
+    if (rc) return rc;
+  }
   find_shared_inputs(b->hg);
   for (int i = 0; i < n; i++) {
     int rc = load_host_inputs(b->hg, i);
@@ -1043,6 +1117,9 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     SS_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     b->own_stream = true;
   }
+  // the early buffer was allocated on the upload stream: order it before this stream's work (the
+  // event precedes the uploads, which the ready flags order)
+  if (b->early) SS_CK(cudaStreamWaitEvent(b->stream, b->ev_up, 0));
   layout(b, nullptr);
   if (external) {
     if (external_bytes < b->arena_bytes) return fail(SS_ERR_OUT_OF_MEMORY, "external arena too small");
@@ -1096,7 +1173,7 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
         SS_CK(cudaMemcpyAsync((void*)G.col_yrange, g.yrange.data(), g.yrange.size() * 4, cudaMemcpyHostToDevice, s));
       }
     }
-    const bool streamed = b->stream_req && !g.frames_dev;  // uploaded by start() on the upload stream
+    const bool streamed = g.early_image != nullptr;  // uploaded by start_frame_uploads
     if (!g.frames_dev && !streamed)
       SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
     SS_CK(cudaMemcpyAsync(g.d_p0, g.p0.data(), g.p0.size() * 8, cudaMemcpyHostToDevice, s));
@@ -1237,7 +1314,6 @@ __global__ void __launch_bounds__(1024) k_join(GroupCtl* __restrict__ ctl, const
   }
 }
 
-__global__ void k_set_flag(int* __restrict__ flag) { *flag = 1; }
 
 // Enqueues one cycle of every group's state machine on the batch stream (assembly, solve, trial
 // rounds or the cluster line search, correlation, iteration end, final pass) and the copy of the
@@ -1476,25 +1552,6 @@ int Batch::start() {
   SS_CK(smem_attr(k_solve_system, (int)kSolveSmem));
   int rc = reset_state(b);
   if (rc) return rc;
-  if (b->d_ready) {  // streamed frames: upload, image sum and ready flag per group, in group order
-    cudaStream_t s = b->stream;
-    if (!b->up_stream) SS_CK(cudaStreamCreateWithFlags(&b->up_stream, cudaStreamNonBlocking));
-    if (!b->ev_up) SS_CK(cudaEventCreateWithFlags(&b->ev_up, cudaEventDisableTiming));
-    SS_CK(cudaMemsetAsync(b->d_ready, 0, b->hg.size() * sizeof(int), s));
-    SS_CK(cudaEventRecord(b->ev_up, s));
-    SS_CK(cudaStreamWaitEvent(b->up_stream, b->ev_up, 0));
-    for (size_t i = 0; i < b->hg.size(); i++) {
-      const HostGroup& g = b->hg[i];
-      if (g.frames_dev) {
-        k_set_flag<<<1, 1, 0, b->up_stream>>>(b->d_ready + i);
-        continue;
-      }
-      SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, b->up_stream));
-      b->sum(b->gd[i].image, (size_t)g.Hb * g.fW, b->d_sum_parts, g.d_sum, b->up_stream);
-      k_set_flag<<<1, 1, 0, b->up_stream>>>(b->d_ready + i);
-    }
-    SS_CK(cudaGetLastError());
-  }
   b->cycles = 0;
   b->rounds = 0;
   b->launches = 0;
