@@ -33,7 +33,9 @@ constexpr int kEvalWarps = 8;       // warps per assembly/final CTA
 constexpr int kLsCluster = 8;       // CTAs per frame in the line-search cluster
 constexpr int kLsMaxKnots = 256;    // knots per cluster CTA: frame_w <= kLsCluster * kLsMaxKnots
 constexpr int kMaxFrameW = kLsCluster * kLsMaxKnots;
-constexpr int kMinWinFrames = 4;    // frames of a tile worth staging a template window for
+// frames of a tile worth staging a template window for (2: trial rounds 61.96 -> 61.57 ms against
+// 4; 8 cost 1%)
+constexpr int kMinWinFrames = 2;
 
 // Resident 256-thread CTAs per SM requested from the register allocator: the FP32 correlation and
 // final passes are latency-bound on frame loads and template gathers and need the warps (three

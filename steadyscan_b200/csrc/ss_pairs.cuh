@@ -72,9 +72,13 @@ struct PairLoad<double> {
 // fewer for wider frame types), assembly (whose 14 accumulators leave fewer registers).
 constexpr int kPrefetch = 8;
 constexpr int kPrefetchAsm = 2;
-// correlation and final passes: six 64-row steps in flight (17.2 -> 16.6 ms over two; four gained
-// nothing)
-constexpr int kPrefetchCorr = 6;
+// Correlation and final passes: 64-row steps of frame samples in flight, by the width of a lane's
+// sample word (16-bit pairs: 16 steps, a whole 1024-row column; the pass took 17.2 ms with 2, 16.5
+// with 6, 15.7 with 8 and 14.3 with 16 steps over the 2000-frame run).
+template <class W>
+struct CorrPrefetch {
+  static constexpr int value = sizeof(W) <= 4 ? 16 : (sizeof(W) <= 8 ? 8 : 4);
+};
 
 // Per-warp constants of one block column for the pair loop.
 struct PairCol {
@@ -376,6 +380,7 @@ template <class FrameT, int MODE>
 __device__ __forceinline__ void corr_pairs(const GroupDesc& G, size_t coli, const PairCol& pc, const PairWin& w,
                                            double (&out)[kCsStride], int& cnt_out, uint8_t* mask_out) {
   using PL = PairLoad<FrameT>;
+  constexpr int kPrefetchCorr = CorrPrefetch<typename PL::W>::value;
   const int lane = threadIdx.x & 31;
   const unsigned twb = __float_as_uint(Limits<float>::lim(G.Wt)), thb = __float_as_uint(Limits<float>::lim(G.Ht));
   const FrameT* col = reinterpret_cast<const FrameT*>(G.image) + coli;
