@@ -417,6 +417,30 @@ static int host_doubles(const ss_matrix& m, const char* name, std::vector<double
   return SS_OK;
 }
 
+// A host matrix read as doubles: the caller's own array when it holds doubles (no copy), else a
+// converted copy. It is read only while the batch prepares, when the call's inputs are valid.
+struct HostDoubles {
+  const double* ext = nullptr;
+  std::vector<double> own;
+  size_t n = 0;
+  const double* data() const { return ext ? ext : own.data(); }
+  size_t size() const { return n; }
+};
+
+static int host_doubles(const ss_matrix& m, const char* name, HostDoubles& out) {
+  out.ext = nullptr;
+  out.own.clear();
+  out.n = 0;
+  if (m.location == SS_HOST && m.dtype == SS_F64 && m.data) {
+    out.ext = static_cast<const double*>(m.data);
+    out.n = (size_t)(m.rows * m.cols);
+    return SS_OK;
+  }
+  int rc = host_doubles(m, name, out.own);
+  out.n = out.own.size();
+  return rc;
+}
+
 static int parse_flags(const char* flags, int& compute, int& bits) {
   if (!flags) return fail(SS_ERR_INVALID_ARGUMENT, "flags is NULL");
   compute = -1;
@@ -466,7 +490,7 @@ struct HostGroup {
   int Hb = 0, W = 0, nF = 0, fW = 0, N = 0, Ht = 0, Wt = 0, group_size = 0, n_rg = 0;
   int frame_dt = SS_F64, tpl_dt = SS_F64;
   bool grad_derived = true, frac_uniform = true;
-  std::vector<double> p0, templ, xg, yg, frac, bx, by;
+  HostDoubles templ, xg, yg, frac, bx, by, ex, ey;  // ex, ey: the initial knots
   std::vector<float> frac_f, bx_f, by_f;  // precision 'S' geometry
   std::vector<float> yrange;              // per block column [min, max] of basey over valid rows
   int frames_per_cta = 32;
@@ -588,58 +612,47 @@ static int load_host_inputs(std::vector<HostGroup>& all, size_t gi) {
     if ((rc = host_doubles(in->xgrad, "xgrad", g.xg))) return rc;
     if ((rc = host_doubles(in->ygrad, "ygrad", g.yg))) return rc;
   }
-  std::vector<double> tmp;
+  HostDoubles tmp;
   if (g.geo_src == -1) {
     if ((rc = host_doubles(in->tfrac, "tfrac", g.frac))) return rc;
     if ((rc = host_doubles(in->basex, "basex", g.bx))) return rc;
     if ((rc = host_doubles(in->basey, "basey", g.by))) return rc;
     if ((rc = host_doubles(in->base_mask, "base_mask", tmp))) return rc;
     g.bmask.resize(tmp.size());
-    for (size_t i = 0; i < tmp.size(); i++) g.bmask[i] = tmp[i] != 0.0;
+    const double* mk = tmp.data();
+    for (size_t i = 0; i < tmp.size(); i++) g.bmask[i] = mk[i] != 0.0;
     if ((rc = host_doubles(in->min_points_per_block, "min_points_per_block", tmp))) return rc;
     g.minp.resize(g.W);
-    for (int i = 0; i < g.W; i++) g.minp[i] = (int32_t)tmp[i];  // static_cast<int> (mexconverter.cpp:97)
+    const double* mp = tmp.data();
+    for (int i = 0; i < g.W; i++) g.minp[i] = (int32_t)mp[i];  // static_cast<int> (mexconverter.cpp:97)
   }
-  std::vector<double> ex, ey;
-  if ((rc = host_doubles(in->est_dx_knots, "est_dx_knots", ex))) return rc;
-  if ((rc = host_doubles(in->est_dy_knots, "est_dy_knots", ey))) return rc;
-  // ParameterOrganizer::organize2D1 (parameterorganizer.cpp:31-55)
-  g.p0.assign(2 * (size_t)g.N, 0.0);
-  for (int f = 0; f < g.nF; f++) {
-    int j = f * g.W + (f != 0);
-    for (int i = (f != 0); i < g.W; i++, j++) {
-      g.p0[j] = ex[(size_t)f * (g.W + 1) + i];
-      g.p0[j + g.N] = ey[(size_t)f * (g.W + 1) + i];
-    }
-    if (f < g.nF - 1) {
-      g.p0[j] = (ex[(size_t)f * (g.W + 1) + g.W] + ex[(size_t)(f + 1) * (g.W + 1)]) / 2;
-      g.p0[j + g.N] = (ey[(size_t)f * (g.W + 1) + g.W] + ey[(size_t)(f + 1) * (g.W + 1)]) / 2;
-    } else {
-      g.p0[j] = ex[(size_t)f * (g.W + 1) + g.W];
-      g.p0[j + g.N] = ey[(size_t)f * (g.W + 1) + g.W];
-    }
-  }
+  if ((rc = host_doubles(in->est_dx_knots, "est_dx_knots", g.ex))) return rc;
+  if ((rc = host_doubles(in->est_dy_knots, "est_dy_knots", g.ey))) return rc;
   if (g.tpl_src == -1) {
     // gradients that are exactly the template's forward differences are re-derived on the device
+    const double* T = g.templ.data();
+    const double* X = g.xg.data();
+    const double* Y = g.yg.data();
     g.grad_derived = true;
     for (int c = 0; c + 1 < g.Wt && g.grad_derived; c++)
       for (int r = 0; r < g.Ht; r++) {
-        double d = g.templ[(size_t)(c + 1) * g.Ht + r] - g.templ[(size_t)c * g.Ht + r];
-        if (!(g.xg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
+        double d = T[(size_t)(c + 1) * g.Ht + r] - T[(size_t)c * g.Ht + r];
+        if (!(X[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
       }
     for (int c = 0; c < g.Wt && g.grad_derived; c++)
       for (int r = 0; r + 1 < g.Ht; r++) {
-        double d = g.templ[(size_t)c * g.Ht + r + 1] - g.templ[(size_t)c * g.Ht + r];
-        if (!(g.yg[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
+        double d = T[(size_t)c * g.Ht + r + 1] - T[(size_t)c * g.Ht + r];
+        if (!(Y[(size_t)c * g.Ht + r] == d)) { g.grad_derived = false; break; }
       }
   } else {
     g.grad_derived = g.tpl_src == kFromSession ? g.ses_hg->grad_derived : all[g.tpl_src].grad_derived;
   }
   if (g.geo_src == -1) {
     g.frac_uniform = true;
+    const double* F = g.frac.data();
     for (int c = 1; c < g.W && g.frac_uniform; c++)
       for (int r = 0; r < g.Hb; r++)
-        if (std::memcmp(&g.frac[(size_t)c * g.Hb + r], &g.frac[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
+        if (std::memcmp(&F[(size_t)c * g.Hb + r], &F[r], sizeof(double)) != 0) { g.frac_uniform = false; break; }
     if (g.compute == 1 && g.frac_uniform) detect_affine_geometry(g);
   } else {
     const HostGroup& s = g.geo_src == kFromSession ? *g.ses_hg : all[g.geo_src];
@@ -662,20 +675,27 @@ static void detect_affine_geometry(HostGroup& g) {
     const int L = Hb / k;
     if (L < 2 || (k > 1 && W < 1)) continue;
     const double fs = 1.0 / ((double)k * L);
-    const double bx0 = g.bx[0], ax = g.bx[k] - g.bx[0];
-    const double by0 = g.by[0];
-    const double ay = (k > 1) ? g.by[1] - g.by[0] : (W > 1 ? g.by[Hb] - g.by[0] : 1.0);
+    const double* BX = g.bx.data();
+    const double* BY = g.by.data();
+    const double* FR = g.frac.data();
+    const uint8_t* MK = g.bmask.data();
+    const double bx0 = BX[0], ax = BX[k] - BX[0];
+    const double by0 = BY[0];
+    const double ay = (k > 1) ? BY[1] - BY[0] : (W > 1 ? BY[Hb] - BY[0] : 1.0);
+    auto near = [](double a, double b) { return std::fabs(a - b) <= 1e-9 * std::max(1.0, std::fabs(b)); };
     bool ok = true;
+    // block row r = j * k + l: pixel j of line cc * k + l
     for (int cc = 0; cc < W && ok; cc++)
-      for (int r = 0; r < Hb; r++) {
-        const int l = r % k, j = r / k;
-        const size_t i = (size_t)cc * Hb + r;
-        const double f = ((double)l * L + j + 0.5) * fs;
-        const double x = ax * j + bx0, y = ay * ((double)cc * k + l) + by0;
-        auto near = [](double a, double b) { return std::fabs(a - b) <= 1e-9 * std::max(1.0, std::fabs(b)); };
-        if (!g.bmask[i] || !near(f, g.frac[i]) || !near(x, g.bx[i]) || !near(y, g.by[i])) {
-          ok = false;
-          break;
+      for (int j = 0; j < L && ok; j++) {
+        const double x = ax * j + bx0;
+        for (int l = 0; l < k; l++) {
+          const size_t i = (size_t)cc * Hb + (size_t)j * k + l;
+          const double f = ((double)l * L + j + 0.5) * fs;
+          const double y = ay * ((double)cc * k + l) + by0;
+          if (!MK[i] || !near(f, FR[i]) || !near(x, BX[i]) || !near(y, BY[i])) {
+            ok = false;
+            break;
+          }
         }
       }
     if (ok) {
@@ -1053,6 +1073,90 @@ static int start_frame_uploads(Batch::Impl* b, int device) {
   return SS_OK;
 }
 
+// ParameterOrganizer::organize2D1 (parameterorganizer.cpp:31-55): the initial knots of every frame
+// as the group's parameter vector (x then y; a frame's last knot and the next frame's first become
+// one parameter at their mean).
+static void organize_p0(const HostGroup& g, double* p0) {
+  const double* ex = g.ex.data();
+  const double* ey = g.ey.data();
+  std::memset(p0, 0, 2 * (size_t)g.N * sizeof(double));
+  for (int f = 0; f < g.nF; f++) {
+    int j = f * g.W + (f != 0);
+    for (int i = (f != 0); i < g.W; i++, j++) {
+      p0[j] = ex[(size_t)f * (g.W + 1) + i];
+      p0[j + g.N] = ey[(size_t)f * (g.W + 1) + i];
+    }
+    if (f < g.nF - 1) {
+      p0[j] = (ex[(size_t)f * (g.W + 1) + g.W] + ex[(size_t)(f + 1) * (g.W + 1)]) / 2;
+      p0[j + g.N] = (ey[(size_t)f * (g.W + 1) + g.W] + ey[(size_t)(f + 1) * (g.W + 1)]) / 2;
+    } else {
+      p0[j] = ex[(size_t)f * (g.W + 1) + g.W];
+      p0[j + g.N] = ey[(size_t)f * (g.W + 1) + g.W];
+    }
+  }
+}
+
+// Page-locked host staging for a batch's small uploads (geometry, template, initial knots,
+// descriptors): one buffer per process, held by one batch at a time from its first staged copy
+// until the batch's stream has drained, so those copies run as DMA from page-locked memory rather
+// than through the driver's pageable path (which stalls behind streamed frame uploads). A copy
+// that does not fit goes the pageable way; the buffer then grows to the batch's total for the
+// next batch. A batch on a borrowed stream, which does not drain it, copies the pageable way.
+static std::mutex g_stage_mu;
+static char* g_stage = nullptr;
+static size_t g_stage_cap = 0;
+
+struct Staging {
+  std::unique_lock<std::mutex> lock;
+  cudaStream_t stream = nullptr;
+  size_t off = 0, want = 0;
+  bool on = false;
+  explicit Staging(cudaStream_t s, bool enable) : stream(s), on(enable) {
+    if (on) lock = std::unique_lock<std::mutex>(g_stage_mu);
+  }
+  // staging space for n bytes (16-byte aligned), or null when it does not fit
+  void* take(size_t n) {
+    if (!on) return nullptr;
+    const size_t m = (n + 15) & ~size_t(15);
+    want += m;
+    if (off + m > g_stage_cap) return nullptr;
+    void* p = g_stage + off;
+    off += m;
+    return p;
+  }
+  // host-to-device copy of n bytes through the staging buffer when it has room
+  cudaError_t put(void* dst, const void* src, size_t n) {
+    if (!n) return cudaSuccess;
+    void* p = take(n);
+    if (p) {
+      std::memcpy(p, src, n);
+      src = p;
+    }
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, stream);
+  }
+  // after the stream has drained: grows the buffer when the batch wanted more
+  void release() {
+    if (!on) return;
+    if (want > g_stage_cap) {
+      if (g_stage) cudaFreeHost(g_stage);
+      g_stage = nullptr;
+      g_stage_cap = 0;
+      const size_t cap = want + want / 4;
+      if (cudaHostAlloc((void**)&g_stage, cap, cudaHostAllocPortable) == cudaSuccess) g_stage_cap = cap;
+      else g_stage = nullptr;
+      cudaGetLastError();  // a failed allocation leaves the pageable path; clear its error
+    }
+    on = false;
+    lock.unlock();
+  }
+  ~Staging() {
+    if (!on) return;
+    cudaStreamSynchronize(stream);  // an early return: no copy may still read the buffer
+    on = false;
+    lock.unlock();
+  }
+};
+
 int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, size_t external_bytes,
                    const Batch* const* sessions, bool measure_only, void* borrow_stream) {
   Impl* b = d;
@@ -1138,50 +1242,68 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
 
   // uploads
   cudaStream_t s = b->stream;
+  Staging stg(s, b->own_stream);
   std::vector<int> chunk_group(std::max(1, b->n_chunks)), frame_group(std::max(1, b->n_frames_total));
   for (size_t i = 0; i < b->hg.size(); i++) {
     HostGroup& g = b->hg[i];
     GroupDesc& G = b->gd[i];
     const size_t hbw = (size_t)g.Hb * g.W;
     if (g.geo_src == -1) {
-      SS_CK(cudaMemcpyAsync((void*)G.frac, g.frac.data(), hbw * 8, cudaMemcpyHostToDevice, s));
-      SS_CK(cudaMemcpyAsync((void*)G.basex, g.bx.data(), hbw * 8, cudaMemcpyHostToDevice, s));
-      SS_CK(cudaMemcpyAsync((void*)G.basey, g.by.data(), hbw * 8, cudaMemcpyHostToDevice, s));
-      if (b->compute == 1) {
-        g.frac_f.assign(g.frac.begin(), g.frac.end());
-        g.bx_f.assign(g.bx.begin(), g.bx.end());
-        g.by_f.assign(g.by.begin(), g.by.end());
-        SS_CK(cudaMemcpyAsync((void*)G.frac_f, g.frac_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
-        SS_CK(cudaMemcpyAsync((void*)G.basex_f, g.bx_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
-        SS_CK(cudaMemcpyAsync((void*)G.basey_f, g.by_f.data(), hbw * 4, cudaMemcpyHostToDevice, s));
+      SS_CK(stg.put((void*)G.frac, g.frac.data(), hbw * 8));
+      SS_CK(stg.put((void*)G.basex, g.bx.data(), hbw * 8));
+      SS_CK(stg.put((void*)G.basey, g.by.data(), hbw * 8));
+      if (b->compute == 1) {  // precision 'S' geometry, converted straight into the staging buffer
+        const double* src[3] = {g.frac.data(), g.bx.data(), g.by.data()};
+        const float* dst[3] = {G.frac_f, G.basex_f, G.basey_f};
+        std::vector<float>* keep[3] = {&g.frac_f, &g.bx_f, &g.by_f};
+        for (int a = 0; a < 3; a++) {
+          float* h = static_cast<float*>(stg.take(hbw * 4));
+          if (!h) {
+            keep[a]->resize(hbw);
+            h = keep[a]->data();
+          }
+          for (size_t e = 0; e < hbw; e++) h[e] = (float)src[a][e];
+          SS_CK(cudaMemcpyAsync((void*)dst[a], h, hbw * 4, cudaMemcpyHostToDevice, s));
+        }
       }
-      SS_CK(cudaMemcpyAsync((void*)G.base_mask, g.bmask.data(), hbw, cudaMemcpyHostToDevice, s));
-      SS_CK(cudaMemcpyAsync((void*)G.min_points, g.minp.data(), g.W * 4, cudaMemcpyHostToDevice, s));
+      SS_CK(stg.put((void*)G.base_mask, g.bmask.data(), hbw));
+      SS_CK(stg.put((void*)G.min_points, g.minp.data(), g.W * 4));
       if (G.col_yrange) {  // [min, max] of basey over the valid rows of each block column
+        const double* BY = g.by.data();
         g.yrange.assign(2 * (size_t)g.W, 0.0f);
         for (int c = 0; c < g.W; c++) {
           double lo = INFINITY, hi = -INFINITY;
           for (int r = 0; r < g.Hb; r++) {
             const size_t i = (size_t)c * g.Hb + r;
             if (!g.bmask[i]) continue;
-            lo = std::min(lo, g.by[i]);
-            hi = std::max(hi, g.by[i]);
+            lo = std::min(lo, BY[i]);
+            hi = std::max(hi, BY[i]);
           }
           g.yrange[2 * c] = (float)lo;
           g.yrange[2 * c + 1] = (float)hi;
         }
-        SS_CK(cudaMemcpyAsync((void*)G.col_yrange, g.yrange.data(), g.yrange.size() * 4, cudaMemcpyHostToDevice, s));
+        SS_CK(stg.put((void*)G.col_yrange, g.yrange.data(), g.yrange.size() * 4));
       }
     }
     const bool streamed = g.early_image != nullptr;  // uploaded by start_frame_uploads
     if (!g.frames_dev && !streamed)
       SS_CK(cudaMemcpyAsync(g.d_image, g.in->bm_data.data, g.frame_bytes, cudaMemcpyHostToDevice, s));
-    SS_CK(cudaMemcpyAsync(g.d_p0, g.p0.data(), g.p0.size() * 8, cudaMemcpyHostToDevice, s));
+    {  // the initial parameter vector, organised straight into the staging buffer
+      const size_t np = 2 * (size_t)g.N;
+      double* h = static_cast<double*>(stg.take(np * 8));
+      std::vector<double> p0;
+      if (!h) {
+        p0.resize(np);
+        h = p0.data();
+      }
+      organize_p0(g, h);
+      SS_CK(cudaMemcpyAsync(g.d_p0, h, np * 8, cudaMemcpyHostToDevice, s));
+    }
     if (g.tpl_src == -1) {
-      SS_CK(cudaMemcpyAsync(g.d_templ_stage, g.templ.data(), g.templ.size() * 8, cudaMemcpyHostToDevice, s));
+      SS_CK(stg.put(g.d_templ_stage, g.templ.data(), g.templ.size() * 8));
       if (!g.grad_derived) {
-        SS_CK(cudaMemcpyAsync(g.d_xg_stage, g.xg.data(), g.xg.size() * 8, cudaMemcpyHostToDevice, s));
-        SS_CK(cudaMemcpyAsync(g.d_yg_stage, g.yg.data(), g.yg.size() * 8, cudaMemcpyHostToDevice, s));
+        SS_CK(stg.put(g.d_xg_stage, g.xg.data(), g.xg.size() * 8));
+        SS_CK(stg.put(g.d_yg_stage, g.yg.data(), g.yg.size() * 8));
       }
     }
     const int nb = 148 * 4;
@@ -1208,11 +1330,13 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
     for (int t = 0; t < nchunks; t++) chunk_group[G.chunk_base + t] = (int)i;
     for (int f = 0; f < g.nF; f++) frame_group[G.frame_base + f] = (int)i;
   }
-  SS_CK(cudaMemcpyAsync(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice, s));
-  SS_CK(cudaMemcpyAsync(b->d_chunk_group, chunk_group.data(), chunk_group.size() * 4, cudaMemcpyHostToDevice, s));
-  SS_CK(cudaMemcpyAsync(b->d_frame_group, frame_group.data(), frame_group.size() * 4, cudaMemcpyHostToDevice, s));
-  // pageable sources are staged before the copies return; an own stream is also drained
+  SS_CK(stg.put(b->d_gd, b->gd.data(), b->gd.size() * sizeof(GroupDesc)));
+  SS_CK(stg.put(b->d_chunk_group, chunk_group.data(), chunk_group.size() * 4));
+  SS_CK(stg.put(b->d_frame_group, frame_group.data(), frame_group.size() * 4));
+  // pageable sources are staged before the copies return; an own stream is also drained, after
+  // which the staging buffer is free for the next batch
   if (b->own_stream) SS_CK(cudaStreamSynchronize(s));
+  stg.release();
   return SS_OK;
 }
 
