@@ -157,6 +157,7 @@ struct GroupDesc {
   double* o_iter_times;     // flags T and t: max_iter seconds
   uint8_t* o_mask;          // Hb x fW column-major, may be null
   uint8_t* o_blocks_used;   // fW: block column has a valid pixel in the final mask, may be null
+  const double* p0;         // 2N: the initial parameter vector, copied into p when a run starts
 };
 
 // ---------------------------------------------------------------------------------------------

@@ -134,6 +134,42 @@ __global__ void k_fill(double* p, size_t n, double v) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
 
+// The per-group state reset at the start of a run (task_allocate.cu:201-255) as one launch:
+// blockIdx.y is the group, the CTAs of a row stride over its buffers. The knot buffers start as
+// NaN (an all-invalid mask and a zero difference image until the first knots are written), no
+// column keeps assembly sums of an earlier run, and the errvals start at the reference's fill.
+__global__ void k_reset_groups(const GroupDesc* __restrict__ gd) {
+  const GroupDesc& G = gd[blockIdx.y];
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, st = (size_t)gridDim.x * blockDim.x;
+  const size_t N = G.N, nF = G.nF, mi = G.max_iter, nrg2 = 2 * (size_t)G.n_rg;
+  const size_t nk = nF * 2 * (size_t)(G.W + 1), na = (size_t)G.fW * 8;
+  for (size_t i = t0; i < 2 * N; i += st) {
+    G.p[i] = G.p0[i];
+    G.p_last[i] = 0.0;
+    G.delta_p[i] = 0.0;
+  }
+  for (size_t i = t0; i < N; i += st) {
+    G.params_used[i] = 0;
+    G.blocks_present[i] = 0;
+    G.eig_valid[i] = 0;
+  }
+  for (size_t i = t0; i <= nrg2; i += st) G.grp_active[i] = i < nrg2 ? 1 : 0;
+  for (size_t i = t0; i < nF; i += st) {
+    G.o_frame_corr[i] = 0.0;
+    G.ls_done[i] = 0;
+  }
+  for (size_t i = t0; i < 2 * nF; i += st) G.errval[i] = kErrvalFill;
+  for (size_t i = t0; i < nk; i += st) {
+    G.kmask[i] = NAN;
+    G.kdiff[i] = NAN;
+  }
+  for (size_t i = t0; i < na; i += st) G.asmk[i] = NAN;
+  if (G.o_rg_params)
+    for (size_t i = t0; i < 4 * N * mi; i += st) G.o_rg_params[i] = 0.0;
+  if (G.o_iter_times)
+    for (size_t i = t0; i < mi; i += st) G.o_iter_times[i] = 0.0;
+}
+
 // ---------------------------------------------------------------------------------------------
 // kernel dispatch by (compute, frame type, template type)
 
@@ -965,6 +1001,7 @@ static void layout(Batch::Impl* b, char* base) {
     g.d_sum = g.early_sum ? g.early_sum : cv.take<double>(1);
     G.sum_image = g.d_sum;
     g.d_p0 = cv.take<double>(2 * N);
+    G.p0 = g.d_p0;
     G.p = cv.take<double>(2 * N);
     G.p_last = cv.take<double>(2 * N);
     G.p_snap = cv.take<double>(2 * N);
@@ -1105,6 +1142,8 @@ static void organize_p0(const HostGroup& g, double* p0) {
 static std::mutex g_stage_mu;
 static char* g_stage = nullptr;
 static size_t g_stage_cap = 0;
+constexpr size_t kStageItemMax = size_t(16) << 20;  // larger copies (frames, masks) go direct
+constexpr size_t kStageMax = size_t(128) << 20;
 
 struct Staging {
   std::unique_lock<std::mutex> lock;
@@ -1116,7 +1155,7 @@ struct Staging {
   }
   // staging space for n bytes (16-byte aligned), or null when it does not fit
   void* take(size_t n) {
-    if (!on) return nullptr;
+    if (!on || n > kStageItemMax) return nullptr;
     const size_t m = (n + 15) & ~size_t(15);
     want += m;
     if (off + m > g_stage_cap) return nullptr;
@@ -1137,11 +1176,11 @@ struct Staging {
   // after the stream has drained: grows the buffer when the batch wanted more
   void release() {
     if (!on) return;
-    if (want > g_stage_cap) {
+    if (want > g_stage_cap && g_stage_cap < kStageMax) {
       if (g_stage) cudaFreeHost(g_stage);
       g_stage = nullptr;
       g_stage_cap = 0;
-      const size_t cap = want + want / 4;
+      const size_t cap = std::min(want + want / 4, kStageMax);
       if (cudaHostAlloc((void**)&g_stage, cap, cudaHostAllocPortable) == cudaSuccess) g_stage_cap = cap;
       else g_stage = nullptr;
       cudaGetLastError();  // a failed allocation leaves the pageable path; clear its error
@@ -1344,29 +1383,13 @@ int Batch::prepare(int n, const ss_inputs* in, ss_outputs* out, void* external, 
 static int reset_state(Batch::Impl* b) {
   cudaStream_t s = b->stream;
   b->h_ctl.assign(b->gd.size(), GroupCtl{});
+  // the device buffers of every group (d_gd is on the device since the batch was prepared)
+  const int nG = (int)b->gd.size();
+  for (int g0 = 0; g0 < nG; g0 += 65535)
+    k_reset_groups<<<dim3(16, std::min(nG - g0, 65535)), 256, 0, s>>>(b->d_gd + g0);
+  SS_CK(cudaGetLastError());
   for (size_t i = 0; i < b->gd.size(); i++) {
     const HostGroup& g = b->hg[i];
-    const GroupDesc& G = b->gd[i];
-    const size_t N = g.N, nF = g.nF;
-    SS_CK(cudaMemcpyAsync(G.p, g.d_p0, 2 * N * 8, cudaMemcpyDeviceToDevice, s));
-    SS_CK(cudaMemsetAsync(G.p_last, 0, 2 * N * 8, s));
-    SS_CK(cudaMemsetAsync(G.delta_p, 0, 2 * N * 8, s));
-    SS_CK(cudaMemsetAsync(G.params_used, 0, N, s));
-    SS_CK(cudaMemsetAsync(G.blocks_present, 0, N, s));
-    SS_CK(cudaMemsetAsync(G.grp_active, 1, 2 * (size_t)g.n_rg, s));
-    SS_CK(cudaMemsetAsync(G.grp_active + 2 * (size_t)g.n_rg, 0, 1, s));
-    SS_CK(cudaMemsetAsync(G.o_frame_corr, 0, nF * 8, s));
-    SS_CK(cudaMemsetAsync(G.eig_valid, 0, N, s));
-    SS_CK(cudaMemsetAsync(G.ls_done, 0, nF * sizeof(int), s));
-    if (G.o_rg_params) SS_CK(cudaMemsetAsync(G.o_rg_params, 0, (size_t)2 * N * 2 * g.in->max_iter * 8, s));
-    if (G.o_iter_times) SS_CK(cudaMemsetAsync(G.o_iter_times, 0, (size_t)g.in->max_iter * 8, s));
-    k_fill<<<64, 256, 0, s>>>(G.errval, 2 * nF, kErrvalFill);
-    // the reference's x/y/mask/difference buffers start zero-filled: NaN knots give an all-invalid
-    // mask and a zero difference image
-    k_fill<<<64, 256, 0, s>>>(G.kmask, nF * 2 * (g.W + 1), NAN);
-    k_fill<<<64, 256, 0, s>>>(G.kdiff, nF * 2 * (g.W + 1), NAN);
-    k_fill<<<64, 256, 0, s>>>(G.asmk, (size_t)g.fW * 8, NAN);  // no column keeps sums of an earlier run
-    SS_CK(cudaGetLastError());
     GroupCtl& C = b->h_ctl[i];
     std::memset(&C, 0, sizeof(C));
     C.phase = b->stream_req && !g.frames_dev ? kPhWait : kPhHalf;
@@ -1804,6 +1827,22 @@ void Batch::stats(ss_batch_stats* st) const {
 int Batch::collect() {
   Impl* b = d;
   cudaStream_t s = b->stream;
+  // outputs come back through the page-locked staging buffer where it has room (copied out after
+  // the stream has drained), else straight into the caller's arrays
+  Staging stg(s, b->own_stream);
+  struct Pending {
+    void* dst;
+    const void* src;
+    size_t n;
+  };
+  std::vector<Pending> pend;
+  auto get = [&](void* dst, const void* src, size_t n) -> cudaError_t {
+    if (!n) return cudaSuccess;
+    void* p = stg.take(n);
+    if (!p) return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s);
+    pend.push_back({dst, p, n});
+    return cudaMemcpyAsync(p, src, n, cudaMemcpyDeviceToHost, s);
+  };
   SS_CK(cudaMemcpyAsync(b->h_ctl.data(), b->d_ctl, b->h_ctl.size() * sizeof(GroupCtl), cudaMemcpyDeviceToHost, s));
   for (size_t i = 0; i < b->gd.size(); i++) {
     ss_outputs* o = b->outs[i];
@@ -1812,32 +1851,32 @@ int Batch::collect() {
     const GroupDesc& G = b->gd[i];
     const size_t nF = g.nF, nk = (size_t)(g.W + 1) * nF;
     const bool frame_ordered = g.flags & kFlagFrameOrdered;
-    if (o->dx_knots && !frame_ordered) SS_CK(cudaMemcpyAsync(o->dx_knots, G.o_dx, nk * 8, cudaMemcpyDeviceToHost, s));
-    if (o->dy_knots && !frame_ordered) SS_CK(cudaMemcpyAsync(o->dy_knots, G.o_dy, nk * 8, cudaMemcpyDeviceToHost, s));
-    if (o->frame_corr) SS_CK(cudaMemcpyAsync(o->frame_corr, G.o_frame_corr, nF * 8, cudaMemcpyDeviceToHost, s));
-    if (o->residrms) SS_CK(cudaMemcpyAsync(o->residrms, G.o_residrms, nF * 8, cudaMemcpyDeviceToHost, s));
-    if (o->mask) SS_CK(cudaMemcpyAsync(o->mask, G.o_mask, (size_t)g.Hb * g.fW, cudaMemcpyDeviceToHost, s));
-    if (o->blocks_used) SS_CK(cudaMemcpyAsync(o->blocks_used, G.o_blocks_used, g.fW, cudaMemcpyDeviceToHost, s));
+    if (o->dx_knots && !frame_ordered) SS_CK(get(o->dx_knots, G.o_dx, nk * 8));
+    if (o->dy_knots && !frame_ordered) SS_CK(get(o->dy_knots, G.o_dy, nk * 8));
+    if (o->frame_corr) SS_CK(get(o->frame_corr, G.o_frame_corr, nF * 8));
+    if (o->residrms) SS_CK(get(o->residrms, G.o_residrms, nF * 8));
+    if (o->mask) SS_CK(get(o->mask, G.o_mask, (size_t)g.Hb * g.fW));
+    if (o->blocks_used) SS_CK(get(o->blocks_used, G.o_blocks_used, g.fW));
     const size_t mi = g.in->max_iter;
-    if (o->iteration_corr) SS_CK(cudaMemcpyAsync(o->iteration_corr, G.o_iter_corr, mi * 8, cudaMemcpyDeviceToHost, s));
+    if (o->iteration_corr) SS_CK(get(o->iteration_corr, G.o_iter_corr, mi * 8));
     if (o->frame_corr_history)
-      SS_CK(cudaMemcpyAsync(o->frame_corr_history, G.o_frame_corr_hist, mi * nF * 8, cudaMemcpyDeviceToHost, s));
+      SS_CK(get(o->frame_corr_history, G.o_frame_corr_hist, mi * nF * 8));
     if (o->iteration_errvals)
-      SS_CK(cudaMemcpyAsync(o->iteration_errvals, G.o_iter_errvals, 2 * mi * nF * 8, cudaMemcpyDeviceToHost, s));
-    if (o->all_params) SS_CK(cudaMemcpyAsync(o->all_params, G.o_all_params, 2 * (size_t)g.N * mi * 8, cudaMemcpyDeviceToHost, s));
+      SS_CK(get(o->iteration_errvals, G.o_iter_errvals, 2 * mi * nF * 8));
+    if (o->all_params) SS_CK(get(o->all_params, G.o_all_params, 2 * (size_t)g.N * mi * 8));
     if (o->frame_params && frame_ordered)
-      SS_CK(cudaMemcpyAsync(o->frame_params, G.o_frame_params, 2 * nk * 8, cudaMemcpyDeviceToHost, s));
+      SS_CK(get(o->frame_params, G.o_frame_params, 2 * nk * 8));
     if (o->raw_params && (g.flags & kFlagRawParams))
-      SS_CK(cudaMemcpyAsync(o->raw_params, G.o_raw, 2 * (size_t)g.N * 8, cudaMemcpyDeviceToHost, s));
+      SS_CK(get(o->raw_params, G.o_raw, 2 * (size_t)g.N * 8));
     // outputs 9, 10, 14: zeros where the flags do not produce them
     if (o->rg_params) {
       if (G.o_rg_params)
-        SS_CK(cudaMemcpyAsync(o->rg_params, G.o_rg_params, (size_t)2 * g.N * 2 * mi * 8, cudaMemcpyDeviceToHost, s));
+        SS_CK(get(o->rg_params, G.o_rg_params, (size_t)2 * g.N * 2 * mi * 8));
       else
         std::memset(o->rg_params, 0, (size_t)2 * g.N * 2 * mi * 8);
     }
     if (o->iteration_times) {
-      if (G.o_iter_times) SS_CK(cudaMemcpyAsync(o->iteration_times, G.o_iter_times, mi * 8, cudaMemcpyDeviceToHost, s));
+      if (G.o_iter_times) SS_CK(get(o->iteration_times, G.o_iter_times, mi * 8));
       else std::memset(o->iteration_times, 0, mi * 8);
     }
     if (o->function_times)
@@ -1845,6 +1884,8 @@ int Batch::collect() {
         o->function_times[k] = (g.flags & kFlagTimeSub) ? b->ftimes[k] : 0.0;
   }
   SS_CK(cudaStreamSynchronize(s));
+  for (const Pending& q : pend) std::memcpy(q.dst, q.src, q.n);
+  stg.release();
   for (size_t i = 0; i < b->gd.size(); i++) {
     ss_outputs* o = b->outs[i];
     if (!o) continue;
