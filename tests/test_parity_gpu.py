@@ -306,6 +306,39 @@ def test_streamed_uploads_equal_the_resident_batch(prec):
             np.testing.assert_array_equal(a[k], r[k])
 
 
+def test_concurrent_calls_share_the_staging_buffer():
+    """Calls from several host threads at once (ctypes releases the GIL) take turns on the
+    library's page-locked staging buffer for their small uploads and result copies: each call gets
+    the results it gets alone."""
+    import threading
+    specs = [dict(seed=51 + k, n_frames=2 + k % 3, frame_dtype=np.uint16) for k in range(4)]
+    groups = [dict(make_args(**sp)[0], flags="S" if k % 2 else "D") for k, sp in enumerate(specs)]
+    alone = [api.align_group(g) for g in groups]
+    out = [[] for _ in groups]
+    errs = []
+
+    def work(k):
+        try:
+            for _ in range(3):
+                out[k].append(api.align_group(groups[k]))
+        except Exception as e:  # noqa: BLE001 - reported below
+            errs.append(e)
+
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(len(groups))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    assert not errs, errs
+    assert not any(t.is_alive() for t in threads)
+    for a, rs in zip(alone, out):
+        assert len(rs) == 3
+        for r in rs:
+            assert a["iter_used"] == r["iter_used"]
+            for k in ("dx", "dy", "frame_corr", "residrms", "mask"):
+                np.testing.assert_array_equal(a[k], r[k])
+
+
 def test_persistent_grid_many_tiles_precision_s():
     """A batch with more tiles (block column x frame chunk) than the persistent grid has CTAs, so
     every CTA takes several tiles, and searches spread over several cycles: each group still gets
