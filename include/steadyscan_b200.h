@@ -252,8 +252,8 @@ SS_API int ss_solve_block_tridiagonal(int32_t n, const double* diag, const doubl
  * 32768 blocks (3.4 MB, held by every GPU that loads the library until the process exits), so
  * n > 32768 is rejected with SS_ERR_INVALID_ARGUMENT. The first call on a device looks up that
  * array's device address and sets the solve kernel's shared-memory attribute (again after the
- * device's context has been reset, e.g. by cudaDeviceReset), so make that first call before any
- * stream capture. Each call waits for `stream` (cudaStreamSynchronize) before it returns. All calls
+ * device's context has been reset, e.g. by cudaDeviceReset). Each call waits for `stream`
+ * (cudaStreamSynchronize) before it returns. All calls
  * share the one array per device: calls that overlap on the GPU (different streams or threads at
  * the same time) race and corrupt each other's results; serialize them. Each call writes every part
  * of the workspace it reads before reading it. */
